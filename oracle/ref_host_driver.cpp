@@ -1,0 +1,183 @@
+// extern "C" entry points over the reference's own host code (compiled from the
+// reference tree by oracle/build_ref.py).  Test infrastructure only: these pin
+// the oracle restatement (oracle/oracle.cpp) to the reference's behaviour.
+//
+// Including Src/meshmapping.cpp here reaches fillMeshData, which sits in an
+// anonymous namespace (Src/meshmapping.cpp:33-126).  The GL-facing functions it
+// and Src/compute.cpp refer to are linked but never called.
+#include "meshmapping.cpp"
+
+#include "bvh.h"
+#include "compute.h"
+#include "image.h"
+#include "mesh.h"
+#include <cstring>
+
+static unsigned int g_seed = 0;
+unsigned int std::fornos_seeded_device::operator()() { return g_seed; }
+
+// Logging and image export are not part of the path; silent stand-ins.
+void logDebug(const std::string&, const std::string&) {}
+void logWarning(const std::string&, const std::string&) {}
+void logError(const std::string&, const std::string&) {}
+void exportNormalImage(const Vector3*, const CompressedMapUV*, const char*, int) {}
+GLuint LoadComputeShader_MeshMapping() { return 0; }
+GLuint LoadComputeShader_MeshMappingCullBackfaces() { return 0; }
+
+static Mesh* make_mesh(uint32_t np, const float* pos, uint32_t nt, const float* uv, uint32_t nn, const float* nrm,
+                       uint32_t nv, const uint32_t* vtx, uint32_t nf, const uint32_t* tri) {
+  Mesh* m = new Mesh();
+  m->positions.resize(np);
+  for (uint32_t i = 0; i < np; ++i) m->positions[i] = Vector3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+  m->texcoords.resize(nt);
+  for (uint32_t i = 0; i < nt; ++i) m->texcoords[i] = Vector2(uv[2 * i], uv[2 * i + 1]);
+  m->normals.resize(nn);
+  for (uint32_t i = 0; i < nn; ++i) m->normals[i] = Vector3(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]);
+  m->vertices.resize(nv);
+  for (uint32_t i = 0; i < nv; ++i) m->vertices[i] = Mesh::Vertex{vtx[3 * i], vtx[3 * i + 1], vtx[3 * i + 2]};
+  m->triangles.resize(nf);
+  for (uint32_t i = 0; i < nf; ++i) m->triangles[i] = Mesh::Triangle{tri[3 * i], tri[3 * i + 1], tri[3 * i + 2]};
+  return m;
+}
+
+static void copy_normals(const Mesh* m, uint32_t* vtx_out, float* nrm_out) {
+  for (size_t i = 0; i < m->vertices.size(); ++i) {
+    vtx_out[3 * i] = m->vertices[i].positionIndex;
+    vtx_out[3 * i + 1] = m->vertices[i].texcoordIndex;
+    vtx_out[3 * i + 2] = m->vertices[i].normalIndex;
+  }
+  for (size_t i = 0; i < m->normals.size(); ++i) {
+    nrm_out[3 * i] = m->normals[i].x;
+    nrm_out[3 * i + 1] = m->normals[i].y;
+    nrm_out[3 * i + 2] = m->normals[i].z;
+  }
+}
+
+extern "C" {
+
+// which: 0 face, 1 vertex, 2 welded (aggressive).  Returns the normal count.
+int ref_normals(int which, uint32_t np, const float* pos, uint32_t nv, const uint32_t* vtx, uint32_t nf,
+                const uint32_t* tri, uint32_t* vtx_out, float* nrm_out) {
+  Mesh* m = make_mesh(np, pos, 0, nullptr, 0, nullptr, nv, vtx, nf, tri);
+  if (which == 0) m->computeFaceNormals();
+  else if (which == 1) m->computeVertexNormals();
+  else m->computeVertexNormalsAggressive();
+  copy_normals(m, vtx_out, nrm_out);
+  int n = (int)m->normals.size();
+  delete m;
+  return n;
+}
+
+int ref_tangent_space(uint32_t np, const float* pos, uint32_t nt, const float* uv, uint32_t nn, const float* nrm,
+                      uint32_t nv, const uint32_t* vtx, uint32_t nf, const uint32_t* tri, float* tan_out,
+                      float* bit_out) {
+  Mesh* m = make_mesh(np, pos, nt, uv, nn, nrm, nv, vtx, nf, tri);
+  m->computeTangentSpace();
+  for (uint32_t i = 0; i < nv; ++i) {
+    tan_out[3 * i] = m->tangents[i].x; tan_out[3 * i + 1] = m->tangents[i].y; tan_out[3 * i + 2] = m->tangents[i].z;
+    bit_out[3 * i] = m->bitangents[i].x; bit_out[3 * i + 1] = m->bitangents[i].y; bit_out[3 * i + 2] = m->bitangents[i].z;
+  }
+  delete m;
+  return 0;
+}
+
+struct RefScene {
+  std::vector<BVHGPUData> nodes;
+  std::vector<Vector4> pos, nrm;
+};
+
+void* ref_scene_build(uint32_t np, const float* pos, uint32_t nn, const float* nrm, uint32_t nv, const uint32_t* vtx,
+                      uint32_t nf, const uint32_t* tri, uint32_t max_tris, uint32_t max_depth) {
+  Mesh* m = make_mesh(np, pos, 0, nullptr, nn, nrm, nv, vtx, nf, tri);
+  BVH* root = BVH::createBinary(m, max_tris, max_depth);
+  RefScene* s = new RefScene();
+  fillMeshData(m, *root, s->nodes, s->pos, s->nrm);
+  delete root;
+  delete m;
+  return s;
+}
+
+int ref_scene_sizes(void* h, uint32_t* nodes, uint32_t* corners) {
+  RefScene* s = (RefScene*)h;
+  *nodes = (uint32_t)s->nodes.size();
+  *corners = (uint32_t)s->pos.size();
+  return 0;
+}
+
+int ref_scene_copy(void* h, void* nodes36, float* pos4, float* nrm4) {
+  RefScene* s = (RefScene*)h;
+  static_assert(sizeof(BVHGPUData) == 36, "node layout");
+  if (!s->nodes.empty()) std::memcpy(nodes36, s->nodes.data(), s->nodes.size() * 36);
+  for (size_t i = 0; i < s->pos.size(); ++i) {
+    pos4[4 * i] = s->pos[i].x; pos4[4 * i + 1] = s->pos[i].y; pos4[4 * i + 2] = s->pos[i].z; pos4[4 * i + 3] = s->pos[i].w;
+    nrm4[4 * i] = s->nrm[i].x; nrm4[4 * i + 1] = s->nrm[i].y; nrm4[4 * i + 2] = s->nrm[i].z; nrm4[4 * i + 3] = s->nrm[i].w;
+  }
+  return 0;
+}
+
+void ref_scene_free(void* h) { delete (RefScene*)h; }
+
+// mode: 0 Smooth (fromMeshes), 1 LowPolyNormals (fromMesh), 2 Hybrid.
+// tan/bit: per-vertex tangent frame or null.  dvtx/dnrm: the direction mesh's
+// vertex normal indices and normals (modes 0 and 2).
+void* ref_raster(uint32_t np, const float* pos, uint32_t nt, const float* uv, uint32_t nn, const float* nrm,
+                 uint32_t nv, const uint32_t* vtx, uint32_t nf, const uint32_t* tri, const float* tan,
+                 const float* bit, const uint32_t* dvtx, uint32_t dnn, const float* dnrm, uint32_t w, uint32_t h,
+                 int mode, float edge) {
+  Mesh* m = make_mesh(np, pos, nt, uv, nn, nrm, nv, vtx, nf, tri);
+  if (tan) {
+    m->tangents.resize(nv);
+    m->bitangents.resize(nv);
+    for (uint32_t i = 0; i < nv; ++i) {
+      m->tangents[i] = Vector3(tan[3 * i], tan[3 * i + 1], tan[3 * i + 2]);
+      m->bitangents[i] = Vector3(bit[3 * i], bit[3 * i + 1], bit[3 * i + 2]);
+    }
+  }
+  Mesh* d = nullptr;
+  if (mode != 1) {
+    d = Mesh::createCopy(m);
+    d->normals.resize(dnn);
+    for (uint32_t i = 0; i < dnn; ++i) d->normals[i] = Vector3(dnrm[3 * i], dnrm[3 * i + 1], dnrm[3 * i + 2]);
+    for (uint32_t i = 0; i < nv; ++i) d->vertices[i].normalIndex = dvtx[3 * i + 2];
+  }
+  MapUV* map = nullptr;
+  if (mode == 0) map = MapUV::fromMeshes(m, d, w, h);
+  else if (mode == 1) map = MapUV::fromMesh(m, w, h);
+  else map = MapUV::fromMeshes_Hybrid(m, d, w, h, edge);
+  CompressedMapUV* c = map ? new CompressedMapUV(map) : nullptr;
+  delete map;
+  delete d;
+  delete m;
+  return c;
+}
+
+int ref_cmap_copy(void* h, uint32_t* count, uint32_t* idx, float* pos, float* dir, float* nrm, float* tan,
+                  float* bit) {
+  CompressedMapUV* c = (CompressedMapUV*)h;
+  *count = (uint32_t)c->indices.size();
+  if (!idx) return 0;
+  for (size_t i = 0; i < c->indices.size(); ++i) {
+    idx[i] = c->indices[i];
+    const Vector3* src[5] = {&c->positions[i], &c->directions[i], &c->normals[i], &c->tangents[i], &c->bitangents[i]};
+    float* dst[5] = {pos, dir, nrm, tan, bit};
+    for (int k = 0; k < 5; ++k) {
+      dst[k][3 * i] = src[k]->x; dst[k][3 * i + 1] = src[k]->y; dst[k][3 * i + 2] = src[k]->z;
+    }
+  }
+  return 0;
+}
+
+void ref_cmap_free(void* h) { delete (CompressedMapUV*)h; }
+
+// Src/math.h:363-382, engine seeded with `seed` through the shim.
+int ref_samples(uint32_t spp, uint32_t perms, uint32_t seed, float* out4) {
+  g_seed = seed;
+  std::vector<Vector3> v((size_t)spp * perms);
+  computeSamplesImportanceCosDir(spp, perms, v.data());
+  for (size_t i = 0; i < v.size(); ++i) {
+    out4[4 * i] = v[i].x; out4[4 * i + 1] = v[i].y; out4[4 * i + 2] = v[i].z; out4[4 * i + 3] = 0.0f;
+  }
+  return 0;
+}
+
+}  // extern "C"
