@@ -1,0 +1,466 @@
+"""Headline benchmark: plain bake throughput (Mrays/s) on one or more B200s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fornos|reference]
+                    [--workload plane2048|sphere512|icosphere4096] [--traverse auto|ordered|skip]
+
+One step = one full plain bake of the workload with every input resident in
+HBM: mesh mapping (2 rays / texel), height, position and tangent-space normal
+gathers, ambient occlusion + bent normals (one traversal, spp rays / texel,
+counted as the reference's two sampling kernels) and thickness (spp rays /
+texel).  value = rays of all ranks / max-over-ranks device time.  e2e = the
+same bake through fk_bake from pinned host arrays (uploads and result copies
+inside the timed region).  Multi-GPU: one process per GPU, each baking its
+own seeded replica of the workload (weak scaling, no data-path collective).
+
+--impl reference times the reference's own CPU implementation of the path
+(the reference's shaders and host code compiled by oracle/build_ref.py, or
+the oracle restatement when that build is absent) on the host cores, on a
+strided texel sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from fornos_b200 import workloads as W  # noqa: E402
+
+WORKLOADS = {
+    "plane2048": dict(
+        desc="plain bake, all six bakers, 2048x2048: 64x64-quad plane low-poly, 1024x1024-quad heightfield "
+             "high-poly (2,097,152 tris, 4-octave value noise + 200 bumps), AO / bent normals / thickness "
+             "256 spp, min 0.001, max 0.3",
+        gen=lambda seed: W.plane_pair(seed=seed, lo_quads=64, hi_quads=1024, bumps=200),
+        tex=2048, spp=256, min_d=0.001, max_d=0.3, bakers=("height", "position", "normals", "ao", "bn", "thick")),
+    "sphere512": dict(
+        desc="plain bake, 512x512: 32x16 UV-sphere low-poly, 512x256 perturbed UV-sphere high-poly, height, "
+             "tangent-space normals, AO 64 spp (min 0.001, max 0.5)",
+        gen=lambda seed: W.sphere_pair(seed=seed),
+        tex=512, spp=64, min_d=0.001, max_d=0.5, bakers=("height", "normals", "ao")),
+    "icosphere4096": dict(
+        desc="plain large bake, 4096x4096: subdivision-3 icosphere low-poly (cube-projection UVs), "
+             "subdivision-9 icosphere high-poly (5,242,880 tris, 6-octave gradient noise), AO / bent normals / "
+             "thickness 1024 spp, max 0.5",
+        gen=lambda seed: W.icosphere_pair(seed=seed),
+        tex=4096, spp=1024, min_d=0.001, max_d=0.5, bakers=("ao", "bn", "thick")),
+}
+TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2}
+# DRAM bytes per hemisphere-kernel launch from ncu captures (profiles/), by workload.
+NCU_TRAFFIC = {}
+
+
+def rays_per_texel(wl):
+    spp = wl["spp"]
+    return 2 + spp * sum(k in wl["bakers"] for k in ("ao", "bn", "thick"))
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clock and throttle reasons through NVML while running."""
+
+    def __init__(self, device_index):
+        self.samples, self.reasons, self.max_mhz = [], set(), None
+        self._stop = threading.Event()
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self.nv = None
+
+    def _run(self):
+        nv = self.nv
+        names = {
+            "hw_slowdown": getattr(nv, "nvmlClocksEventReasonHwSlowdown", 0x8),
+            "sw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+            "hw_thermal_slowdown": getattr(nv, "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+            "sw_power_cap": getattr(nv, "nvmlClocksEventReasonSwPowerCap", 0x4),
+        }
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for k, bit in names.items():
+                    if r & bit:
+                        self.reasons.add(k)
+            except Exception:
+                pass
+            self._stop.wait(0.1)
+
+    def __enter__(self):
+        if self.nv:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        if self.nv:
+            self.t.join()
+
+    def summary(self):
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": sorted(self.reasons)}
+
+
+# ---------------------------------------------------------------- setup
+class Prepared:
+    """Host preprocessing of Src/fornos.cpp:53-157 with the product's host code."""
+
+    def __init__(self, wl, seed):
+        from fornos_b200 import api
+        t0 = time.perf_counter()
+        lo, hi = wl["gen"](seed)
+        self.gen_s = time.perf_counter() - t0
+        self.hm = api.Mesh(hi)
+        self.hm.compute_vertex_normals()
+        self.lm = api.Mesh(lo)
+        self.lm.compute_tangent_space()
+        self.dm = self.lm.copy()
+        self.dm.compute_vertex_normals_aggressive()
+        t0 = time.perf_counter()
+        self.bvh = api.BVH.create_binary(self.hm, 8, 8192)
+        self.bvh_s = time.perf_counter() - t0
+        self.nodes, self.pos4, self.nrm4 = self.bvh.flatten(self.hm)
+        self.triangles = hi.triangle_count
+
+
+def pinned(shape, dtype):
+    import torch
+    t = torch.empty(int(np.prod(shape)) * np.dtype(dtype).itemsize, dtype=torch.uint8, pin_memory=True)
+    return t.numpy().view(dtype).reshape(shape), t
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_fornos(args, wl, rank, world):
+    import torch
+
+    from fornos_b200 import api
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    ctx = api.Context(dev)
+    ctx.set_stream(stream.cuda_stream)
+    trav = TRAVERSE[args.traverse]
+    prep = Prepared(wl, args.seed + rank)
+    tex, spp, lo_d, hi_d = wl["tex"], wl["spp"], wl["min_d"], wl["max_d"]
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        tmap = api.TexelMap.from_meshes(ctx, prep.lm, prep.dm, tex, tex)
+        e1.record(stream)
+    stream.synchronize()
+    raster_ms = e0.elapsed_time(e1)
+    n = tmap.count
+    scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
+    info = scene.info()
+    samples = api.samples_cosine(spp, api.PERMS, args.seed)
+    sbuf = ctx.upload(samples)
+    B = {k: ctx.buffer(w * max(n, 1)) for k, w in (("coords", 16), ("tidx", 4), ("height", 4), ("position", 12),
+                                                  ("normals", 12), ("ao", 4), ("bn", 12), ("thick", 4))}
+    bakers = wl["bakers"]
+    hemi_events = []
+
+    def step(record):
+        api.meshmap(ctx, scene, tmap, True, B["coords"], B["tidx"])
+        if "height" in bakers:
+            api.gather(ctx, scene, api.GATHER_HEIGHT, B["coords"], B["tidx"], B["height"], 0, n)
+        if "position" in bakers:
+            api.gather(ctx, scene, api.GATHER_POSITION, B["coords"], B["tidx"], B["position"], 0, n)
+        if "normals" in bakers:
+            api.gather(ctx, scene, api.GATHER_NORMAL, B["coords"], B["tidx"], B["normals"], 0, n)
+            api.tangent_space(ctx, tmap, B["normals"])
+        launches = []
+        if "ao" in bakers or "bn" in bakers:
+            kind = api.AO_BN if ("ao" in bakers and "bn" in bakers) else (api.AO if "ao" in bakers else api.BN)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            api.hemisphere(ctx, scene, B["coords"], B["tidx"], kind, spp, lo_d, hi_d, sbuf,
+                           B["ao"] if kind != api.BN else B["bn"], B["bn"] if kind == api.AO_BN else None,
+                           None, None, 0, n, traverse=trav)
+            b.record(stream)
+            launches.append((a, b, kind))
+            if "bn" in bakers:
+                api.tangent_space(ctx, tmap, B["bn"])
+        if "thick" in bakers:
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            api.hemisphere(ctx, scene, B["coords"], B["tidx"], api.THICK, spp, lo_d, hi_d, sbuf, B["thick"],
+                           None, None, None, 0, n, traverse=trav)
+            b.record(stream)
+            launches.append((a, b, api.THICK))
+        if record:
+            hemi_events.append(launches)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step(False)
+    stream.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.launches
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        with torch.cuda.stream(stream):
+            t0.record(stream)
+            for _ in range(args.steps):
+                step(True)
+            t1.record(stream)
+        stream.synchronize()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    gpu_launches = ctx.launches - launches0
+    ms = t0.elapsed_time(t1) / args.steps
+    hemi_ms = {}
+    for launches in hemi_events:
+        for a, b, kind in launches:
+            hemi_ms.setdefault(kind, []).append(a.elapsed_time(b))
+    rays = rays_per_texel(wl) * n
+    ms_max = ms
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+        tot = torch.tensor([float(rays)], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(tot)
+        rays_all = float(tot.item())
+    else:
+        rays_all = float(rays)
+
+    # ---- end to end through fk_bake from pinned host memory
+    keep = []
+
+    def pin(a):
+        p, t = pinned(a.shape, a.dtype)
+        p[...] = a
+        keep.append(t)
+        return p
+
+    cm = tmap.download()
+    pix8 = np.zeros((n, 8), np.float32)
+    pix8[:, 0:3], pix8[:, 4:7] = cm["positions"], cm["directions"]
+    pixt = np.zeros((n, 12), np.float32)
+    pixt[:, 0:3], pixt[:, 4:7], pixt[:, 8:11] = cm["normals"], cm["tangents"], cm["bitangents"]
+    h_nodes, h_pos, h_nrm = pin(prep.nodes), pin(prep.pos4), pin(prep.nrm4)
+    h_pix, h_pixt, h_idx = pin(pix8), pin(pixt), pin(cm["indices"])
+    outs = {k: pinned(shape, dt) for k, shape, dt in (
+        ("height", (n,), np.float32), ("position3", (n, 3), np.float32), ("normals3", (n, 3), np.float32),
+        ("ao", (n,), np.float32), ("bent_normals3", (n, 3), np.float32), ("thickness", (n,), np.float32))}
+    out_arrays = {k: v[0] for k, v in outs.items()}
+    sampler = dict(sample_count=spp, min_distance=lo_d, max_distance=hi_d, seed=args.seed)
+    kw = dict(height_map="height" in bakers, position_map="position" in bakers, normals_map="normals" in bakers,
+              ao=sampler if "ao" in bakers else None,
+              bent_normals=dict(sampler, tangent_space=True) if "bn" in bakers else None,
+              thickness=sampler if "thick" in bakers else None, traverse=trav)
+
+    def e2e_step():
+        api.bake(ctx, h_nodes, h_pos, h_nrm, tex, tex, h_pix, h_pixt, h_idx, out_arrays, **kw)
+
+    e2e_step()  # warm-up
+    if world > 1:
+        torch.distributed.barrier()
+    w0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_ms = (time.perf_counter() - w0) * 1e3 / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    h2d = sum(a.nbytes for a in (h_nodes, h_pos, h_nrm, h_pix, h_pixt, h_idx)) + samples.nbytes
+    d2h = sum(a.nbytes for k, a in out_arrays.items()
+              if (k == "height" and "height" in bakers) or (k == "position3" and "position" in bakers)
+              or (k == "normals3" and "normals" in bakers) or (k == "ao" and "ao" in bakers)
+              or (k == "bent_normals3" and "bn" in bakers) or (k == "thickness" and "thick" in bakers))
+
+    # ---- roofline of the dominant kernel (hemisphere traversal)
+    peak = api.fp32_peak(ctx)
+    tests = {}
+    for launches in hemi_events[:1]:
+        for _, _, kind in launches:
+            tests[kind] = api.traversal_counts(ctx, scene, B["coords"], B["tidx"], kind, spp, lo_d, hi_d, sbuf, 0, n,
+                                               traverse=trav)
+    flops = sum(24 * b + 104 * t for b, t in tests.values())
+    kern_ms = sum(statistics.mean(v) for v in hemi_ms.values())
+    achieved = flops / (kern_ms * 1e-3)
+    mrays = rays_all / (ms_max * 1e-3) / 1e6
+    result = {
+        "metric": "Mrays/s (plain bake: mapping + AO + bent normals + thickness rays)",
+        "value": round(mrays, 3), "unit": "Mrays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms_max, 3), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded generated meshes; no public dataset)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "texels": n, "texture": tex, "spp": spp,
+                   "high_poly_triangles": prep.triangles, "bvh_nodes": info["node_count"],
+                   "bvh_depth": info["depth"], "traverse": args.traverse,
+                   "rays_per_texel": rays_per_texel(wl),
+                   "rays_counted": "2 mapping + spp each for AO, bent normals, thickness (AO and bent normals "
+                                   "share one traversal)",
+                   "l2": "inputs larger than L2 (scene %.0f MB resident)" % (info["device_bytes"] / 1e6),
+                   "bvh_build_s": round(prep.bvh_s, 3), "raster_ms": round(raster_ms, 3),
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "e2e": {"value": round(rays_all / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
+                "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(gpu_launches),
+        "roofline": {"bound": "fp32", "kernel": "hemi_kernel", "achieved": round(achieved / 1e12, 3),
+                     "peak": round(peak / 1e12, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
+                     "traffic": NCU_TRAFFIC.get(args.workload),
+                     "peak_source": "measured in-run: fk_diag_fp32_peak (add/mul/min chains, 1 op per instruction)",
+                     "flops_per_step": int(flops), "kernel_ms_per_step": round(kern_ms, 3),
+                     "box_tests": {str(k): v[0] for k, v in tests.items()},
+                     "tri_tests": {str(k): v[1] for k, v in tests.items()},
+                     "flop_model": "24 per ray-box test + 104 per ray-triangle test, tests counted on the GPU"},
+        "clocks": clk.summary(),
+    }
+    return result, (prep, tmap, B, n)
+
+
+# ---------------------------------------------------------------- CPU arm
+class CpuBaseline:
+    """The reference's CPU implementation of the path, timed on the host
+    cores (all OpenMP threads) over a strided sample of the workload's
+    compressed texels: the reference's shaders and host code compiled by
+    oracle/build_ref.py, or the oracle restatement where that build is absent."""
+
+    def __init__(self, wl, seed, prep=None, cmap=None, prefer_ref=True):
+        from oracle import pyoracle
+        self.oracle = pyoracle.Oracle()
+        ref = None
+        if prefer_ref:
+            try:
+                ref = pyoracle.Reference()
+            except OSError:
+                ref = None
+        self.impl = ref if ref is not None else self.oracle
+        self.kind = "reference" if ref is not None else "port"
+        self.cores = self.oracle.threads()
+        self.wl, self.spp = wl, wl["spp"]
+        tex = wl["tex"]
+        if prep is None:
+            impl = self.impl
+            lo, hi = wl["gen"](seed)
+            v, nrm = impl.normals(hi, "vertex")
+            hi.vertices, hi.normals = v, nrm
+            lo.tangents, lo.bitangents = impl.tangent_space(lo)
+            cmap = impl.raster(lo, tex, tex, 0, impl.normals(lo, "welded"))
+            self.nodes, self.pos4, self.nrm4 = impl.scene(hi)
+        else:
+            self.nodes, self.pos4, self.nrm4 = prep.nodes, prep.pos4, prep.nrm4
+        self.n = n = len(cmap["indices"])
+        self.pix8 = np.zeros((n, 8), np.float32)
+        self.pix8[:, 0:3], self.pix8[:, 4:7] = cmap["positions"], cmap["directions"]
+        self.kinds = [k for k, b in ((0, "ao"), (1, "bn"), (2, "thick")) if b in wl["bakers"]]
+        self.samples = self.impl.samples(self.spp, 4096, seed)
+        self.stride = max(1, n // 64)
+
+    def run(self, stride=None):
+        stride = stride or self.stride
+        n, impl = self.n, self.impl
+        sel = np.arange(0, n, stride, dtype=np.uint32)
+        t0 = time.perf_counter()
+        c_sel, t_sel = impl.meshmap(self.nodes, self.pos4, self.pix8[sel], True)
+        coords = np.zeros((n, 4), np.float32)
+        tidx = np.full(n, 0xFFFFFFFF, np.uint32)
+        coords[sel], tidx[sel] = c_sel, t_sel
+        for k in self.kinds:
+            impl.hemisphere(k, self.nodes, self.pos4, self.nrm4, coords, tidx, self.samples, self.spp,
+                            self.wl["min_d"], self.wl["max_d"], texels=sel)
+        dt = time.perf_counter() - t0
+        rays = len(sel) * (2 + self.spp * len(self.kinds))
+        return rays / dt / 1e6, rays, dt, len(sel)
+
+    def calibrate(self, budget_s):
+        """Chooses the texel stride so one run takes about budget_s seconds."""
+        stride = max(1, self.n // 64)
+        _, _, dt, _ = self.run(stride)
+        while dt < 0.25 and stride > 1:
+            stride = max(1, stride // 8)
+            _, _, dt, _ = self.run(stride)
+        self.stride = max(1, int(stride * dt / budget_s)) if dt < budget_s else stride
+        return self.stride
+
+    def describe(self, rays, m):
+        return "every %d-th of %d compressed texels (%d texels, %d rays): mapping + %s at %d spp" % (
+            self.stride, self.n, m, rays, " + ".join({0: "AO", 1: "BN", 2: "thickness"}[k] for k in self.kinds),
+            self.spp)
+
+
+def run_reference_arm(args, wl):
+    cpu = CpuBaseline(wl, args.seed)
+    cpu.calibrate(args.cpu_seconds)
+    vals = []
+    rays = m = 0
+    for i in range(args.warmup + args.steps):
+        mr, rays, dt, m = cpu.run()
+        if i >= args.warmup:
+            vals.append(mr)
+    value = statistics.median(vals)
+    return {
+        "metric": "Mrays/s (plain bake: mapping + AO + bent normals + thickness rays)", "impl": "reference",
+        "value": round(value, 4), "unit": "Mrays/s", "n_gpus": 0, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generated meshes; no public dataset)",
+        "config": {"workload": args.workload, "desc": wl["desc"]},
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cpu.cores, "kind": cpu.kind,
+                         "sample": cpu.describe(rays, m)},
+        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="fornos", choices=["fornos", "reference"])
+    ap.add_argument("--workload", default="plane2048", choices=list(WORKLOADS))
+    ap.add_argument("--traverse", default="auto", choices=list(TRAVERSE))
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference_arm(args, wl)))
+        return 0
+
+    import datetime
+
+    import torch
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
+    result, state = run_fornos(args, wl, rank, world)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        prep, tmap, _, _ = state
+        cpu = CpuBaseline(wl, args.seed, prep, tmap.download())
+        cpu.calibrate(args.cpu_seconds)
+        mr, rays, dt, m = cpu.run()
+        result["cpu_baseline"] = {"value": round(mr, 4), "unit": "Mrays/s", "cores": cpu.cores, "kind": cpu.kind,
+                                  "sample": cpu.describe(rays, m)}
+    if rank == 0:
+        print(json.dumps(result))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

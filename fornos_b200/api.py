@@ -1,0 +1,560 @@
+"""Python front-end of the bake path, over the C ABI (include/fornos_gpu.h).
+
+Names follow the reference's host API: Mesh (Src/mesh.h), BVH.create_binary
+(Src/bvh.h), TexelMap = MapUV + CompressedMapUV (Src/compute.h), MeshMapping
+(Src/meshmapping.h) and the six solvers (Src/solver_*.h) with init /
+run_step / get_results / progress.  FornosRunner (Src/fornos.h:129-149)
+drives a whole bake from FornosParameters-like settings.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib as L
+from .workloads import MeshArrays
+
+OK = 0
+MISS = 0xFFFFFFFF
+
+# kinds (include/fornos_gpu.h)
+AO, BN, THICK, AO_BN = 0, 1, 2, 3
+TRAVERSE_AUTO, TRAVERSE_ORDERED, TRAVERSE_SKIP = 0, 1, 2
+GATHER_HEIGHT, GATHER_POSITION, GATHER_NORMAL = 0, 1, 2
+MAP_SMOOTH, MAP_LOWPOLY_NORMALS, MAP_HYBRID = 0, 1, 2
+SOLVER_HEIGHT, SOLVER_POSITION, SOLVER_NORMALS, SOLVER_AO, SOLVER_BENT_NORMALS, SOLVER_THICKNESS = range(6)
+PERMS = 4096  # k_samplePermCount (Src/solver_ao.cpp:34)
+
+NODE_DTYPE = np.dtype([("lo", np.float32, 3), ("hi", np.float32, 3), ("start", np.uint32), ("end", np.uint32),
+                       ("jump", np.uint32)])
+
+
+class FornosError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("fornos error %d: %s" % (code, msg))
+        self.code = code
+
+
+def _f32(a):
+    return a.ctypes.data_as(L.f32p)
+
+
+def _u32(a):
+    return a.ctypes.data_as(L.u32p)
+
+
+def _check(rc, ctx=None, what=""):
+    if rc != OK:
+        msg = what
+        if ctx is not None and ctx.handle:
+            msg = (what + ": " if what else "") + L.load().fk_last_error(ctx.handle).decode()
+        raise FornosError(rc, msg)
+
+
+# ------------------------------------------------------------------ context
+class Context:
+    """One device context (fk_ctx); device work runs on its stream."""
+
+    def __init__(self, device=0):
+        self.lib = L.load()
+        h = L.c_vp()
+        rc = self.lib.fk_ctx_create(device, ctypes.byref(h))
+        if rc != OK:
+            raise FornosError(rc, "fk_ctx_create(%d) failed (needs a compute capability 10.x GPU)" % device)
+        self.handle = h.value
+
+    def close(self):
+        if self.handle:
+            self.lib.fk_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, cuda_stream_ptr):
+        _check(self.lib.fk_ctx_set_stream(self.handle, cuda_stream_ptr), self)
+
+    def sync(self):
+        _check(self.lib.fk_sync(self.handle), self)
+
+    @property
+    def launches(self):
+        return int(self.lib.fk_launch_count(self.handle))
+
+    def buffer(self, nbytes):
+        return Buffer(self, nbytes)
+
+    def upload(self, arr):
+        arr = np.ascontiguousarray(arr)
+        b = Buffer(self, max(arr.nbytes, 4))
+        b.upload(arr)
+        return b
+
+
+class Buffer:
+    """Device allocation (fk_buf), zero-filled on creation."""
+
+    def __init__(self, ctx, nbytes):
+        self.ctx = ctx
+        h = L.c_vp()
+        _check(ctx.lib.fk_buf_alloc(ctx.handle, nbytes, ctypes.byref(h)), ctx, "fk_buf_alloc")
+        self.handle = h.value
+        self.nbytes = nbytes
+        self.owned = True
+
+    @classmethod
+    def borrowed(cls, ctx, handle):
+        b = cls.__new__(cls)
+        b.ctx, b.handle, b.owned = ctx, handle, False
+        b.nbytes = ctx.lib.fk_buf_size(handle)
+        return b
+
+    def upload(self, arr, offset=0):
+        arr = np.ascontiguousarray(arr)
+        _check(self.ctx.lib.fk_buf_upload(self.ctx.handle, self.handle, offset, arr.ctypes.data, arr.nbytes), self.ctx)
+
+    def download(self, dtype, shape, offset=0):
+        out = np.empty(shape, dtype)
+        _check(self.ctx.lib.fk_buf_download(self.ctx.handle, self.handle, offset, out.ctypes.data, out.nbytes), self.ctx)
+        return out
+
+    @property
+    def device_ptr(self):
+        return self.ctx.lib.fk_buf_device_ptr(self.handle)
+
+    def free(self):
+        if self.owned and self.handle and self.ctx.handle:
+            self.ctx.lib.fk_buf_free(self.ctx.handle, self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# ------------------------------------------------------------------ mesh / BVH
+class Mesh:
+    """Host indexed mesh (fk_mesh, Src/mesh.h:35-63)."""
+
+    def __init__(self, arrays=None, handle=None):
+        self.lib = L.load()
+        if handle is not None:
+            self.handle = handle
+            return
+        a = arrays
+        self._keep = [a.positions, a.texcoords, a.normals, a.vertices, a.triangles, a.tangents, a.bitangents]
+        d = L.MeshDesc(len(a.positions), _f32(a.positions), len(a.texcoords), _f32(a.texcoords), len(a.normals),
+                       _f32(a.normals), len(a.vertices), _u32(a.vertices), a.triangle_count, _u32(a.triangles),
+                       _f32(a.tangents) if a.tangents is not None else None,
+                       _f32(a.bitangents) if a.bitangents is not None else None)
+        h = L.c_vp()
+        _check(self.lib.fk_mesh_create(ctypes.byref(d), ctypes.byref(h)), None, "fk_mesh_create: invalid mesh")
+        self.handle = h.value
+        self._keep = None
+
+    def __del__(self):
+        try:
+            if self.handle:
+                self.lib.fk_mesh_free(self.handle)
+        except Exception:
+            pass
+
+    def copy(self):
+        h = L.c_vp()
+        _check(self.lib.fk_mesh_copy(self.handle, ctypes.byref(h)))
+        return Mesh(handle=h.value)
+
+    def compute_face_normals(self):
+        _check(self.lib.fk_mesh_compute_face_normals(self.handle))
+
+    def compute_vertex_normals(self):
+        _check(self.lib.fk_mesh_compute_vertex_normals(self.handle))
+
+    def compute_vertex_normals_aggressive(self):
+        _check(self.lib.fk_mesh_compute_vertex_normals_welded(self.handle))
+
+    def compute_tangent_space(self):
+        _check(self.lib.fk_mesh_compute_tangent_space(self.handle))
+
+    def arrays(self):
+        d = L.MeshDesc()
+        _check(self.lib.fk_mesh_describe(self.handle, ctypes.byref(d)))
+
+        def grab(p, n, w, dt):
+            if n == 0 or not p:
+                return np.zeros((0, w), dt)
+            return np.ctypeslib.as_array(p, shape=(n * w,)).reshape(n, w).astype(dt, copy=True)
+
+        tan = grab(d.tangents, d.vertex_count, 3, np.float32) if d.tangents else None
+        bit = grab(d.bitangents, d.vertex_count, 3, np.float32) if d.bitangents else None
+        return MeshArrays(grab(d.positions, d.position_count, 3, np.float32),
+                          grab(d.texcoords, d.texcoord_count, 2, np.float32),
+                          grab(d.normals, d.normal_count, 3, np.float32),
+                          grab(d.vertices, d.vertex_count, 3, np.uint32),
+                          grab(d.triangles, d.triangle_count, 3, np.uint32), tan, bit)
+
+
+class BVH:
+    """Host BVH (fk_bvh): BVH::createBinary (Src/bvh.cpp:283-314)."""
+
+    def __init__(self, handle):
+        self.lib = L.load()
+        self.handle = handle
+
+    @classmethod
+    def create_binary(cls, mesh, max_triangle_count=8, max_tree_depth=8192):
+        h = L.c_vp()
+        _check(L.load().fk_bvh_build(mesh.handle, max_triangle_count, max_tree_depth, ctypes.byref(h)))
+        return cls(h.value)
+
+    def flatten(self, mesh):
+        """fillMeshData (Src/meshmapping.cpp:62-125): (nodes, positions4, normals4)."""
+        nn, nc = L.c_u32(), L.c_u32()
+        _check(self.lib.fk_bvh_flatten_sizes(self.handle, ctypes.byref(nn), ctypes.byref(nc)))
+        nodes = np.zeros(nn.value, NODE_DTYPE)
+        pos4 = np.zeros((nc.value, 4), np.float32)
+        nrm4 = np.zeros((nc.value, 4), np.float32)
+        _check(self.lib.fk_bvh_flatten(self.handle, mesh.handle, nodes.ctypes.data, _f32(pos4), _f32(nrm4)))
+        return nodes, pos4, nrm4
+
+    def __del__(self):
+        try:
+            if self.handle:
+                self.lib.fk_bvh_free(self.handle)
+        except Exception:
+            pass
+
+
+class Scene:
+    """High-poly mesh + BVH resident on the device (fk_scene)."""
+
+    def __init__(self, ctx, nodes, pos4, nrm4):
+        self.ctx = ctx
+        nodes = np.ascontiguousarray(nodes)
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        nrm4 = np.ascontiguousarray(nrm4, np.float32)
+        h = L.c_vp()
+        _check(ctx.lib.fk_scene_upload(ctx.handle, nodes.ctypes.data, len(nodes), _f32(pos4), _f32(nrm4), len(pos4),
+                                       ctypes.byref(h)), ctx, "fk_scene_upload")
+        self.handle = h.value
+        self.owned = True
+
+    @classmethod
+    def borrowed(cls, ctx, handle):
+        s = cls.__new__(cls)
+        s.ctx, s.handle, s.owned = ctx, handle, False
+        return s
+
+    def info(self):
+        i = L.SceneInfo()
+        _check(self.ctx.lib.fk_scene_get_info(self.handle, ctypes.byref(i)))
+        return {k: getattr(i, k) for k, _ in L.SceneInfo._fields_}
+
+    def free(self):
+        if self.owned and self.handle and self.ctx.handle:
+            self.ctx.lib.fk_scene_free(self.ctx.handle, self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class TexelMap:
+    """Compressed texel map on the device: MapUV::from* + CompressedMapUV."""
+
+    def __init__(self, ctx, handle):
+        self.ctx = ctx
+        self.handle = handle
+        w, h, c = L.c_u32(), L.c_u32(), L.c_u32()
+        _check(ctx.lib.fk_texel_map_info(handle, ctypes.byref(w), ctypes.byref(h), ctypes.byref(c)))
+        self.width, self.height, self.count = w.value, h.value, c.value
+
+    @classmethod
+    def rasterize(cls, ctx, mesh, width, height, mode=MAP_SMOOTH, dirs=None, edge=0.05):
+        h = L.c_vp()
+        _check(ctx.lib.fk_raster_uv(ctx.handle, mesh.handle, dirs.handle if dirs is not None else None, width, height,
+                                    mode, edge, ctypes.byref(h)), ctx, "fk_raster_uv")
+        return cls(ctx, h.value)
+
+    @classmethod
+    def from_mesh(cls, ctx, mesh, width, height):
+        return cls.rasterize(ctx, mesh, width, height, MAP_LOWPOLY_NORMALS)
+
+    @classmethod
+    def from_meshes(cls, ctx, mesh, mesh_dirs, width, height):
+        return cls.rasterize(ctx, mesh, width, height, MAP_SMOOTH, mesh_dirs)
+
+    @classmethod
+    def from_meshes_hybrid(cls, ctx, mesh, mesh_dirs, width, height, edge):
+        return cls.rasterize(ctx, mesh, width, height, MAP_HYBRID, mesh_dirs, edge)
+
+    @classmethod
+    def from_host(cls, ctx, width, height, pix8, pixt12, indices):
+        pix8 = np.ascontiguousarray(pix8, np.float32)
+        pixt12 = np.ascontiguousarray(pixt12, np.float32)
+        indices = np.ascontiguousarray(indices, np.uint32)
+        h = L.c_vp()
+        _check(ctx.lib.fk_texel_map_from_host(ctx.handle, width, height, len(indices), _f32(pix8), _f32(pixt12),
+                                              _u32(indices), ctypes.byref(h)), ctx, "fk_texel_map_from_host")
+        return cls(ctx, h.value)
+
+    def download(self):
+        n = self.count
+        pix = np.zeros((n, 8), np.float32)
+        pixt = np.zeros((n, 12), np.float32)
+        idx = np.zeros(n, np.uint32)
+        _check(self.ctx.lib.fk_texel_map_download(self.ctx.handle, self.handle, _f32(pix), _f32(pixt), _u32(idx)), self.ctx)
+        return {"positions": pix[:, 0:3].copy(), "directions": pix[:, 4:7].copy(), "normals": pixt[:, 0:3].copy(),
+                "tangents": pixt[:, 4:7].copy(), "bitangents": pixt[:, 8:11].copy(), "indices": idx}
+
+    def free(self):
+        if self.handle and self.ctx.handle:
+            self.ctx.lib.fk_texel_map_free(self.ctx.handle, self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def samples_cosine(spp, perms=PERMS, seed=0):
+    """computeSamplesImportanceCosDir (Src/math.h:363-382), seeded."""
+    out = np.zeros((perms * spp, 4), np.float32)
+    _check(L.load().fk_samples_cosine(spp, perms, seed, _f32(out)))
+    return out
+
+
+# ------------------------------------------------------------------ kernels
+def meshmap(ctx, scene, tmap, cull_backfaces, coords, tidx, offset=0, count=None):
+    count = tmap.count - offset if count is None else count
+    _check(ctx.lib.fk_meshmap(ctx.handle, scene.handle, tmap.handle, int(cull_backfaces), offset, count, coords.handle,
+                              tidx.handle), ctx, "fk_meshmap")
+
+
+def hemisphere(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, out0, out1=None, hits0=None, hits1=None,
+               offset=0, count=0, perms=PERMS, traverse=TRAVERSE_AUTO):
+    p = L.SampleParams(spp, perms, min_d, max_d)
+    hv = lambda b: b.handle if b is not None else None
+    _check(ctx.lib.fk_hemisphere(ctx.handle, scene.handle, coords.handle, tidx.handle, kind, ctypes.byref(p),
+                                 samples.handle, offset, count, traverse, out0.handle, hv(out1), hv(hits0), hv(hits1)),
+           ctx, "fk_hemisphere")
+
+
+def gather(ctx, scene, kind, coords, tidx, out, offset=0, count=0):
+    _check(ctx.lib.fk_gather(ctx.handle, scene.handle, kind, coords.handle, tidx.handle, offset, count, out.handle),
+           ctx, "fk_gather")
+
+
+def tangent_space(ctx, tmap, io3, offset=0, count=None):
+    count = tmap.count - offset if count is None else count
+    _check(ctx.lib.fk_tangent_space(ctx.handle, tmap.handle, offset, count, io3.handle), ctx, "fk_tangent_space")
+
+
+# ------------------------------------------------------------------ solvers
+class MeshMapping:
+    """MeshMapping (Src/meshmapping.h:42-75)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = L.c_vp()
+        _check(ctx.lib.fk_meshmapping_create(ctx.handle, ctypes.byref(h)), ctx)
+        self.handle = h.value
+
+    def init(self, tmap, mesh, bvh, cull_backfaces=True):
+        _check(self.ctx.lib.fk_meshmapping_init(self.handle, tmap.handle, mesh.handle, bvh.handle, int(cull_backfaces)),
+               self.ctx, "MeshMapping.init")
+        self.tmap = tmap
+
+    def init_scene(self, tmap, scene, cull_backfaces=True):
+        _check(self.ctx.lib.fk_meshmapping_init_scene(self.handle, tmap.handle, scene.handle, int(cull_backfaces)),
+               self.ctx, "MeshMapping.init")
+        self.tmap = tmap
+
+    def set_work_per_step(self, texels):
+        _check(self.ctx.lib.fk_meshmapping_set_work_per_step(self.handle, texels))
+
+    def run_step(self):
+        done = L.c_int()
+        _check(self.ctx.lib.fk_meshmapping_run_step(self.handle, ctypes.byref(done)), self.ctx, "MeshMapping.runStep")
+        return bool(done.value)
+
+    def run(self):
+        while not self.run_step():
+            pass
+
+    def progress(self):
+        return float(self.ctx.lib.fk_meshmapping_progress(self.handle))
+
+    def results(self):
+        n = (self.tmap.count + 63) // 64 * 64 or 64
+        coords = np.zeros((n, 4), np.float32)
+        tidx = np.zeros(n, np.uint32)
+        _check(self.ctx.lib.fk_meshmapping_results(self.handle, _f32(coords), _u32(tidx)), self.ctx)
+        return coords, tidx
+
+    @property
+    def coords(self):
+        return Buffer.borrowed(self.ctx, self.ctx.lib.fk_meshmapping_coords(self.handle))
+
+    @property
+    def coords_tidx(self):
+        return Buffer.borrowed(self.ctx, self.ctx.lib.fk_meshmapping_tidx(self.handle))
+
+    @property
+    def scene(self):
+        return Scene.borrowed(self.ctx, self.ctx.lib.fk_meshmapping_scene(self.handle))
+
+    def __del__(self):
+        try:
+            if self.handle and self.ctx.handle:
+                self.ctx.lib.fk_meshmapping_free(self.handle)
+        except Exception:
+            pass
+
+
+class _Solver:
+    KIND = None
+    WIDTH = 1
+
+    def __init__(self, ctx, sample_count=0, min_distance=0.0, max_distance=0.0, tangent_space=False,
+                 normalize_output=False, seed=0, traverse=TRAVERSE_AUTO):
+        self.ctx = ctx
+        p = L.SolverParams(self.KIND, sample_count, min_distance, max_distance, int(tangent_space),
+                           int(normalize_output), seed, traverse)
+        h = L.c_vp()
+        _check(ctx.lib.fk_solver_create(ctx.handle, ctypes.byref(p), ctypes.byref(h)), ctx, "solver create")
+        self.handle = h.value
+
+    def init(self, tmap, mesh_mapping):
+        _check(self.ctx.lib.fk_solver_init(self.handle, tmap.handle, mesh_mapping.handle), self.ctx, "solver init")
+        self.tmap = tmap
+
+    def set_work_per_step(self, texels):
+        _check(self.ctx.lib.fk_solver_set_work_per_step(self.handle, texels))
+
+    def run_step(self):
+        done = L.c_int()
+        _check(self.ctx.lib.fk_solver_run_step(self.handle, ctypes.byref(done)), self.ctx, "solver runStep")
+        return bool(done.value)
+
+    def run(self):
+        while not self.run_step():
+            pass
+
+    def progress(self):
+        return float(self.ctx.lib.fk_solver_progress(self.handle))
+
+    def get_results(self):
+        n = int(self.ctx.lib.fk_solver_result_count(self.handle))
+        out = np.zeros(n, np.float32)
+        _check(self.ctx.lib.fk_solver_results(self.handle, _f32(out), n), self.ctx, "getResults")
+        return out.reshape(-1, 3) if self.WIDTH == 3 else out
+
+    def hits(self):
+        n = int(self.ctx.lib.fk_solver_result_count(self.handle)) // self.WIDTH
+        out = np.zeros(n, np.uint32)
+        _check(self.ctx.lib.fk_solver_hits(self.handle, _u32(out), n), self.ctx, "hits")
+        return out
+
+    @property
+    def result_buffer(self):
+        return Buffer.borrowed(self.ctx, self.ctx.lib.fk_solver_result_buffer(self.handle))
+
+    def __del__(self):
+        try:
+            if self.handle and self.ctx.handle:
+                self.ctx.lib.fk_solver_free(self.handle)
+        except Exception:
+            pass
+
+
+class HeightSolver(_Solver):
+    KIND = SOLVER_HEIGHT
+
+    def __init__(self, ctx, normalize_output=True, max_distance=0.0):
+        super().__init__(ctx, max_distance=max_distance, normalize_output=normalize_output)
+
+
+class PositionSolver(_Solver):
+    KIND = SOLVER_POSITION
+    WIDTH = 3
+
+    def __init__(self, ctx):
+        super().__init__(ctx)
+
+
+class NormalsSolver(_Solver):
+    KIND = SOLVER_NORMALS
+    WIDTH = 3
+
+    def __init__(self, ctx, tangent_space=True):
+        super().__init__(ctx, tangent_space=tangent_space)
+
+
+class AmbientOcclusionSolver(_Solver):
+    KIND = SOLVER_AO
+
+
+class BentNormalsSolver(_Solver):
+    KIND = SOLVER_BENT_NORMALS
+    WIDTH = 3
+
+
+class ThicknessSolver(_Solver):
+    KIND = SOLVER_THICKNESS
+
+
+# ------------------------------------------------------------------ runner
+def fp32_peak(ctx):
+    """Measured FP32 add/mul/min instruction throughput (ops/s) of the device."""
+    v = ctypes.c_double()
+    _check(ctx.lib.fk_diag_fp32_peak(ctx.handle, ctypes.byref(v)), ctx, "fk_diag_fp32_peak")
+    return v.value
+
+
+def traversal_counts(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, offset=0, count=0, perms=PERMS,
+                     traverse=TRAVERSE_AUTO):
+    """Box and triangle tests the GPU traversal executes for these rays."""
+    p = L.SampleParams(spp, perms, min_d, max_d)
+    out = (L.c_u64 * 2)()
+    _check(ctx.lib.fk_diag_traversal_counts(ctx.handle, scene.handle, coords.handle, tidx.handle, kind, ctypes.byref(p),
+                                            samples.handle, offset, count, traverse, out), ctx, "traversal counts")
+    return int(out[0]), int(out[1])
+
+
+def _sampler(cfg):
+    if not cfg:
+        return L.BakeSampler(0, 0, 0.0, 0.0, 0, 0)
+    return L.BakeSampler(1, cfg["sample_count"], cfg["min_distance"], cfg["max_distance"], cfg.get("seed", 0),
+                         int(cfg.get("tangent_space", False)))
+
+
+def bake(ctx, nodes, pos4, nrm4, width, height, pix8, pixt12, indices, outputs, cull_backfaces=True,
+         height_map=False, position_map=False, normals_map=False, normals_tangent_space=True, ao=None,
+         bent_normals=None, thickness=None, traverse=TRAVERSE_AUTO):
+    """fk_bake: one call from host arrays to host results.  `outputs` maps
+    'coords4', 'tidx', 'height', 'position3', 'normals3', 'ao',
+    'bent_normals3', 'thickness' to preallocated host arrays (pinned memory
+    gives the fastest copies).  ao / bent_normals / thickness: dicts with
+    sample_count, min_distance, max_distance, seed (and tangent_space)."""
+    n = len(indices)
+    d = L.BakeDesc(nodes.ctypes.data, len(nodes), _f32(pos4), _f32(nrm4), len(pos4), width, height, n, _f32(pix8),
+                   _f32(pixt12), _u32(indices), int(cull_backfaces), int(height_map), int(position_map),
+                   int(normals_map), int(normals_tangent_space), _sampler(ao), _sampler(bent_normals),
+                   _sampler(thickness), traverse)
+    o = L.BakeOut()
+    for name, ctype in (("coords4", L.f32p), ("tidx", L.u32p), ("height", L.f32p), ("position3", L.f32p),
+                        ("normals3", L.f32p), ("ao", L.f32p), ("bent_normals3", L.f32p), ("thickness", L.f32p)):
+        a = outputs.get(name)
+        if a is not None:
+            setattr(o, name, a.ctypes.data_as(ctype))
+    _check(ctx.lib.fk_bake(ctx.handle, ctypes.byref(d), ctypes.byref(o)), ctx, "fk_bake")

@@ -1,0 +1,330 @@
+// BVH build and flatten on the host: BVH::createBinary (Src/bvh.cpp:128-314)
+// and fillMeshData (Src/meshmapping.cpp:62-125).
+//
+// The tree is the reference's, node for node: 16 centroid buckets per axis,
+// the reference's cost formula, the split at a bucket boundary, an order-
+// preserving partition, leaves of <= max_tris triangles or at max_depth, boxes
+// kept as (center, half size) and rebuilt from the children after recursion.
+// The top levels are built by parallel tasks; every node's inputs (its
+// triangle list in original order) are the same as in the sequential build, so
+// the result is identical.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <thread>
+
+#include "fk_internal.h"
+
+namespace {
+
+struct Box {
+  float lo[3], hi[3];
+};
+inline Box empty_box() {
+  Box b;
+  for (int a = 0; a < 3; ++a) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; }
+  return b;
+}
+// addPoint (Src/bvh.cpp:31-35): min(p, acc), argument order kept because a
+// tie between +0 and -0 resolves by position.
+inline void add_point(Box& b, const float* p) {
+  for (int a = 0; a < 3; ++a) { b.lo[a] = std::fmin(p[a], b.lo[a]); b.hi[a] = std::fmax(p[a], b.hi[a]); }
+}
+// min(acc, triangle bounds) of the partition loop (Src/bvh.cpp:240-247).
+inline void grow_acc(Box& b, const float* lo, const float* hi) {
+  for (int a = 0; a < 3; ++a) { b.lo[a] = std::fmin(b.lo[a], lo[a]); b.hi[a] = std::fmax(b.hi[a], hi[a]); }
+}
+inline Box join(const Box& a, const Box& b) {
+  Box r = a;
+  for (int k = 0; k < 3; ++k) { r.lo[k] = std::fmin(b.lo[k], r.lo[k]); r.hi[k] = std::fmax(b.hi[k], r.hi[k]); }
+  return r;
+}
+// Src/bvh.cpp:63-68 (x*y appears twice in the reference's area term).
+inline float cost_of(const Box& b, int n) {
+  float ex = b.hi[0] - b.lo[0], ey = b.hi[1] - b.lo[1], ez = b.hi[2] - b.lo[2];
+  return float(n) * (2.0f * (ex * ey + ex * ez + ex * ey));
+}
+
+// Per-triangle values the build reads repeatedly.
+struct Pre {
+  float p[3][3];  // corners
+  float cdiv[3];  // (p0 + p1 + p2) / 3.0f       (bucketing, Src/bvh.cpp:139)
+  float cmul[3];  // (p0 + p1 + p2) * (1.0f/3.0f) (partition, Src/bvh.cpp:227)
+};
+
+using Node = fk_bvh_tree_node;
+
+struct Build {
+  const std::vector<Pre>& pre;
+  std::vector<uint32_t>& order;
+  size_t max_tris, max_depth;
+  int par_depth;
+
+  // Returns (axis, split value) of Src/bvh.cpp:128-203.
+  void choose(uint32_t b, uint32_t e, int* axis, float* value) const {
+    Box cb = empty_box();
+    for (uint32_t i = b; i < e; ++i) add_point(cb, pre[order[i]].cdiv);
+    uint32_t cnt[3][16] = {};
+    Box bb[3][16];
+    for (int a = 0; a < 3; ++a)
+      for (int k = 0; k < 16; ++k) bb[a][k] = empty_box();
+    float ext[3];
+    for (int a = 0; a < 3; ++a) ext[a] = cb.hi[a] - cb.lo[a];
+    for (uint32_t i = b; i < e; ++i) {
+      const Pre& p = pre[order[i]];
+      for (int a = 0; a < 3; ++a) {
+        float r = ((p.cdiv[a] - cb.lo[a]) / ext[a]) * 15.99f;
+        size_t k = std::isnan(r) ? 0 : (size_t)r;
+        cnt[a][k]++;
+        add_point(bb[a][k], p.p[0]);
+        add_point(bb[a][k], p.p[1]);
+        add_point(bb[a][k], p.p[2]);
+      }
+    }
+    float best_cost[3];
+    int best_idx[3];
+    const int n = (int)(e - b);
+    for (int a = 0; a < 3; ++a) {
+      Box right[15];
+      right[14] = bb[a][15];
+      for (int k = 13; k >= 0; --k) right[k] = join(right[k + 1], bb[a][k + 1]);
+      Box left = empty_box();
+      int nl = 0, nr = n;
+      float best = FLT_MAX;
+      int bi = 0;
+      // The all-left step (k = 15) has an empty right side: its cost is NaN
+      // and it never wins (the reference reads past its table there).
+      for (int k = 0; k < 15; ++k) {
+        nl += (int)cnt[a][k];
+        nr -= (int)cnt[a][k];
+        left = join(left, bb[a][k]);
+        float c = cost_of(left, nl) + cost_of(right[k], nr);
+        if (c < best) { best = c; bi = k; }
+      }
+      best_cost[a] = best;
+      best_idx[a] = bi;
+    }
+    int ax;
+    if (best_cost[0] <= best_cost[1] && best_cost[0] <= best_cost[2]) ax = 0;
+    else if (best_cost[1] <= best_cost[0] && best_cost[1] <= best_cost[2]) ax = 1;
+    else ax = 2;
+    *axis = ax;
+    *value = cb.lo[ax] + (cb.hi[ax] - cb.lo[ax]) / 16.0f * float(best_idx[ax] + 1);
+  }
+
+  static void set_box(Node& n, const Box& b) {
+    for (int a = 0; a < 3; ++a) {
+      n.c[a] = (b.lo[a] + b.hi[a]) * 0.5f;
+      n.s[a] = (b.hi[a] - b.lo[a]) * 0.5f;
+    }
+  }
+
+  // Builds the subtree over order[b, e) whose node `ni` already holds its
+  // box; nodes are appended to `out`.
+  void divide(std::vector<Node>& out, int32_t ni, uint32_t b, uint32_t e, size_t depth) {
+    out[ni].first = b;
+    out[ni].count = e - b;
+    if ((size_t)(e - b) <= max_tris || depth >= max_depth) {
+      out[ni].subtree = e - b;
+      return;
+    }
+    int axis;
+    float split;
+    choose(b, e, &axis, &split);
+    // Order-preserving partition (triangles keep their relative order on each side).
+    std::vector<uint32_t> right;
+    Box lb = empty_box(), rb = empty_box();
+    uint32_t w = b;
+    for (uint32_t i = b; i < e; ++i) {
+      uint32_t t = order[i];
+      const Pre& p = pre[t];
+      float lo[3], hi[3];
+      for (int a = 0; a < 3; ++a) {
+        lo[a] = std::fmin(p.p[0][a], std::fmin(p.p[1][a], p.p[2][a]));
+        hi[a] = std::fmax(p.p[0][a], std::fmax(p.p[1][a], p.p[2][a]));
+      }
+      if (p.cmul[axis] <= split) {
+        order[w++] = t;
+        grow_acc(lb, lo, hi);
+      } else {
+        right.push_back(t);
+        grow_acc(rb, lo, hi);
+      }
+    }
+    if (w == b || w == e) {  // Src/bvh.cpp:248-256: cannot split, stays a leaf
+      std::copy(right.begin(), right.end(), order.begin() + w);
+      out[ni].subtree = e - b;
+      return;
+    }
+    std::copy(right.begin(), right.end(), order.begin() + w);
+    std::vector<uint32_t>().swap(right);
+    out[ni].count = 0;
+    Node L, R;
+    set_box(L, lb);
+    set_box(R, rb);
+    int32_t li, ri;
+    if ((int)depth < par_depth && (e - b) > 65536) {
+      std::vector<Node> lv(1, L), rv(1, R);
+      std::thread th([&] { divide(lv, 0, b, w, depth + 1); });
+      divide(rv, 0, w, e, depth + 1);
+      th.join();
+      li = (int32_t)out.size();
+      append(out, lv);
+      ri = (int32_t)out.size();
+      append(out, rv);
+    } else {
+      li = (int32_t)out.size();
+      out.push_back(L);
+      ri = (int32_t)out.size();
+      out.push_back(R);
+      divide(out, li, b, w, depth + 1);
+      divide(out, ri, w, e, depth + 1);
+    }
+    out[ni].kid[0] = li;
+    out[ni].kid[1] = ri;
+    const Node& A = out[li];
+    const Node& B = out[ri];
+    Box u;
+    for (int a = 0; a < 3; ++a) {
+      u.lo[a] = std::fmin(A.c[a] - A.s[a], B.c[a] - B.s[a]);
+      u.hi[a] = std::fmax(A.c[a] + A.s[a], B.c[a] + B.s[a]);
+      out[ni].c[a] = (u.hi[a] + u.lo[a]) * 0.5f;
+      out[ni].s[a] = (u.hi[a] - u.lo[a]) * 0.5f;
+    }
+    out[ni].subtree = A.subtree + B.subtree;
+  }
+
+  static void append(std::vector<Node>& out, const std::vector<Node>& sub) {
+    int32_t off = (int32_t)out.size();
+    for (Node n : sub) {
+      if (n.kid[0] >= 0) { n.kid[0] += off; n.kid[1] += off; }
+      out.push_back(n);
+    }
+  }
+};
+
+// Walks the fillMeshData recursion: emits nodes / corners through callbacks.
+struct Flatten {
+  const fk_bvh& t;
+  const fk_mesh* mesh;
+  fk_bvh_node* nodes;
+  float* pos4;
+  float* nrm4;
+  uint32_t n_nodes = 0, n_corners = 0;
+
+  void visit(int32_t ni) {
+    const Node& n = t.nodes[ni];
+    bool kids = n.kid[0] >= 0;
+    if (!kids && n.count == 0) return;
+    if (kids) {
+      const Node& a = t.nodes[n.kid[0]];
+      const Node& b = t.nodes[n.kid[1]];
+      if (a.subtree > 0 && b.subtree == 0) { visit(n.kid[0]); return; }
+      if (b.subtree > 0 && a.subtree == 0) { visit(n.kid[1]); return; }
+    }
+    uint32_t me = n_nodes++;
+    uint32_t start = n_corners;
+    if (!kids) {
+      for (uint32_t i = 0; i < n.count; ++i) {
+        uint32_t f = t.order[n.first + i];
+        for (int k = 0; k < 3; ++k) {
+          if (pos4) {
+            const uint32_t* v = &mesh->vertices[3 * (size_t)mesh->triangles[3 * (size_t)f + k]];
+            const float* p = &mesh->positions[3 * (size_t)v[0]];
+            const float* q = &mesh->normals[3 * (size_t)v[2]];
+            float* dp = pos4 + 4 * (size_t)n_corners;
+            float* dn = nrm4 + 4 * (size_t)n_corners;
+            dp[0] = p[0]; dp[1] = p[1]; dp[2] = p[2]; dp[3] = 0.0f;
+            dn[0] = q[0]; dn[1] = q[1]; dn[2] = q[2]; dn[3] = 0.0f;
+          }
+          ++n_corners;
+        }
+      }
+    }
+    if (nodes) {
+      fk_bvh_node& d = nodes[me];
+      for (int a = 0; a < 3; ++a) {
+        d.aabb_min[a] = n.c[a] - n.s[a];
+        d.aabb_max[a] = n.c[a] + n.s[a];
+      }
+      d.start = start;
+      d.end = n_corners;
+    }
+    if (kids) {
+      visit(n.kid[0]);
+      visit(n.kid[1]);
+    }
+    if (nodes) nodes[me].jump = n_nodes;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+int fk_bvh_build(const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, fk_bvh** out) {
+  if (!mesh || !out || max_tris == 0) return FK_ERR_INVALID;
+  const uint32_t nf = mesh->triangle_count();
+  std::vector<Pre> pre(nf);
+  for (uint32_t f = 0; f < nf; ++f) {
+    const float* p[3];
+    for (int k = 0; k < 3; ++k) p[k] = &mesh->positions[3 * (size_t)mesh->vertices[3 * (size_t)mesh->triangles[3 * (size_t)f + k]]];
+    Pre& q = pre[f];
+    for (int a = 0; a < 3; ++a) {
+      float s = p[0][a] + p[1][a] + p[2][a];
+      q.cdiv[a] = s / 3.0f;
+      q.cmul[a] = s * (1.0f / 3.0f);
+      for (int k = 0; k < 3; ++k) q.p[k][a] = p[k][a];
+    }
+  }
+  fk_bvh* t = new (std::nothrow) fk_bvh();
+  if (!t) return FK_ERR_NOMEM;
+  t->triangle_count = nf;
+  t->order.resize(nf);
+  for (uint32_t i = 0; i < nf; ++i) t->order[i] = i;
+  // Root box over all positions (Src/bvh.cpp:287-297), including unreferenced ones.
+  Box rb = empty_box();
+  for (uint32_t i = 0; i < mesh->position_count(); ++i) {
+    const float* p = &mesh->positions[3 * (size_t)i];
+    grow_acc(rb, p, p);
+  }
+  Node root;
+  Build::set_box(root, rb);
+  t->nodes.reserve(nf / 2 + 16);
+  t->nodes.push_back(root);
+  unsigned hw = std::thread::hardware_concurrency();
+  int par = 0;
+  while ((1u << par) < (hw ? hw : 1) && par < 6) ++par;
+  Build b{pre, t->order, max_tris, max_depth, par};
+  b.divide(t->nodes, 0, 0, nf, 0);
+  *out = t;
+  return FK_OK;
+}
+
+int fk_bvh_free(fk_bvh* bvh) {
+  delete bvh;
+  return FK_OK;
+}
+
+int fk_bvh_flatten_sizes(const fk_bvh* bvh, uint32_t* node_count, uint32_t* corner_count) {
+  if (!bvh || !node_count || !corner_count) return FK_ERR_INVALID;
+  Flatten f{*bvh, nullptr, nullptr, nullptr, nullptr};
+  f.visit(0);
+  *node_count = f.n_nodes;
+  *corner_count = f.n_corners;
+  return FK_OK;
+}
+
+int fk_bvh_flatten(const fk_bvh* bvh, const fk_mesh* mesh, fk_bvh_node* nodes, float* pos4, float* nrm4) {
+  if (!bvh || !mesh || !nodes || !pos4 || !nrm4) return FK_ERR_INVALID;
+  if (mesh->triangle_count() != bvh->triangle_count) return FK_ERR_INVALID;
+  uint32_t nn = (uint32_t)(mesh->normals.size() / 3);
+  for (uint32_t v = 0; v < mesh->vertex_count(); ++v)
+    if (mesh->vertices[3 * (size_t)v + 2] >= nn) return FK_ERR_INVALID;
+  Flatten f{*bvh, mesh, nodes, pos4, nrm4};
+  f.visit(0);
+  return FK_OK;
+}
+
+}  // extern "C"

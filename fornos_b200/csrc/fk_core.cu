@@ -1,0 +1,349 @@
+// Context, device buffers, device scene and texel-map handles of the C ABI
+// (include/fornos_gpu.h).  Replaces the GL buffer layer: ComputeBuffer<T>
+// (Src/compute.h:37-87) and the uploads of MeshMapping::init
+// (Src/meshmapping.cpp:128-184).
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "fk_internal.h"
+
+int fk_fail(fk_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int fk_cuda_fail(fk_ctx* ctx, cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+  return fk_fail(ctx, e == cudaErrorMemoryAllocation ? FK_ERR_NOMEM : FK_ERR_CUDA, m);
+}
+
+int fk_after_launch(fk_ctx* ctx, const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fk_cuda_fail(ctx, e, what);
+  ctx->launches++;
+  return FK_OK;
+}
+
+int fk_dev_alloc(fk_ctx* ctx, void** p, size_t bytes) {
+  *p = nullptr;
+  if (bytes == 0) return FK_OK;
+  FK_CUDA(ctx, cudaMalloc(p, bytes));
+  return FK_OK;
+}
+
+void fk_dev_free(void* p) {
+  if (p) cudaFree(p);
+}
+
+uint32_t* fk_take_counter(fk_ctx* ctx) {
+  uint32_t* c = ctx->counters + (ctx->next_counter++ % ctx->counter_slots);
+  cudaMemsetAsync(c, 0, sizeof(uint32_t), ctx->stream);
+  return c;
+}
+
+extern "C" {
+
+int fk_ctx_create(int device, fk_ctx** out) {
+  if (!out) return FK_ERR_INVALID;
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) return FK_ERR_UNSUPPORTED;
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return FK_ERR_CUDA;
+  if (prop.major != 10) return FK_ERR_UNSUPPORTED;  // kernels are built for sm_100a only
+  if (cudaSetDevice(device) != cudaSuccess) return FK_ERR_CUDA;
+  fk_ctx* c = new (std::nothrow) fk_ctx();
+  if (!c) return FK_ERR_NOMEM;
+  c->device = device;
+  c->sm_count = prop.multiProcessorCount;
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete c;
+    return FK_ERR_CUDA;
+  }
+  c->stream = c->own_stream;
+  c->counter_slots = 1024;
+  if (cudaMalloc(&c->counters, c->counter_slots * sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&c->status, sizeof(int)) != cudaSuccess) {
+    cudaFree(c->counters);
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+    return FK_ERR_NOMEM;
+  }
+  cudaMemset(c->counters, 0, c->counter_slots * sizeof(uint32_t));
+  cudaMemset(c->status, 0, sizeof(int));
+  *out = c;
+  return FK_OK;
+}
+
+int fk_ctx_destroy(fk_ctx* ctx) {
+  if (!ctx) return FK_ERR_INVALID;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  for (fk_buf* b : ctx->bufs) { cudaFree(b->ptr); delete b; }
+  for (fk_scene* s : std::set<fk_scene*>(ctx->scenes)) fk_scene_free(ctx, s);
+  for (fk_texel_map* m : std::set<fk_texel_map*>(ctx->maps)) fk_texel_map_free(ctx, m);
+  cudaFree(ctx->counters);
+  cudaFree(ctx->status);
+  cudaStreamDestroy(ctx->own_stream);
+  delete ctx;
+  return FK_OK;
+}
+
+const char* fk_last_error(const fk_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int fk_ctx_set_stream(fk_ctx* ctx, void* s) {
+  if (!ctx) return FK_ERR_INVALID;
+  ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
+  return FK_OK;
+}
+
+void* fk_ctx_stream(const fk_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int fk_sync(fk_ctx* ctx) {
+  if (!ctx) return FK_ERR_INVALID;
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return FK_OK;
+}
+
+uint64_t fk_launch_count(const fk_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+// ------------------------------------------------------------------ buffers
+int fk_buf_alloc(fk_ctx* ctx, size_t bytes, fk_buf** out) {
+  if (!ctx || !out || bytes == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_alloc: zero size or null");
+  fk_buf* b = new (std::nothrow) fk_buf();
+  if (!b) return FK_ERR_NOMEM;
+  cudaError_t e = cudaMalloc(&b->ptr, bytes);
+  if (e != cudaSuccess) {
+    delete b;
+    return fk_cuda_fail(ctx, e, "cudaMalloc");
+  }
+  e = cudaMemsetAsync(b->ptr, 0, bytes, ctx->stream);
+  if (e != cudaSuccess) {
+    cudaFree(b->ptr);
+    delete b;
+    return fk_cuda_fail(ctx, e, "cudaMemsetAsync");
+  }
+  b->ctx = ctx;
+  b->bytes = bytes;
+  ctx->bufs.insert(b);
+  *out = b;
+  return FK_OK;
+}
+
+int fk_buf_upload(fk_ctx* ctx, fk_buf* b, size_t off, const void* src, size_t bytes) {
+  if (!ctx || !b || (!src && bytes) || off > b->bytes || bytes > b->bytes - off)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_upload: range outside the buffer");
+  if (!bytes) return FK_OK;
+  FK_CUDA(ctx, cudaMemcpyAsync((char*)b->ptr + off, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return FK_OK;
+}
+
+int fk_buf_download(fk_ctx* ctx, const fk_buf* b, size_t off, void* dst, size_t bytes) {
+  if (!ctx || !b || (!dst && bytes) || off > b->bytes || bytes > b->bytes - off)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_download: range outside the buffer");
+  if (!bytes) return FK_OK;
+  FK_CUDA(ctx, cudaMemcpyAsync(dst, (const char*)b->ptr + off, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return FK_OK;
+}
+
+int fk_buf_free(fk_ctx* ctx, fk_buf* b) {
+  if (!ctx || !b || !ctx->bufs.count(b)) return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_free: unknown buffer");
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(b->ptr);
+  ctx->bufs.erase(b);
+  delete b;
+  return FK_OK;
+}
+
+size_t fk_buf_size(const fk_buf* b) { return b ? b->bytes : 0; }
+void* fk_buf_device_ptr(const fk_buf* b) { return b ? b->ptr : nullptr; }
+
+// ------------------------------------------------------------------ scene
+int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const float* pos4, const float* nrm4,
+                    uint32_t nc, fk_scene** out) {
+  if (!ctx || !out || !nodes || !pos4 || !nrm4 || nn == 0 || nc == 0 || nc % 3 != 0)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: empty or malformed scene");
+  // Validate the skip-pointer structure so no kernel can walk outside it.
+  std::vector<float4> lo(nn), hi(nn);
+  std::vector<uint32_t> jump(nn);
+  uint32_t leaves = 0;
+  for (uint32_t i = 0; i < nn; ++i) {
+    const fk_bvh_node& n = nodes[i];
+    if (n.start > n.end || n.end > nc || n.start % 3 || n.end % 3 || n.jump <= i || n.jump > nn)
+      return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node " + std::to_string(i) + " is malformed");
+    bool leaf = n.jump == i + 1;
+    if (leaf != (n.end > n.start))
+      return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node " + std::to_string(i) + " mixes children and triangles");
+    leaves += leaf;
+    uint32_t s = n.start, e = n.end;
+    float fs, fe;
+    std::memcpy(&fs, &s, 4);
+    std::memcpy(&fe, &e, 4);
+    lo[i] = make_float4(n.aabb_min[0], n.aabb_min[1], n.aabb_min[2], fs);
+    hi[i] = make_float4(n.aabb_max[0], n.aabb_max[1], n.aabb_max[2], fe);
+    jump[i] = n.jump;
+  }
+  if (nodes[0].jump != nn) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node 0 does not span the array");
+  // Inner node i has children i + 1 and nodes[i + 1].jump; depth and the
+  // ordered (children-in-parent) layout follow from that.
+  std::vector<int32_t> wide_of(nn, -1);
+  uint32_t nw = 0;
+  for (uint32_t i = 0; i < nn; ++i)
+    if (nodes[i].jump != i + 1) {
+      uint32_t r = nodes[i + 1].jump;
+      if (i + 1 >= nn || r >= nodes[i].jump || nodes[r].jump != nodes[i].jump)
+        return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node " + std::to_string(i) + " children inconsistent");
+      wide_of[i] = (int32_t)nw++;
+    }
+  std::vector<float4> wide(4 * (size_t)nw);
+  std::vector<uint32_t> depth(nn, 1);
+  uint32_t maxd = 1;
+  for (uint32_t i = 0; i < nn; ++i) {
+    maxd = depth[i] > maxd ? depth[i] : maxd;
+    if (wide_of[i] < 0) continue;
+    uint32_t c[2] = {i + 1, nodes[i + 1].jump};
+    depth[c[0]] = depth[c[1]] = depth[i] + 1;
+    int32_t ref[2], cnt[2];
+    for (int k = 0; k < 2; ++k) {
+      const fk_bvh_node& n = nodes[c[k]];
+      if (wide_of[c[k]] >= 0) { ref[k] = wide_of[c[k]]; cnt[k] = 0; }
+      else { ref[k] = (int32_t)(n.start / 3); cnt[k] = (int32_t)((n.end - n.start) / 3); }
+    }
+    const fk_bvh_node& L = nodes[c[0]];
+    const fk_bvh_node& R = nodes[c[1]];
+    float4* w = &wide[4 * (size_t)wide_of[i]];
+    w[0] = make_float4(L.aabb_min[0], L.aabb_max[0], L.aabb_min[1], L.aabb_max[1]);
+    w[1] = make_float4(R.aabb_min[0], R.aabb_max[0], R.aabb_min[1], R.aabb_max[1]);
+    w[2] = make_float4(L.aabb_min[2], L.aabb_max[2], R.aabb_min[2], R.aabb_max[2]);
+    float f[4];
+    int32_t ints[4] = {ref[0], ref[1], cnt[0], cnt[1]};
+    std::memcpy(f, ints, 16);
+    w[3] = make_float4(f[0], f[1], f[2], f[3]);
+  }
+  fk_scene* s = new (std::nothrow) fk_scene();
+  if (!s) return FK_ERR_NOMEM;
+  s->ctx = ctx;
+  s->node_count = nn;
+  s->corner_count = nc;
+  s->depth = maxd;
+  s->leaf_count = leaves;
+  s->wide_count = nw;
+  s->root_is_leaf = nodes[0].jump == 1;
+  size_t nb = sizeof(float4) * nn, cb = sizeof(float4) * (size_t)nc;
+  int rc = FK_OK;
+  auto up = [&](void** dst, const void* src, size_t bytes) {
+    if (rc != FK_OK || bytes == 0) return;
+    rc = fk_dev_alloc(ctx, dst, bytes);
+    if (rc == FK_OK) {
+      cudaError_t e = cudaMemcpyAsync(*dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+      if (e != cudaSuccess) rc = fk_cuda_fail(ctx, e, "scene upload");
+    }
+    s->bytes += bytes;
+  };
+  up((void**)&s->node_lo, lo.data(), nb);
+  up((void**)&s->node_hi, hi.data(), nb);
+  up((void**)&s->node_jump, jump.data(), sizeof(uint32_t) * nn);
+  up((void**)&s->pos4, pos4, cb);
+  up((void**)&s->nrm4, nrm4, cb);
+  up((void**)&s->wide, wide.data(), sizeof(float4) * wide.size());
+  if (rc == FK_OK) {
+    rc = fk_dev_alloc(ctx, (void**)&s->tri_rec, 4 * sizeof(float4) * (size_t)(nc / 3));
+    s->bytes += 4 * sizeof(float4) * (size_t)(nc / 3);
+  }
+  if (rc == FK_OK) rc = fk::launch_tri_records(ctx, s);
+  if (rc == FK_OK) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = fk_cuda_fail(ctx, e, "scene upload sync");
+  }
+  if (rc != FK_OK) {
+    ctx->scenes.insert(s);
+    fk_scene_free(ctx, s);
+    return rc;
+  }
+  ctx->scenes.insert(s);
+  *out = s;
+  return FK_OK;
+}
+
+int fk_scene_free(fk_ctx* ctx, fk_scene* s) {
+  if (!ctx || !s || !ctx->scenes.count(s)) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_free: unknown scene");
+  cudaStreamSynchronize(ctx->stream);
+  void* ps[] = {s->node_lo, s->node_hi, s->node_jump, s->pos4, s->nrm4, s->wide, s->tri_rec};
+  for (void* p : ps) fk_dev_free(p);
+  ctx->scenes.erase(s);
+  delete s;
+  return FK_OK;
+}
+
+int fk_scene_get_info(const fk_scene* s, fk_scene_info* o) {
+  if (!s || !o) return FK_ERR_INVALID;
+  o->node_count = s->node_count;
+  o->corner_count = s->corner_count;
+  o->depth = s->depth;
+  o->leaf_count = s->leaf_count;
+  o->device_bytes = s->bytes;
+  return FK_OK;
+}
+
+// ------------------------------------------------------------------ texel map
+int fk_texel_map_from_host(fk_ctx* ctx, uint32_t w, uint32_t h, uint32_t count, const float* pix8,
+                           const float* pixt12, const uint32_t* idx, fk_texel_map** out) {
+  if (!ctx || !out || (count && (!pix8 || !pixt12 || !idx)) || (uint64_t)count > (uint64_t)w * h)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_texel_map_from_host: bad arguments");
+  fk_texel_map* m = new (std::nothrow) fk_texel_map();
+  if (!m) return FK_ERR_NOMEM;
+  m->ctx = ctx;
+  m->width = w;
+  m->height = h;
+  m->count = count;
+  int rc = fk_dev_alloc(ctx, (void**)&m->pix, 32 * (size_t)count);
+  if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&m->pixt, 48 * (size_t)count);
+  if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&m->indices, 4 * (size_t)count);
+  ctx->maps.insert(m);
+  if (rc != FK_OK) {
+    fk_texel_map_free(ctx, m);
+    return rc;
+  }
+  if (count) {
+    FK_CUDA(ctx, cudaMemcpyAsync(m->pix, pix8, 32 * (size_t)count, cudaMemcpyHostToDevice, ctx->stream));
+    FK_CUDA(ctx, cudaMemcpyAsync(m->pixt, pixt12, 48 * (size_t)count, cudaMemcpyHostToDevice, ctx->stream));
+    FK_CUDA(ctx, cudaMemcpyAsync(m->indices, idx, 4 * (size_t)count, cudaMemcpyHostToDevice, ctx->stream));
+    FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
+  *out = m;
+  return FK_OK;
+}
+
+int fk_texel_map_info(const fk_texel_map* m, uint32_t* w, uint32_t* h, uint32_t* count) {
+  if (!m) return FK_ERR_INVALID;
+  if (w) *w = m->width;
+  if (h) *h = m->height;
+  if (count) *count = m->count;
+  return FK_OK;
+}
+
+int fk_texel_map_download(fk_ctx* ctx, const fk_texel_map* m, float* pix8, float* pixt12, uint32_t* idx) {
+  if (!ctx || !m) return fk_fail(ctx, FK_ERR_INVALID, "fk_texel_map_download: null");
+  if (!m->count) return FK_OK;
+  if (pix8) FK_CUDA(ctx, cudaMemcpyAsync(pix8, m->pix, 32 * (size_t)m->count, cudaMemcpyDeviceToHost, ctx->stream));
+  if (pixt12) FK_CUDA(ctx, cudaMemcpyAsync(pixt12, m->pixt, 48 * (size_t)m->count, cudaMemcpyDeviceToHost, ctx->stream));
+  if (idx) FK_CUDA(ctx, cudaMemcpyAsync(idx, m->indices, 4 * (size_t)m->count, cudaMemcpyDeviceToHost, ctx->stream));
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return FK_OK;
+}
+
+int fk_texel_map_free(fk_ctx* ctx, fk_texel_map* m) {
+  if (!ctx || !m || !ctx->maps.count(m)) return fk_fail(ctx, FK_ERR_INVALID, "fk_texel_map_free: unknown map");
+  cudaStreamSynchronize(ctx->stream);
+  fk_dev_free(m->pix);
+  fk_dev_free(m->pixt);
+  fk_dev_free(m->indices);
+  ctx->maps.erase(m);
+  delete m;
+  return FK_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// Device-side arithmetic for the bake kernels.
+//
+// Hit identity must match the reference's shaders bit for bit, so every
+// parity-relevant operation is an explicit IEEE-rounded intrinsic: no FMA
+// contraction (the build also passes --fmad=false), correctly rounded division
+// and square root, fminf / fmaxf (a NaN operand loses), dot products summed
+// left to right, normalize(v) = v * (1 / sqrt(dot(v, v))) (Src/math.h:110-113).
+#pragma once
+#include <cfloat>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace fk {
+
+static constexpr uint32_t kMiss = 0xFFFFFFFFu;
+
+struct f3 {
+  float x, y, z;
+};
+
+__device__ __forceinline__ f3 mk3(float x, float y, float z) { f3 r; r.x = x; r.y = y; r.z = z; return r; }
+__device__ __forceinline__ f3 xyz(float4 v) { return mk3(v.x, v.y, v.z); }
+__device__ __forceinline__ f3 add(f3 a, f3 b) { return mk3(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z)); }
+__device__ __forceinline__ f3 sub(f3 a, f3 b) { return mk3(__fsub_rn(a.x, b.x), __fsub_rn(a.y, b.y), __fsub_rn(a.z, b.z)); }
+__device__ __forceinline__ f3 neg(f3 a) { return mk3(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ f3 scale(f3 a, float k) { return mk3(__fmul_rn(a.x, k), __fmul_rn(a.y, k), __fmul_rn(a.z, k)); }
+__device__ __forceinline__ f3 divv(f3 a, f3 b) { return mk3(__fdiv_rn(a.x, b.x), __fdiv_rn(a.y, b.y), __fdiv_rn(a.z, b.z)); }
+__device__ __forceinline__ float dot(f3 a, f3 b) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+__device__ __forceinline__ f3 cross(f3 a, f3 b) {
+  return mk3(__fsub_rn(__fmul_rn(a.y, b.z), __fmul_rn(a.z, b.y)), __fsub_rn(__fmul_rn(a.z, b.x), __fmul_rn(a.x, b.z)),
+             __fsub_rn(__fmul_rn(a.x, b.y), __fmul_rn(a.y, b.x)));
+}
+__device__ __forceinline__ f3 normalize(f3 v) { return scale(v, __fdiv_rn(1.0f, __fsqrt_rn(dot(v, v)))); }
+__device__ __forceinline__ f3 vmin(f3 a, f3 b) { return mk3(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+__device__ __forceinline__ f3 vmax(f3 a, f3 b) { return mk3(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+// a*w.x + b*w.y + c*w.z, evaluated ((a*wx + b*wy) + c*wz) as the shaders write it
+__device__ __forceinline__ f3 blend3(f3 a, f3 b, f3 c, float wx, float wy, float wz) {
+  return add(add(scale(a, wx), scale(b, wy)), scale(c, wz));
+}
+
+// RayAABB of Shaders/ao_step1.comp:43-52 (same in every shader): entry distance
+// when the slab interval is non-empty and not behind the origin, else FLT_MAX.
+__device__ __forceinline__ float ray_box(f3 o, f3 d, f3 lo, f3 hi) {
+  f3 t1 = divv(sub(lo, o), d);
+  f3 t2 = divv(sub(hi, o), d);
+  f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
+  float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
+  float b = fminf(tx.x, fminf(tx.y, tx.z));
+  return (b >= 0.0f && a <= b) ? a : FLT_MAX;
+}
+
+// Binary64 barycentric of Shaders/meshmapping_nobackfaces.comp:48-62.
+__device__ __forceinline__ f3 bary_f64(f3 p, f3 a, f3 b, f3 c) {
+  double ax = a.x, ay = a.y, az = a.z;
+  double v0x = __dsub_rn((double)b.x, ax), v0y = __dsub_rn((double)b.y, ay), v0z = __dsub_rn((double)b.z, az);
+  double v1x = __dsub_rn((double)c.x, ax), v1y = __dsub_rn((double)c.y, ay), v1z = __dsub_rn((double)c.z, az);
+  double v2x = __dsub_rn((double)p.x, ax), v2y = __dsub_rn((double)p.y, ay), v2z = __dsub_rn((double)p.z, az);
+#define FK_DDOT(ax_, ay_, az_, bx_, by_, bz_) \
+  __dadd_rn(__dadd_rn(__dmul_rn(ax_, bx_), __dmul_rn(ay_, by_)), __dmul_rn(az_, bz_))
+  double d00 = FK_DDOT(v0x, v0y, v0z, v0x, v0y, v0z);
+  double d01 = FK_DDOT(v0x, v0y, v0z, v1x, v1y, v1z);
+  double d11 = FK_DDOT(v1x, v1y, v1z, v1x, v1y, v1z);
+  double d20 = FK_DDOT(v2x, v2y, v2z, v0x, v0y, v0z);
+  double d21 = FK_DDOT(v2x, v2y, v2z, v1x, v1y, v1z);
+#undef FK_DDOT
+  double den = __dsub_rn(__dmul_rn(d00, d11), __dmul_rn(d01, d01));
+  double y = __ddiv_rn(__dsub_rn(__dmul_rn(d11, d20), __dmul_rn(d01, d21)), den);
+  double z = __ddiv_rn(__dsub_rn(__dmul_rn(d00, d21), __dmul_rn(d01, d20)), den);
+  return mk3(__double2float_rn(__dsub_rn(__dsub_rn(1.0, y), z)), __double2float_rn(y), __double2float_rn(z));
+}
+
+}  // namespace fk

@@ -1,0 +1,132 @@
+// Internal host-side structures shared by the translation units of
+// libfornos_b200.so.  Not part of the ABI (include/fornos_gpu.h is).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <mutex>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/fornos_gpu.h"
+
+// ------------------------------------------------------------------ context
+struct fk_ctx {
+  int device = 0;
+  int sm_count = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  uint64_t launches = 0;
+  uint32_t* counters = nullptr;   // device work-queue counters for persistent kernels
+  uint32_t counter_slots = 0;
+  uint32_t next_counter = 0;
+  int* status = nullptr;          // device status word (limits a kernel could not honour)
+  std::set<fk_buf*> bufs;
+  std::set<fk_scene*> scenes;
+  std::set<fk_texel_map*> maps;
+};
+
+struct fk_buf {
+  fk_ctx* ctx = nullptr;
+  void* ptr = nullptr;
+  size_t bytes = 0;
+};
+
+// High-poly mesh + BVH on the device.
+struct fk_scene {
+  fk_ctx* ctx = nullptr;
+  uint32_t node_count = 0, corner_count = 0, depth = 0, leaf_count = 0;
+  // Reference layout, one entry per flattened node (skip-pointer walk):
+  float4* node_lo = nullptr;     // aabbMin.xyz, start (bits)
+  float4* node_hi = nullptr;     // aabbMax.xyz, end (bits)
+  uint32_t* node_jump = nullptr;
+  float4* pos4 = nullptr;        // triangle corners, DFS leaf order
+  float4* nrm4 = nullptr;
+  // Ordered layout: one 64-byte record per inner node holding both children's
+  // boxes (4 x float4), and one 64-byte precomputed record per triangle.
+  float4* wide = nullptr;
+  uint32_t wide_count = 0;
+  float4* tri_rec = nullptr;
+  uint32_t root_is_leaf = 0;
+  size_t bytes = 0;
+};
+
+struct fk_texel_map {
+  fk_ctx* ctx = nullptr;
+  uint32_t width = 0, height = 0, count = 0;
+  float4* pix = nullptr;     // 2 float4 per texel: p, d
+  float4* pixt = nullptr;    // 3 float4 per texel: n, t, b
+  uint32_t* indices = nullptr;
+};
+
+// ------------------------------------------------------------------ helpers
+int fk_fail(fk_ctx* ctx, int code, const std::string& msg);
+int fk_cuda_fail(fk_ctx* ctx, cudaError_t e, const char* what);
+
+#define FK_CUDA(ctx, call)                                   \
+  do {                                                       \
+    cudaError_t fk_e_ = (call);                              \
+    if (fk_e_ != cudaSuccess) return fk_cuda_fail((ctx), fk_e_, #call); \
+  } while (0)
+
+// Checks a launch just issued on ctx->stream and counts it.
+int fk_after_launch(fk_ctx* ctx, const char* what);
+
+// Device memory owned by the library (not visible as fk_buf).
+int fk_dev_alloc(fk_ctx* ctx, void** p, size_t bytes);
+void fk_dev_free(void* p);
+
+// Reserves a zeroed device counter for one persistent-kernel launch.
+uint32_t* fk_take_counter(fk_ctx* ctx);
+
+// Kernel launchers (fk_*.cu).
+namespace fk {
+int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, uint32_t offset, uint32_t count,
+                   float4* coords, uint32_t* tidx);
+struct HemiLaunch {
+  int kind;
+  uint32_t spp, perms;
+  float min_d, max_d;
+  const float4* samples;
+  const float4* coords;
+  const uint32_t* tidx;
+  uint32_t offset, count;
+  int traverse;
+  float* out0;
+  float* out1;
+  uint32_t* hits0;
+  uint32_t* hits1;
+  unsigned long long* tally = nullptr;  // non-null: counting variant
+};
+int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h);
+int launch_gather(fk_ctx* ctx, const fk_scene* s, int kind, const float4* coords, const uint32_t* tidx,
+                  uint32_t offset, uint32_t count, float* out);
+int launch_tangent_space(fk_ctx* ctx, const fk_texel_map* m, uint32_t offset, uint32_t count, float* io3);
+int launch_tri_records(fk_ctx* ctx, fk_scene* s);
+struct RasterTri;  // defined in fk_raster.cu
+}  // namespace fk
+
+// Host mesh (Src/mesh.h:35-63).
+struct fk_mesh {
+  std::vector<float> positions, texcoords, normals, tangents, bitangents;
+  std::vector<uint32_t> vertices, triangles;
+  uint32_t position_count() const { return (uint32_t)(positions.size() / 3); }
+  uint32_t vertex_count() const { return (uint32_t)(vertices.size() / 3); }
+  uint32_t triangle_count() const { return (uint32_t)(triangles.size() / 3); }
+};
+
+// Host BVH tree (Src/bvh.h:32-46).
+struct fk_bvh_tree_node {
+  float c[3], s[3];            // center, half size (Src/math.h:147-154)
+  int32_t kid[2] = {-1, -1};
+  uint32_t first = 0, count = 0;  // triangle range in fk_bvh::order (leaves)
+  uint64_t subtree = 0;
+};
+struct fk_bvh {
+  std::vector<fk_bvh_tree_node> nodes;  // nodes[0] = root
+  std::vector<uint32_t> order;          // triangle ids, leaf ranges contiguous
+  uint32_t triangle_count = 0;
+};

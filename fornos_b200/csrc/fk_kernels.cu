@@ -1,0 +1,582 @@
+// Ray kernels of the bake path, sm_100a:
+//   * per-triangle records            (precomputed terms of the ray/triangle test)
+//   * mesh mapping                    Shaders/meshmapping_nobackfaces.comp, meshmapping.comp
+//   * hemisphere sampling             Shaders/ao_step0/1/2, bentnormals_step1/2, thick_step1/2
+//   * gathers and tangent space       Shaders/heights, positions, normals, tangentspace
+//
+// Every comparison and every float the shaders produce is reproduced with the
+// same IEEE operations in the same order (fk_device.cuh), so hit identity,
+// occluder counts and sums match the reference bit for bit.  Two traversals:
+//   SKIP    the reference's skip-pointer walk over the flattened node array,
+//           in array order (exact by construction);
+//   ORDERED near-first stack traversal over a children-in-parent BVH2 layout
+//           (64-byte records, both child boxes per 128-bit loads), with the
+//           reference's pruning rule (entry distance < min(best, max)).  It
+//           visits the same leaves the reference can improve from, so results
+//           agree except where a triangle's hit distance rounds below its own
+//           leaf box's entry distance (grazing hits on box faces).
+#include <cuda_runtime.h>
+
+#include "fk_device.cuh"
+#include "fk_internal.h"
+
+namespace fk {
+
+struct SceneDev {
+  const float4* __restrict__ node_lo;
+  const float4* __restrict__ node_hi;
+  const uint32_t* __restrict__ node_jump;
+  const float4* __restrict__ pos4;
+  const float4* __restrict__ nrm4;
+  const float4* __restrict__ wide;
+  const float4* __restrict__ rec;
+  uint32_t node_count;
+  uint32_t root_is_leaf;
+  uint32_t corner_count;
+};
+
+// A hit index read from a caller's buffer: a miss, or the first corner of a
+// triangle inside the scene.  Anything else is reported and treated as a miss.
+__device__ __forceinline__ bool valid_hit(uint32_t id, uint32_t corners) {
+  return id % 3 == 0 && id < corners;
+}
+
+static SceneDev dev_of(const fk_scene* s) {
+  SceneDev d;
+  d.node_lo = s->node_lo;
+  d.node_hi = s->node_hi;
+  d.node_jump = s->node_jump;
+  d.pos4 = s->pos4;
+  d.nrm4 = s->nrm4;
+  d.wide = s->wide;
+  d.rec = s->tri_rec;
+  d.node_count = s->node_count;
+  d.root_is_leaf = s->root_is_leaf;
+  d.corner_count = s->corner_count;
+  return d;
+}
+
+__device__ __forceinline__ uint32_t as_u32(float f) { return __float_as_uint(f); }
+
+// ------------------------------------------------------------------ records
+// Per triangle (a, b, c): n = normalize(cross(b - a, c - a)) and dot(a, n) as
+// Shaders/ao_step1.comp:73-77 computes them, plus the barycentric terms of
+// :54-62.  Layout: (n, a.n), (a, d01), (v0, d00), (v1, d11).
+__global__ void tri_records_kernel(const float4* __restrict__ pos4, float4* __restrict__ rec, uint32_t ntri) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntri) return;
+  f3 a = xyz(pos4[3 * (size_t)t]), b = xyz(pos4[3 * (size_t)t + 1]), c = xyz(pos4[3 * (size_t)t + 2]);
+  f3 v0 = sub(b, a), v1 = sub(c, a);
+  f3 n = normalize(cross(v0, v1));
+  float an = dot(a, n);
+  rec[4 * (size_t)t + 0] = make_float4(n.x, n.y, n.z, an);
+  rec[4 * (size_t)t + 1] = make_float4(a.x, a.y, a.z, dot(v0, v1));
+  rec[4 * (size_t)t + 2] = make_float4(v0.x, v0.y, v0.z, dot(v0, v0));
+  rec[4 * (size_t)t + 3] = make_float4(v1.x, v1.y, v1.z, dot(v1, v1));
+}
+
+int launch_tri_records(fk_ctx* ctx, fk_scene* s) {
+  uint32_t nt = s->corner_count / 3;
+  tri_records_kernel<<<(nt + 255) / 256, 256, 0, ctx->stream>>>(s->pos4, s->tri_rec, nt);
+  return fk_after_launch(ctx, "tri_records_kernel");
+}
+
+// ------------------------------------------------------------------ sampling test
+// Shaders/ao_step1.comp:71-92 followed by the range test of :100-105: returns
+// true and lowers `best` when the triangle is hit at t in [lo, best).  The
+// barycentric part only runs for hits inside the range (rejecting earlier
+// cannot change which t survive).
+__device__ __forceinline__ void tri_sample(const float4* __restrict__ rec, uint32_t t, f3 o, f3 d, float lo,
+                                           float& best) {
+  float4 A = __ldg(rec + 4 * (size_t)t);
+  f3 n = xyz(A);
+  float nd = dot(d, n);
+  if (!(fabsf(nd) > 0.0f)) return;
+  float pn = dot(o, n);
+  float th = __fdiv_rn(__fsub_rn(A.w, pn), nd);
+  if (!(th >= 0.0f && th >= lo && th < best)) return;
+  float4 B = __ldg(rec + 4 * (size_t)t + 1);
+  float4 C = __ldg(rec + 4 * (size_t)t + 2);
+  float4 D = __ldg(rec + 4 * (size_t)t + 3);
+  f3 p = add(o, scale(d, th));
+  f3 v2 = sub(p, xyz(B));
+  float d20 = dot(v2, xyz(C)), d21 = dot(v2, xyz(D));
+  float d00 = C.w, d01 = B.w, d11 = D.w;
+  float den = __fsub_rn(__fmul_rn(d00, d11), __fmul_rn(d01, d01));
+  float y = __fdiv_rn(__fsub_rn(__fmul_rn(d11, d20), __fmul_rn(d01, d21)), den);
+  float z = __fdiv_rn(__fsub_rn(__fmul_rn(d00, d21), __fmul_rn(d01, d20)), den);
+  float x = __fsub_rn(__fsub_rn(1.0f, y), z);
+  if (x >= 0.0f && y >= 0.0f && y <= 1.0f && z >= 0.0f && z <= 1.0f) best = th;
+}
+
+// Stop rules: which outcomes a caller needs.
+enum Stop { kClosest = 0, kUnderMax = 1, kAnyHit = 2 };
+
+template <int STOP>
+__device__ __forceinline__ bool settled(float best, float hi) {
+  if (STOP == kUnderMax) return best < hi;
+  if (STOP == kAnyHit) return best != FLT_MAX;
+  return false;
+}
+
+// Per-ray test counters of the counting variants (box tests, triangle tests).
+struct Tally {
+  uint32_t box = 0, tri = 0;
+};
+
+// raycastBVH of Shaders/ao_step1.comp:111-138, node order, skip pointers.
+template <int STOP, bool COUNT>
+__device__ float trace_skip(const SceneDev& s, f3 o, f3 d, float lo, float hi, Tally& c) {
+  float best = FLT_MAX;
+  uint32_t i = 0;
+  while (i < s.node_count) {
+    float4 L = __ldg(s.node_lo + i), H = __ldg(s.node_hi + i);
+    float a = ray_box(o, d, xyz(L), xyz(H));
+    if (COUNT) c.box++;
+    if (a < best && a < hi) {
+      uint32_t e = as_u32(H.w);
+      if (COUNT) c.tri += (e - as_u32(L.w)) / 3;
+      for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
+      if (settled<STOP>(best, hi)) break;
+      ++i;
+    } else {
+      i = __ldg(s.node_jump + i);
+    }
+  }
+  return best;
+}
+
+static constexpr int kStack = 64;
+
+// Near-first traversal of the children-in-parent layout with the same
+// pruning rule.  The host selects it only when the tree depth fits kStack;
+// an overflow is still caught and reported through `status`.
+template <int STOP, bool COUNT>
+__device__ float trace_ordered(const SceneDev& s, f3 o, f3 d, float lo, float hi, int* status, Tally& tally) {
+  float best = FLT_MAX;
+  {
+    float4 L = __ldg(s.node_lo), H = __ldg(s.node_hi);
+    float a = ray_box(o, d, xyz(L), xyz(H));
+    if (COUNT) tally.box++;
+    if (!(a < hi)) return best;
+    if (s.root_is_leaf) {
+      uint32_t e = as_u32(H.w);
+      if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
+      for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
+      return best;
+    }
+  }
+  int32_t stack_node[kStack];
+  float stack_dist[kStack];
+  int sp = 0;
+  int32_t cur = 0;
+  for (;;) {
+    const float4* w = s.wide + 4 * (size_t)cur;
+    float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
+    float aL = ray_box(o, d, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y));
+    float aR = ray_box(o, d, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w));
+    if (COUNT) tally.box += 2;
+    int32_t ref[2] = {__float_as_int(w3.x), __float_as_int(w3.y)};
+    int32_t cnt[2] = {__float_as_int(w3.z), __float_as_int(w3.w)};
+    float dist[2] = {aL, aR};
+    int first = aR < aL ? 1 : 0;
+    int32_t next = -1;
+    float next_d = 0.0f;
+    for (int q = 0; q < 2; ++q) {
+      int c = q == 0 ? first : 1 - first;
+      if (!(dist[c] < fminf(best, hi))) continue;
+      if (cnt[c] > 0) {
+        uint32_t t0 = (uint32_t)ref[c];
+        if (COUNT) tally.tri += (uint32_t)cnt[c];
+        for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s.rec, t, o, d, lo, best);
+        if (settled<STOP>(best, hi)) return best;
+      } else if (next < 0) {
+        next = ref[c];
+        next_d = dist[c];
+      } else {
+        if (sp >= kStack) {
+          atomicOr(status, 1);
+          return best;
+        }
+        stack_node[sp] = ref[c];
+        stack_dist[sp] = dist[c];
+        ++sp;
+      }
+    }
+    (void)next_d;
+    if (next >= 0) {
+      cur = next;
+      continue;
+    }
+    bool found = false;
+    while (sp > 0) {
+      --sp;
+      if (stack_dist[sp] < fminf(best, hi)) {
+        cur = stack_node[sp];
+        found = true;
+        break;
+      }
+    }
+    if (!found) return best;
+  }
+}
+
+template <int STOP, int TRAV, bool COUNT>
+__device__ __forceinline__ float trace(const SceneDev& s, f3 o, f3 d, float lo, float hi, int* status, Tally& c) {
+  if (TRAV == FK_TRAVERSE_ORDERED) return trace_ordered<STOP, COUNT>(s, o, d, lo, hi, status, c);
+  return trace_skip<STOP, COUNT>(s, o, d, lo, hi, c);
+}
+
+// ------------------------------------------------------------------ hemisphere
+struct HemiArgs {
+  SceneDev s;
+  const float4* __restrict__ samples;
+  const float4* __restrict__ coords;
+  const uint32_t* __restrict__ tidx;
+  uint32_t spp, perms, offset, count;
+  float lo, hi;
+  float* out0;
+  float* out1;
+  uint32_t* hits0;
+  uint32_t* hits1;
+  uint32_t* queue;
+  int* status;
+  unsigned long long* tally;  // counting variant: total box tests, triangle tests
+};
+
+// Ray frame of Shaders/ao_step0.comp:39-50.
+__device__ __forceinline__ void texel_frame(const SceneDev& s, float4 c, uint32_t id, f3& o, f3& d, f3& tx, f3& ty) {
+  o = blend3(xyz(__ldg(s.pos4 + id)), xyz(__ldg(s.pos4 + id + 1)), xyz(__ldg(s.pos4 + id + 2)), c.y, c.z, c.w);
+  d = normalize(blend3(xyz(__ldg(s.nrm4 + id)), xyz(__ldg(s.nrm4 + id + 1)), xyz(__ldg(s.nrm4 + id + 2)), c.y, c.z, c.w));
+  ty = normalize(fabsf(d.x) > fabsf(d.y) ? mk3(d.z, 0.0f, -d.x) : mk3(0.0f, d.z, -d.y));
+  tx = cross(d, ty);
+}
+
+// One warp per texel (texels pulled from an atomic queue), lanes = samples in
+// rounds of 32.  Per-sample values are folded in sample order with shuffles,
+// which reproduces the sequential sums of the *_step2 shaders exactly.
+// KIND: FK_AO, FK_BN, FK_THICK, FK_AO_BN.
+template <int KIND, int TRAV, bool COUNT>
+__global__ void __launch_bounds__(256) hemi_kernel(HemiArgs p) {
+  constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  for (;;) {
+    uint32_t item = 0;
+    if (lane == 0) item = atomicAdd(p.queue, 1u);
+    item = __shfl_sync(full, item, 0);
+    if (item >= p.count) return;
+    const uint32_t g = p.offset + item;
+    uint32_t id = __ldg(p.tidx + g);
+    if (id != kMiss && !valid_hit(id, p.s.corner_count)) {
+      if (lane == 0) atomicOr(p.status, 2);
+      id = kMiss;
+    }
+    if (id == kMiss) {
+      if (lane == 0) {
+        if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = 1.0f;
+        if (KIND == FK_THICK) p.out0[g] = p.hi;
+        float* bn = KIND == FK_BN ? p.out0 : (KIND == FK_AO_BN ? p.out1 : nullptr);
+        if (bn) { bn[3 * (size_t)g] = 0.0f; bn[3 * (size_t)g + 1] = 0.0f; bn[3 * (size_t)g + 2] = 0.0f; }
+        if (p.hits0) p.hits0[g] = 0;
+        if (p.hits1) p.hits1[g] = 0;
+      }
+      continue;
+    }
+    f3 o, d, tx, ty;
+    texel_frame(p.s, __ldg(p.coords + g), id, o, d, tx, ty);
+    if (KIND == FK_THICK) d = neg(d);  // Shaders/thick_step1.comp:149
+    const float4* row = p.samples + (size_t)(g % p.perms) * p.spp;
+    uint32_t occ = 0, anyhit = 0;
+    Tally tl;
+    float acc = 0.0f;
+    f3 vacc = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t k0 = 0; k0 < p.spp; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      const bool active = k < p.spp;
+      float t = FLT_MAX;
+      f3 dir = mk3(0.0f, 0.0f, 0.0f);
+      if (active) {
+        float4 rs = __ldg(row + k);
+        dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+        t = trace<STOP, TRAV, COUNT>(p.s, o, dir, p.lo, p.hi, p.status, tl);
+      }
+      const bool hit = active && t != FLT_MAX;
+      const bool under = hit && t < p.hi;
+      if (KIND == FK_AO || KIND == FK_AO_BN) occ += __popc(__ballot_sync(full, under));
+      anyhit += __popc(__ballot_sync(full, hit));
+      const int nact = (int)min(32u, p.spp - k0);
+      if (KIND == FK_BN || KIND == FK_AO_BN) {
+        f3 v = hit ? mk3(0.0f, 0.0f, 0.0f) : dir;
+        for (int j = 0; j < nact; ++j) {
+          vacc.x = __fadd_rn(vacc.x, __shfl_sync(full, v.x, j));
+          vacc.y = __fadd_rn(vacc.y, __shfl_sync(full, v.y, j));
+          vacc.z = __fadd_rn(vacc.z, __shfl_sync(full, v.z, j));
+        }
+      }
+      if (KIND == FK_THICK) {
+        float v = hit ? t : p.hi;
+        for (int j = 0; j < nact; ++j) acc = __fadd_rn(acc, __shfl_sync(full, v, j));
+      }
+    }
+    if (COUNT) {
+      unsigned long long b = tl.box, t = tl.tri;
+      for (int off = 16; off > 0; off >>= 1) {
+        b += __shfl_down_sync(full, b, off);
+        t += __shfl_down_sync(full, t, off);
+      }
+      if (lane == 0) {
+        atomicAdd(p.tally, b);
+        atomicAdd(p.tally + 1, t);
+      }
+    }
+    if (lane == 0) {
+      const float fs = (float)p.spp;
+      if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = __fsub_rn(1.0f, __fdiv_rn((float)occ, fs));
+      if (KIND == FK_THICK) p.out0[g] = __fdiv_rn(acc, fs);
+      if (KIND == FK_BN || KIND == FK_AO_BN) {
+        float* bn = KIND == FK_BN ? p.out0 : p.out1;
+        f3 v = normalize(vacc);
+        bn[3 * (size_t)g] = v.x;
+        bn[3 * (size_t)g + 1] = v.y;
+        bn[3 * (size_t)g + 2] = v.z;
+      }
+      if (KIND == FK_AO_BN) {
+        if (p.hits0) p.hits0[g] = occ;
+        if (p.hits1) p.hits1[g] = anyhit;
+      } else if (p.hits0) {
+        p.hits0[g] = KIND == FK_AO ? occ : anyhit;
+      }
+    }
+  }
+}
+
+template <int KIND, int TRAV>
+static int run_hemi(fk_ctx* ctx, const HemiArgs& a) {
+  auto kern = a.tally ? hemi_kernel<KIND, TRAV, true> : hemi_kernel<KIND, TRAV, false>;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 256, 0);
+  if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "occupancy");
+  if (per_sm < 1) per_sm = 1;
+  uint32_t warps_needed = a.count;
+  uint32_t blocks = (uint32_t)ctx->sm_count * (uint32_t)per_sm;
+  uint32_t max_blocks = (warps_needed + 7) / 8;
+  if (blocks > max_blocks) blocks = max_blocks;
+  if (blocks == 0) return FK_OK;
+  kern<<<blocks, 256, 0, ctx->stream>>>(a);
+  return fk_after_launch(ctx, "hemi_kernel");
+}
+
+int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
+  HemiArgs a;
+  a.s = dev_of(s);
+  a.samples = h.samples;
+  a.coords = h.coords;
+  a.tidx = h.tidx;
+  a.spp = h.spp;
+  a.perms = h.perms;
+  a.offset = h.offset;
+  a.count = h.count;
+  a.lo = h.min_d;
+  a.hi = h.max_d;
+  a.out0 = h.out0;
+  a.out1 = h.out1;
+  a.hits0 = h.hits0;
+  a.hits1 = h.hits1;
+  a.queue = fk_take_counter(ctx);
+  a.status = ctx->status;
+  a.tally = h.tally;
+  int trav = h.traverse;
+  if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= (uint32_t)kStack ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
+  if (trav == FK_TRAVERSE_ORDERED && s->depth > (uint32_t)kStack)
+    return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 64; use FK_TRAVERSE_SKIP");
+#define FK_HEMI_CASE(K)                                                        \
+  case K:                                                                      \
+    return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a) \
+                                       : run_hemi<K, FK_TRAVERSE_SKIP>(ctx, a);
+  switch (h.kind) {
+    FK_HEMI_CASE(FK_AO)
+    FK_HEMI_CASE(FK_BN)
+    FK_HEMI_CASE(FK_THICK)
+    FK_HEMI_CASE(FK_AO_BN)
+    default:
+      return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown kind");
+  }
+#undef FK_HEMI_CASE
+}
+
+// ------------------------------------------------------------------ mesh mapping
+__device__ __forceinline__ bool bary_ok_map(f3 w) {
+  return w.x >= -1e-5f && w.y >= -1e-5f && w.y <= 1.0f && w.z >= -1e-5f && w.z <= 1.0f;
+}
+
+// raycastBVH / raycastBackBVH of Shaders/meshmapping_nobackfaces.comp:102-180:
+// accepts triangles facing along +d (SIGN > 0) or against it (SIGN < 0) with
+// t in [0, cur); the closest so far is threaded through both passes.
+template <int SIGN>
+__device__ void walk_oneside(const SceneDev& s, f3 o, f3 d, float& cur, uint32_t& id, f3& w) {
+  uint32_t i = 0;
+  while (i < s.node_count) {
+    float4 L = __ldg(s.node_lo + i), H = __ldg(s.node_hi + i);
+    float a = ray_box(o, d, xyz(L), xyz(H));
+    if (a < cur) {
+      uint32_t e = as_u32(H.w);
+      for (uint32_t k = as_u32(L.w); k < e; k += 3) {
+        float4 A = __ldg(s.rec + 4 * (size_t)(k / 3));
+        f3 n = xyz(A);
+        float nd = dot(d, n);
+        if (SIGN > 0 ? !(nd > 0.0f) : !(nd < 0.0f)) continue;
+        float pn = dot(o, n);
+        float t = __fdiv_rn(__fsub_rn(A.w, pn), nd);
+        if (!(t >= 0.0f && t < cur)) continue;
+        f3 q = bary_f64(add(o, scale(d, t)), xyz(__ldg(s.pos4 + k)), xyz(__ldg(s.pos4 + k + 1)),
+                        xyz(__ldg(s.pos4 + k + 2)));
+        if (bary_ok_map(q)) {
+          cur = t;
+          id = k;
+          w = q;
+        }
+      }
+      ++i;
+    } else {
+      i = __ldg(s.node_jump + i);
+    }
+  }
+}
+
+// raycastBVH of Shaders/meshmapping.comp:87-137 (either facing, t >= 0).
+__device__ float walk_twoside(const SceneDev& s, f3 o, f3 d, float mint, uint32_t& id, f3& w) {
+  uint32_t i = 0;
+  while (i < s.node_count) {
+    float4 L = __ldg(s.node_lo + i), H = __ldg(s.node_hi + i);
+    float a = ray_box(o, d, xyz(L), xyz(H));
+    if (a < mint) {
+      float lm = FLT_MAX;
+      uint32_t lid = 0;
+      f3 lw = mk3(0.0f, 0.0f, 0.0f);
+      uint32_t e = as_u32(H.w);
+      for (uint32_t k = as_u32(L.w); k < e; k += 3) {
+        float4 A = __ldg(s.rec + 4 * (size_t)(k / 3));
+        f3 n = xyz(A);
+        float nd = dot(d, n);
+        if (!(fabsf(nd) > 0.0f)) continue;
+        float pn = dot(o, n);
+        float t = __fdiv_rn(__fsub_rn(A.w, pn), nd);
+        if (!(t >= 0.0f && t < lm)) continue;
+        f3 q = bary_f64(add(o, scale(d, t)), xyz(__ldg(s.pos4 + k)), xyz(__ldg(s.pos4 + k + 1)),
+                        xyz(__ldg(s.pos4 + k + 2)));
+        if (bary_ok_map(q)) {
+          lm = t;
+          lid = k;
+          lw = q;
+        }
+      }
+      if (lm < mint) {
+        mint = lm;
+        id = lid;
+        w = lw;
+      }
+      ++i;
+    } else {
+      i = __ldg(s.node_jump + i);
+    }
+  }
+  return mint;
+}
+
+template <int CULL>
+__global__ void __launch_bounds__(128) meshmap_kernel(SceneDev s, const float4* __restrict__ pix, uint32_t offset,
+                                                      uint32_t count, float4* __restrict__ coords,
+                                                      uint32_t* __restrict__ tidx) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  uint32_t g = offset + j;
+  f3 p = xyz(__ldg(pix + 2 * (size_t)g)), d = xyz(__ldg(pix + 2 * (size_t)g + 1));
+  uint32_t id = kMiss;
+  f3 w = mk3(0.0f, 0.0f, 0.0f);
+  float t = FLT_MAX;
+  if (CULL) {
+    walk_oneside<+1>(s, p, d, t, id, w);
+    walk_oneside<-1>(s, p, neg(d), t, id, w);
+  } else {
+    t = fminf(t, walk_twoside(s, p, d, t, id, w));
+    t = fminf(t, walk_twoside(s, p, neg(d), t, id, w));
+  }
+  coords[g] = make_float4(t, w.x, w.y, w.z);
+  tidx[g] = id;
+}
+
+int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, uint32_t offset, uint32_t count,
+                   float4* coords, uint32_t* tidx) {
+  if (count == 0) return FK_OK;
+  uint32_t blocks = (count + 127) / 128;
+  if (cull) meshmap_kernel<1><<<blocks, 128, 0, ctx->stream>>>(dev_of(s), m->pix, offset, count, coords, tidx);
+  else meshmap_kernel<0><<<blocks, 128, 0, ctx->stream>>>(dev_of(s), m->pix, offset, count, coords, tidx);
+  return fk_after_launch(ctx, "meshmap_kernel");
+}
+
+// ------------------------------------------------------------------ gathers
+// Shaders/heights.comp:13-19, positions.comp:17-32, normals.comp:13-28.
+template <int KIND>
+__global__ void gather_kernel(SceneDev s, const float4* __restrict__ coords, const uint32_t* __restrict__ tidx,
+                              uint32_t offset, uint32_t count, float* __restrict__ out) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  uint32_t g = offset + j;
+  float4 c = __ldg(coords + g);
+  if (KIND == FK_GATHER_HEIGHT) {
+    out[g] = c.x != FLT_MAX ? c.x : 0.0f;
+    return;
+  }
+  uint32_t id = __ldg(tidx + g);
+  f3 v = mk3(0.0f, 0.0f, 0.0f);
+  if (id != kMiss && valid_hit(id, s.corner_count)) {
+    const float4* src = KIND == FK_GATHER_POSITION ? s.pos4 : s.nrm4;
+    v = blend3(xyz(__ldg(src + id)), xyz(__ldg(src + id + 1)), xyz(__ldg(src + id + 2)), c.y, c.z, c.w);
+    if (KIND == FK_GATHER_NORMAL) v = normalize(v);
+  }
+  out[3 * (size_t)g] = v.x;
+  out[3 * (size_t)g + 1] = v.y;
+  out[3 * (size_t)g + 2] = v.z;
+}
+
+int launch_gather(fk_ctx* ctx, const fk_scene* s, int kind, const float4* coords, const uint32_t* tidx,
+                  uint32_t offset, uint32_t count, float* out) {
+  if (count == 0) return FK_OK;
+  uint32_t blocks = (count + 255) / 256;
+  SceneDev d = dev_of(s);
+  switch (kind) {
+    case FK_GATHER_HEIGHT: gather_kernel<FK_GATHER_HEIGHT><<<blocks, 256, 0, ctx->stream>>>(d, coords, tidx, offset, count, out); break;
+    case FK_GATHER_POSITION: gather_kernel<FK_GATHER_POSITION><<<blocks, 256, 0, ctx->stream>>>(d, coords, tidx, offset, count, out); break;
+    case FK_GATHER_NORMAL: gather_kernel<FK_GATHER_NORMAL><<<blocks, 256, 0, ctx->stream>>>(d, coords, tidx, offset, count, out); break;
+    default: return fk_fail(ctx, FK_ERR_INVALID, "fk_gather: unknown kind");
+  }
+  return fk_after_launch(ctx, "gather_kernel");
+}
+
+// Shaders/tangentspace.comp:22-41: rows of the adjugate of (n, t, b).
+__global__ void tangent_kernel(const float4* __restrict__ pixt, uint32_t offset, uint32_t count, float* io3) {
+  uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= count) return;
+  uint32_t g = offset + j;
+  f3 v = mk3(io3[3 * (size_t)g], io3[3 * (size_t)g + 1], io3[3 * (size_t)g + 2]);
+  f3 n = xyz(__ldg(pixt + 3 * (size_t)g)), t = xyz(__ldg(pixt + 3 * (size_t)g + 1)), b = xyz(__ldg(pixt + 3 * (size_t)g + 2));
+  f3 d0 = mk3(__fsub_rn(__fmul_rn(n.z, b.y), __fmul_rn(n.y, b.z)), __fsub_rn(__fmul_rn(n.x, b.z), __fmul_rn(n.z, b.x)),
+              __fsub_rn(__fmul_rn(n.y, b.x), __fmul_rn(n.x, b.y)));
+  f3 d1 = mk3(__fsub_rn(__fmul_rn(t.z, n.y), __fmul_rn(t.y, n.z)), __fsub_rn(__fmul_rn(t.x, n.z), __fmul_rn(n.x, t.z)),
+              __fsub_rn(__fmul_rn(n.x, t.y), __fmul_rn(t.x, n.y)));
+  f3 d2 = mk3(__fsub_rn(__fmul_rn(t.y, b.z), __fmul_rn(t.z, b.y)), __fsub_rn(__fmul_rn(t.z, b.x), __fmul_rn(t.x, b.z)),
+              __fsub_rn(__fmul_rn(t.x, b.y), __fmul_rn(t.y, b.x)));
+  f3 r = normalize(mk3(dot(v, d0), dot(v, d1), dot(v, d2)));
+  io3[3 * (size_t)g] = r.x;
+  io3[3 * (size_t)g + 1] = r.y;
+  io3[3 * (size_t)g + 2] = r.z;
+}
+
+int launch_tangent_space(fk_ctx* ctx, const fk_texel_map* m, uint32_t offset, uint32_t count, float* io3) {
+  if (count == 0) return FK_OK;
+  tangent_kernel<<<(count + 255) / 256, 256, 0, ctx->stream>>>(m->pixt, offset, count, io3);
+  return fk_after_launch(ctx, "tangent_kernel");
+}
+
+}  // namespace fk

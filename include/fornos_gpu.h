@@ -1,0 +1,341 @@
+/*
+ * fornos_gpu.h - C ABI of the B200 (sm_100a) texture-baking path.
+ *
+ * This ABI replaces the OpenGL buffer-and-dispatch layer of Fornos:
+ *   ComputeBuffer<T>            Src/compute.h:37-87     -> fk_buf_*
+ *   LoadComputeShader_*()       Src/computeshaders.h:28-46
+ *   + glDispatchCompute in every runStep (e.g. Src/solver_ao.cpp:91-118)
+ *                                                       -> fk_meshmap, fk_hemisphere,
+ *                                                          fk_gather, fk_tangent_space
+ * and exposes the host solver API that sits on top of it:
+ *   MeshMapping                 Src/meshmapping.h:42-75 -> fk_meshmapping_*
+ *   Height/Position/Normals/AmbientOcclusion/BentNormals/Thickness solvers
+ *                               Src/solver_*.h          -> fk_solver_*
+ *   Mesh, normal / tangent generators
+ *                               Src/mesh.h:35-63, Src/mesh.cpp:619-768 -> fk_mesh_*
+ *   BVH::createBinary + fillMeshData
+ *                               Src/bvh.h:32-46, Src/meshmapping.cpp:62-125 -> fk_bvh_*
+ *   MapUV::from* + CompressedMapUV
+ *                               Src/compute.h:214-259   -> fk_raster_uv, fk_texel_map_*
+ *   computeSamplesImportanceCosDir
+ *                               Src/math.h:363-382      -> fk_samples_cosine
+ *
+ * Conventions.  Every function returns FK_OK (0) or a negative FK_ERR_* code;
+ * nothing aborts or throws across the ABI.  fk_last_error(ctx) describes the
+ * last failure of that context.  Device work is ordered on the context's
+ * stream (fk_ctx_set_stream); functions that return host data synchronise it.
+ * Handles belong to the context that made them and are freed by their *_free
+ * call or by fk_ctx_destroy.  One context per host thread.
+ */
+#ifndef FORNOS_GPU_H
+#define FORNOS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define FK_OK 0
+#define FK_ERR_INVALID (-1)     /* bad argument: null handle, size, range, kind */
+#define FK_ERR_CUDA (-2)        /* a CUDA runtime call failed */
+#define FK_ERR_NOMEM (-3)       /* device or host allocation failed */
+#define FK_ERR_STATE (-4)       /* call out of order (e.g. run_step before init) */
+#define FK_ERR_DEVICE (-5)      /* a kernel reported a limit it could not honour */
+#define FK_ERR_UNSUPPORTED (-6) /* no sm_100 device, or feature not built */
+
+/* ------------------------------------------------------------ handles */
+typedef struct fk_ctx fk_ctx;
+typedef struct fk_buf fk_buf;               /* device allocation */
+typedef struct fk_mesh fk_mesh;             /* host indexed mesh (Src/mesh.h) */
+typedef struct fk_bvh fk_bvh;               /* host BVH tree (Src/bvh.h) */
+typedef struct fk_scene fk_scene;           /* high-poly mesh + BVH resident on the device */
+typedef struct fk_texel_map fk_texel_map;   /* compressed texel map on the device */
+typedef struct fk_meshmapping fk_meshmapping;
+typedef struct fk_solver fk_solver;
+
+/* ------------------------------------------------------------ context */
+/* Opens `device` (must be compute capability 10.x).  No graphics context. */
+int fk_ctx_create(int device, fk_ctx** out);
+int fk_ctx_destroy(fk_ctx* ctx);
+const char* fk_last_error(const fk_ctx* ctx);
+/* cudaStream_t to order work on; NULL = the context's own stream. */
+int fk_ctx_set_stream(fk_ctx* ctx, void* cuda_stream);
+void* fk_ctx_stream(const fk_ctx* ctx);
+int fk_sync(fk_ctx* ctx);
+/* Kernel launches issued by this context so far. */
+uint64_t fk_launch_count(const fk_ctx* ctx);
+
+/* ------------------------------------------------------------ buffers
+ * Replaces ComputeBuffer<T> (Src/compute.h:37-87).  New buffers are
+ * zero-filled like ComputeBuffer(count, usage) (Src/compute.h:57-65). */
+int fk_buf_alloc(fk_ctx* ctx, size_t bytes, fk_buf** out);
+int fk_buf_upload(fk_ctx* ctx, fk_buf* buf, size_t offset, const void* src, size_t bytes);
+int fk_buf_download(fk_ctx* ctx, const fk_buf* buf, size_t offset, void* dst, size_t bytes);
+int fk_buf_free(fk_ctx* ctx, fk_buf* buf);
+size_t fk_buf_size(const fk_buf* buf);
+void* fk_buf_device_ptr(const fk_buf* buf);
+
+/* ------------------------------------------------------------ host mesh
+ * Indexed mesh exactly as Src/mesh.h:35-63: per-vertex (position, texcoord,
+ * normal) indices, per-triangle vertex indices; tangents / bitangents per
+ * vertex (may be absent).  Arrays are copied on create. */
+typedef struct fk_mesh_desc {
+  uint32_t position_count;
+  const float* positions;   /* 3 floats each */
+  uint32_t texcoord_count;
+  const float* texcoords;   /* 2 floats each */
+  uint32_t normal_count;
+  const float* normals;     /* 3 floats each */
+  uint32_t vertex_count;
+  const uint32_t* vertices; /* 3 u32 each: position, texcoord, normal index */
+  uint32_t triangle_count;
+  const uint32_t* triangles;/* 3 u32 each: vertex indices */
+  const float* tangents;    /* 3 floats per vertex, or NULL */
+  const float* bitangents;  /* 3 floats per vertex, or NULL */
+} fk_mesh_desc;
+
+int fk_mesh_create(const fk_mesh_desc* desc, fk_mesh** out);
+/* Fills `out` with pointers into the mesh's own arrays (valid until the
+ * mesh changes or is freed). */
+int fk_mesh_describe(const fk_mesh* mesh, fk_mesh_desc* out);
+int fk_mesh_copy(const fk_mesh* mesh, fk_mesh** out);                 /* Mesh::createCopy */
+int fk_mesh_free(fk_mesh* mesh);
+int fk_mesh_compute_face_normals(fk_mesh* mesh);                      /* Src/mesh.cpp:627 */
+int fk_mesh_compute_vertex_normals(fk_mesh* mesh);                    /* Src/mesh.cpp:650 */
+int fk_mesh_compute_vertex_normals_welded(fk_mesh* mesh);             /* Src/mesh.cpp:680 (Aggressive) */
+int fk_mesh_compute_tangent_space(fk_mesh* mesh);                     /* Src/mesh.cpp:724 */
+
+/* ------------------------------------------------------------ BVH (host)
+ * BVH::createBinary (Src/bvh.cpp:283-314): 16-bucket split, leaves of at
+ * most max_tris_per_node triangles, depth limit max_depth (8192 in
+ * Src/fornos.cpp:157).  Multi-threaded; the tree is identical to the
+ * single-threaded build. */
+int fk_bvh_build(const fk_mesh* mesh, uint32_t max_tris_per_node, uint32_t max_depth, fk_bvh** out);
+int fk_bvh_free(fk_bvh* bvh);
+
+/* Flattened skip-pointer node (BVHGPUData, Src/meshmapping.h:33-40), 36 B. */
+typedef struct fk_bvh_node {
+  float aabb_min[3];
+  float aabb_max[3];
+  uint32_t start; /* first triangle corner (multiple of 3) */
+  uint32_t end;   /* one past the last corner; start == end for inner nodes */
+  uint32_t jump;  /* index of the node after this subtree */
+} fk_bvh_node;
+
+/* fillMeshData (Src/meshmapping.cpp:62-125): node and corner counts, then the
+ * arrays (positions / normals as 4 floats per corner, w = 0). */
+int fk_bvh_flatten_sizes(const fk_bvh* bvh, uint32_t* node_count, uint32_t* corner_count);
+int fk_bvh_flatten(const fk_bvh* bvh, const fk_mesh* mesh, fk_bvh_node* nodes, float* positions4, float* normals4);
+
+/* ------------------------------------------------------------ device scene */
+int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t node_count, const float* positions4,
+                    const float* normals4, uint32_t corner_count, fk_scene** out);
+int fk_scene_free(fk_ctx* ctx, fk_scene* scene);
+typedef struct fk_scene_info {
+  uint32_t node_count;
+  uint32_t corner_count;
+  uint32_t depth;        /* levels from the root to the deepest leaf */
+  uint32_t leaf_count;
+  uint64_t device_bytes;
+} fk_scene_info;
+int fk_scene_get_info(const fk_scene* scene, fk_scene_info* out);
+
+/* ------------------------------------------------------------ texel map
+ * MapUV::fromMesh / fromMeshes / fromMeshes_Hybrid (Src/compute.cpp:352-370)
+ * followed by CompressedMapUV (Src/compute.cpp:372-416), on the device.
+ * Pixel rows: Pix_GPUData {p, pad, d, pad} (32 B) and PixT_GPUData
+ * {n, pad, t, pad, b, pad} (48 B) (Src/meshmapping.h:15-31), plus the texel
+ * index in the full map. */
+#define FK_MAP_SMOOTH 0           /* directions from `dirs` (welded normals) */
+#define FK_MAP_LOWPOLY_NORMALS 1  /* directions = the mesh's own normals */
+#define FK_MAP_HYBRID 2           /* blend by edge distance (mappingEdge) */
+int fk_raster_uv(fk_ctx* ctx, const fk_mesh* lowpoly, const fk_mesh* dirs, uint32_t width, uint32_t height,
+                 int mode, float edge, fk_texel_map** out);
+int fk_texel_map_from_host(fk_ctx* ctx, uint32_t width, uint32_t height, uint32_t count, const float* pix8,
+                           const float* pixt12, const uint32_t* indices, fk_texel_map** out);
+int fk_texel_map_info(const fk_texel_map* map, uint32_t* width, uint32_t* height, uint32_t* count);
+int fk_texel_map_download(fk_ctx* ctx, const fk_texel_map* map, float* pix8, float* pixt12, uint32_t* indices);
+int fk_texel_map_free(fk_ctx* ctx, fk_texel_map* map);
+
+/* ------------------------------------------------------------ sample table
+ * computeSamplesImportanceCosDir(spp, perms) (Src/math.h:363-382) with a
+ * seeded std::mt19937 in place of std::random_device; 4 floats per sample
+ * (w = 0), perms rows of spp samples.  Host function. */
+int fk_samples_cosine(uint32_t spp, uint32_t perms, uint32_t seed, float* out4);
+
+/* ------------------------------------------------------------ kernels
+ * Mesh mapping, Shaders/meshmapping_nobackfaces.comp (cull_backfaces = 1,
+ * the default of Src/fornos.h:48) or Shaders/meshmapping.comp, over texels
+ * [offset, offset + count) of `map`.  coords: float4 (t, b0, b1, b2) per
+ * texel; tidx: u32 per texel, 0xFFFFFFFF on a miss. */
+int fk_meshmap(fk_ctx* ctx, const fk_scene* scene, const fk_texel_map* map, int cull_backfaces, uint32_t offset,
+               uint32_t count, fk_buf* coords, fk_buf* tidx);
+
+/* ShaderParams of Src/solver_ao.h:67-73. */
+typedef struct fk_sample_params {
+  uint32_t sample_count;
+  uint32_t perm_count;   /* rows of the sample table; 4096 in the reference */
+  float min_distance;
+  float max_distance;
+} fk_sample_params;
+
+#define FK_AO 0     /* ao_step0/1/2: 1 - occluded / spp */
+#define FK_BN 1     /* bentnormals_step1/2: normalize(sum of free directions) */
+#define FK_THICK 2  /* thick_step1/2: mean hit distance around -normal */
+#define FK_AO_BN 3  /* AO and bent normals from one traversal (same params) */
+
+/* Traversal strategy. */
+#define FK_TRAVERSE_AUTO 0    /* tuned choice for the scene */
+#define FK_TRAVERSE_ORDERED 1 /* near-first stack traversal over the BVH2 layout */
+#define FK_TRAVERSE_SKIP 2    /* the reference's skip-pointer walk, node order */
+
+/* Hemisphere sampling for texels [offset, offset + count) (global indices
+ * into coords / tidx).  Outputs, indexed by texel:
+ *   FK_AO    out0: float            out_hits0: occluded samples (t < max)
+ *   FK_BN    out0: 3 floats (V3)    out_hits0: samples with any hit
+ *   FK_THICK out0: float            out_hits0: samples with any hit
+ *   FK_AO_BN out0: AO, out1: BN     out_hits0 / out_hits1 as above
+ * hits buffers may be NULL.  Texels whose mapping missed get AO 1, BN (0,0,0),
+ * thickness max_distance and 0 hits. */
+int fk_hemisphere(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
+                  const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
+                  int traverse, fk_buf* out0, fk_buf* out1, fk_buf* out_hits0, fk_buf* out_hits1);
+
+/* Gathers, Shaders/heights.comp, positions.comp, normals.comp, over texels
+ * [offset, offset + count).  HEIGHT: float; POSITION / NORMAL: 3 floats.
+ * Missed texels: height 0 (the shader's rule), position / normal (0,0,0). */
+#define FK_GATHER_HEIGHT 0
+#define FK_GATHER_POSITION 1
+#define FK_GATHER_NORMAL 2
+int fk_gather(fk_ctx* ctx, const fk_scene* scene, int kind, const fk_buf* coords, const fk_buf* tidx,
+              uint32_t offset, uint32_t count, fk_buf* out);
+
+/* Shaders/tangentspace.comp in place over 3-float values [offset, offset+count). */
+int fk_tangent_space(fk_ctx* ctx, const fk_texel_map* map, uint32_t offset, uint32_t count, fk_buf* io3);
+
+/* ------------------------------------------------------------ MeshMapping
+ * Src/meshmapping.h:42-75.  init flattens the BVH (fillMeshData), uploads the
+ * pixels, mesh and nodes, and sizes the result buffers to the texel count
+ * rounded up to 64 (Src/meshmapping.cpp:165).  run_step maps the next chunk
+ * of work_per_step texels (0 = all remaining); *done = 1 when finished. */
+int fk_meshmapping_create(fk_ctx* ctx, fk_meshmapping** out);
+int fk_meshmapping_init(fk_meshmapping* mm, const fk_texel_map* map, const fk_mesh* hipoly, const fk_bvh* bvh,
+                        int cull_backfaces);
+int fk_meshmapping_init_scene(fk_meshmapping* mm, const fk_texel_map* map, const fk_scene* scene,
+                              int cull_backfaces);
+int fk_meshmapping_set_work_per_step(fk_meshmapping* mm, uint32_t texels);
+int fk_meshmapping_run_step(fk_meshmapping* mm, int* done);
+float fk_meshmapping_progress(const fk_meshmapping* mm);
+int fk_meshmapping_results(fk_meshmapping* mm, float* coords4, uint32_t* tidx);
+const fk_buf* fk_meshmapping_coords(const fk_meshmapping* mm);
+const fk_buf* fk_meshmapping_tidx(const fk_meshmapping* mm);
+const fk_scene* fk_meshmapping_scene(const fk_meshmapping* mm);
+int fk_meshmapping_free(fk_meshmapping* mm);
+
+/* ------------------------------------------------------------ solvers
+ * One handle type for the six solvers of Src/solver_*.h.  Params mirror
+ * FornosParameters_Solver* (Src/fornos.h:57-112). */
+#define FK_SOLVER_HEIGHT 0
+#define FK_SOLVER_POSITION 1
+#define FK_SOLVER_NORMALS 2
+#define FK_SOLVER_AO 3
+#define FK_SOLVER_BENT_NORMALS 4
+#define FK_SOLVER_THICKNESS 5
+
+typedef struct fk_solver_params {
+  int kind;                /* FK_SOLVER_* */
+  uint32_t sample_count;   /* AO / BN / thickness */
+  float min_distance;      /* AO / BN / thickness */
+  float max_distance;      /* AO / BN / thickness; height: export range */
+  int tangent_space;       /* normals / bent normals */
+  int normalize_output;    /* height (export option, carried only) */
+  uint32_t seed;           /* sample-table seed (std::random_device in the reference) */
+  int traverse;            /* FK_TRAVERSE_* */
+} fk_solver_params;
+
+int fk_solver_create(fk_ctx* ctx, const fk_solver_params* params, fk_solver** out);
+int fk_solver_init(fk_solver* s, const fk_texel_map* map, fk_meshmapping* mm);
+/* Texels per run_step (0 = all remaining).  Progress is kept, so a long bake
+ * advances (and can be resumed) chunk by chunk. */
+int fk_solver_set_work_per_step(fk_solver* s, uint32_t texels);
+int fk_solver_run_step(fk_solver* s, int* done);
+float fk_solver_progress(const fk_solver* s);
+/* getResults(): floats per texel (1 or 3) times the texel count rounded up to
+ * 64, as the reference's result buffers are sized. */
+size_t fk_solver_result_count(const fk_solver* s);
+int fk_solver_results(fk_solver* s, float* host_out, size_t floats);
+/* Occluder / hit counts per texel (sampling solvers only). */
+int fk_solver_hits(fk_solver* s, uint32_t* host_out, size_t count);
+const fk_buf* fk_solver_result_buffer(const fk_solver* s);
+int fk_solver_free(fk_solver* s);
+
+/* ------------------------------------------------------------ one-shot bake
+ * FornosRunner::start + run (Src/fornos.cpp:53-251) from host arrays, after
+ * the host preprocessing (mesh loading, normals, BVH build, texel map): uploads
+ * the flattened scene and the texel rows, runs mesh mapping and every enabled
+ * solver, and copies the results back.  AO and bent normals with equal
+ * sample parameters share one traversal. */
+typedef struct fk_bake_sampler {
+  int enabled;
+  uint32_t sample_count;
+  float min_distance;
+  float max_distance;
+  uint32_t seed;
+  int tangent_space; /* bent normals only */
+} fk_bake_sampler;
+
+typedef struct fk_bake_desc {
+  const fk_bvh_node* nodes;
+  uint32_t node_count;
+  const float* positions4;
+  const float* normals4;
+  uint32_t corner_count;
+  uint32_t width, height, texel_count;
+  const float* pix8;        /* Pix_GPUData rows */
+  const float* pixt12;      /* PixT_GPUData rows */
+  const uint32_t* indices;  /* texel index in the full map */
+  int cull_backfaces;
+  int height_enabled;
+  int position_enabled;
+  int normals_enabled;
+  int normals_tangent_space;
+  fk_bake_sampler ao;
+  fk_bake_sampler bent_normals;
+  fk_bake_sampler thickness;
+  int traverse;             /* FK_TRAVERSE_* */
+} fk_bake_desc;
+
+/* Host outputs, texel_count rows each; NULL skips the copy. */
+typedef struct fk_bake_out {
+  float* coords4;
+  uint32_t* tidx;
+  float* height;
+  float* position3;
+  float* normals3;
+  float* ao;
+  float* bent_normals3;
+  float* thickness;
+} fk_bake_out;
+
+int fk_bake(fk_ctx* ctx, const fk_bake_desc* desc, fk_bake_out* out);
+
+/* ------------------------------------------------------------ diagnostics
+ * FP32 throughput of independent add / multiply / min chains on this device
+ * (one operation counted per instruction), the denominator of the traversal
+ * roofline. */
+int fk_diag_fp32_peak(fk_ctx* ctx, double* ops_per_second);
+
+/* Runs fk_hemisphere's counting variant over the same arguments (outputs go
+ * to scratch) and returns the ray-box and ray-triangle tests it executed:
+ * tests[0] = box tests, tests[1] = triangle tests. */
+int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
+                             const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
+                             int traverse, uint64_t* tests);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FORNOS_GPU_H */

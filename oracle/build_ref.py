@@ -14,7 +14,8 @@ reference tree (default /root/reference, override with FORNOS_REF_ROOT):
   * 3rdParty/glad/glad.c                   GL entry-point table the above refer
                                            to (never called: no GL context);
   * Shaders/*.comp                         rewritten on the fly to C++ (buffer and
-                                           uniform declarations become globals,
+                                           uniform declarations become thread-
+                                           local globals,
                                            in/out parameters become references,
                                            float literals get an f suffix) and
                                            compiled against ref_glsl.h.
@@ -63,13 +64,13 @@ def glsl_to_cpp(src, name):
             defines.append(m.group(1))
         m = re.match(r"layout\s*\(\s*location\s*=\s*\d+\s*\)\s*uniform\s+(\w+)\s+(\w+)\s*;", s)
         if m:
-            out.append("static %s %s;" % (m.group(1), m.group(2)))
+            out.append("static thread_local %s %s;" % (m.group(1), m.group(2)))
             continue
         m = re.match(r"layout\s*\(\s*std430\s*,\s*binding\s*=\s*\d+\s*\)\s*(?:readonly\s+|writeonly\s+)?"
                      r"buffer\s+\w+\s*\{\s*(\w+)\s+(\w+)\s*(\[\])?\s*;\s*\}\s*;", s)
         if m:
             star = "*" if m.group(3) else ""
-            out.append("static %s%s %s;" % (m.group(1), star, m.group(2)))
+            out.append("static thread_local %s%s %s;" % (m.group(1), star, m.group(2)))
             continue
         line = re.sub(r"\bin\s+out\s+(\w+)\s+(\w+)", r"\1& \2", line)
         line = re.sub(r"\bout\s+(\w+)\s+(\w+)", r"\1& \2", line)

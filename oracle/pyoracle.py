@@ -265,12 +265,16 @@ class Reference:
                                     _u32(len(nodes)), _u32(n), ptr(coords), ptr(tidx, _u32p))
         return coords, tidx
 
-    def hemisphere(self, kind, nodes, pos4, nrm4, coords, tidx, samples4, spp, min_d, max_d, perms=4096):
-        n = len(tidx)
+    def hemisphere(self, kind, nodes, pos4, nrm4, coords, tidx, samples4, spp, min_d, max_d, texels=None,
+                   perms=4096):
+        """Reference shaders for the listed texels (all when None); one row per
+        listed texel."""
+        n = len(tidx) if texels is None else len(texels)
         out = np.zeros((n, 3) if kind == 1 else n, np.float32)
+        tx = None if texels is None else np.ascontiguousarray(texels, np.uint32)
         self.lib.ref_shader_hemisphere(_int(kind), nodes.ctypes.data_as(_vp), _u32(len(nodes)), ptr(pos4), ptr(nrm4),
                                        ptr(coords), ptr(tidx, _u32p), ptr(samples4), _u32(spp), _u32(perms),
-                                       _f32(min_d), _f32(max_d), _u32(n), ptr(out))
+                                       _f32(min_d), _f32(max_d), ptr(tx, _u32p), _u32(n), ptr(out))
         return out
 
     def gather(self, what, pos4, nrm4, coords, tidx):
