@@ -52,6 +52,7 @@ WORKLOADS = {
         tex=4096, spp=1024, min_d=0.001, max_d=0.5, bakers=("ao", "bn", "thick")),
 }
 TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2}
+SCHEDULE = {"auto": 0, "static": 0x10, "dynamic": 0x20}
 # DRAM bytes per hemisphere-kernel launch from ncu captures (profiles/), by workload.
 NCU_TRAFFIC = {}
 
@@ -151,7 +152,7 @@ def run_fornos(args, wl, rank, world):
     stream = torch.cuda.Stream()
     ctx = api.Context(dev)
     ctx.set_stream(stream.cuda_stream)
-    trav = TRAVERSE[args.traverse]
+    trav = TRAVERSE[args.traverse] | SCHEDULE[args.schedule]
     prep = Prepared(wl, args.seed + rank)
     tex, spp, lo_d, hi_d = wl["tex"], wl["spp"], wl["min_d"], wl["max_d"]
 
@@ -304,7 +305,7 @@ def run_fornos(args, wl, rank, world):
         "dtype": "f32", "data": "synthetic (seeded generated meshes; no public dataset)",
         "config": {"workload": args.workload, "desc": wl["desc"], "texels": n, "texture": tex, "spp": spp,
                    "high_poly_triangles": prep.triangles, "bvh_nodes": info["node_count"],
-                   "bvh_depth": info["depth"], "traverse": args.traverse,
+                   "bvh_depth": info["depth"], "traverse": args.traverse, "schedule": args.schedule,
                    "rays_per_texel": rays_per_texel(wl),
                    "rays_counted": "2 mapping + spp each for AO, bent normals, thickness (AO and bent normals "
                                    "share one traversal)",
@@ -427,6 +428,7 @@ def main():
     ap.add_argument("--impl", default="fornos", choices=["fornos", "reference"])
     ap.add_argument("--workload", default="plane2048", choices=list(WORKLOADS))
     ap.add_argument("--traverse", default="auto", choices=list(TRAVERSE))
+    ap.add_argument("--schedule", default="auto", choices=list(SCHEDULE))
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -19,6 +19,7 @@ MISS = 0xFFFFFFFF
 # kinds (include/fornos_gpu.h)
 AO, BN, THICK, AO_BN = 0, 1, 2, 3
 TRAVERSE_AUTO, TRAVERSE_ORDERED, TRAVERSE_SKIP = 0, 1, 2
+SCHEDULE_STATIC, SCHEDULE_DYNAMIC = 0x10, 0x20  # or-ed into `traverse`
 GATHER_HEIGHT, GATHER_POSITION, GATHER_NORMAL = 0, 1, 2
 MAP_SMOOTH, MAP_LOWPOLY_NORMALS, MAP_HYBRID = 0, 1, 2
 SOLVER_HEIGHT, SOLVER_POSITION, SOLVER_NORMALS, SOLVER_AO, SOLVER_BENT_NORMALS, SOLVER_THICKNESS = range(6)

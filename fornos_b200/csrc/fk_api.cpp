@@ -37,8 +37,9 @@ int fk_hemisphere(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk
     return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: null argument");
   if (kind < FK_AO || kind > FK_AO_BN) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown kind");
   if (prm->sample_count == 0 || prm->perm_count == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: zero samples");
-  if (traverse < FK_TRAVERSE_AUTO || traverse > FK_TRAVERSE_SKIP)
-    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown traversal");
+  if ((traverse & ~(FK_TRAVERSE_MASK | FK_SCHEDULE_MASK)) || (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_SKIP ||
+      (traverse & FK_SCHEDULE_MASK) > FK_SCHEDULE_DYNAMIC)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown traversal or schedule");
   uint64_t end = (uint64_t)offset + count;
   if (!fits(coords, 16 * end) || !fits(tidx, 4 * end)) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: mapping buffers too small");
   if (!fits(samples, 16ull * prm->sample_count * prm->perm_count))

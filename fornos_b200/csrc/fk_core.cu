@@ -42,6 +42,20 @@ uint32_t* fk_take_counter(fk_ctx* ctx) {
   return c;
 }
 
+void* fk_scratch(fk_ctx* ctx, size_t bytes) {
+  if (bytes <= ctx->scratch_bytes) return ctx->scratch;
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->scratch) cudaFree(ctx->scratch);
+  ctx->scratch = nullptr;
+  ctx->scratch_bytes = 0;
+  if (cudaMalloc(&ctx->scratch, bytes) != cudaSuccess) {
+    ctx->scratch = nullptr;
+    return nullptr;
+  }
+  ctx->scratch_bytes = bytes;
+  return ctx->scratch;
+}
+
 extern "C" {
 
 int fk_ctx_create(int device, fk_ctx** out) {
@@ -85,6 +99,7 @@ int fk_ctx_destroy(fk_ctx* ctx) {
   for (fk_texel_map* m : std::set<fk_texel_map*>(ctx->maps)) fk_texel_map_free(ctx, m);
   cudaFree(ctx->counters);
   cudaFree(ctx->status);
+  cudaFree(ctx->scratch);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return FK_OK;

@@ -24,6 +24,8 @@ struct fk_ctx {
   uint32_t counter_slots = 0;
   uint32_t next_counter = 0;
   int* status = nullptr;          // device status word (limits a kernel could not honour)
+  void* scratch = nullptr;        // see fk_scratch
+  size_t scratch_bytes = 0;
   std::set<fk_buf*> bufs;
   std::set<fk_scene*> scenes;
   std::set<fk_texel_map*> maps;
@@ -82,6 +84,10 @@ void fk_dev_free(void* p);
 // Reserves a zeroed device counter for one persistent-kernel launch.
 uint32_t* fk_take_counter(fk_ctx* ctx);
 
+// Context-owned device scratch of at least `bytes` (grown on demand, kept for
+// later calls; growing waits for the stream).  Null on allocation failure.
+void* fk_scratch(fk_ctx* ctx, size_t bytes);
+
 // Kernel launchers (fk_*.cu).
 namespace fk {
 int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, uint32_t offset, uint32_t count,
@@ -100,6 +106,7 @@ struct HemiLaunch {
   uint32_t* hits0;
   uint32_t* hits1;
   unsigned long long* tally = nullptr;  // non-null: counting variant
+  uint32_t refill = 0;                  // dynamic schedule: idle lanes that trigger a refill (0 = default)
 };
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h);
 int launch_gather(fk_ctx* ctx, const fk_scene* s, int kind, const float4* coords, const uint32_t* tidx,

@@ -17,6 +17,8 @@
 //           leaf box's entry distance (grazing hits on box faces).
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "fk_device.cuh"
 #include "fk_internal.h"
 
@@ -367,6 +369,9 @@ static int run_hemi(fk_ctx* ctx, const HemiArgs& a) {
   return fk_after_launch(ctx, "hemi_kernel");
 }
 
+template <int KIND, int TRAV>
+static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill);
+
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   HemiArgs a;
   a.s = dev_of(s);
@@ -386,13 +391,19 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   a.queue = fk_take_counter(ctx);
   a.status = ctx->status;
   a.tally = h.tally;
-  int trav = h.traverse;
+  int trav = h.traverse & FK_TRAVERSE_MASK;
+  int sched = h.traverse & FK_SCHEDULE_MASK;
   if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= (uint32_t)kStack ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
   if (trav == FK_TRAVERSE_ORDERED && s->depth > (uint32_t)kStack)
     return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 64; use FK_TRAVERSE_SKIP");
-#define FK_HEMI_CASE(K)                                                        \
-  case K:                                                                      \
-    return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a) \
+  if (sched == 0) sched = FK_SCHEDULE_DYNAMIC;
+  const uint32_t refill = h.refill ? h.refill : 8;
+#define FK_HEMI_CASE(K)                                                                              \
+  case K:                                                                                            \
+    if (sched == FK_SCHEDULE_DYNAMIC)                                                                \
+      return trav == FK_TRAVERSE_ORDERED ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill)  \
+                                         : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill);    \
+    return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a)                    \
                                        : run_hemi<K, FK_TRAVERSE_SKIP>(ctx, a);
   switch (h.kind) {
     FK_HEMI_CASE(FK_AO)
@@ -403,6 +414,312 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
       return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown kind");
   }
 #undef FK_HEMI_CASE
+}
+
+// ------------------------------------------------------------------ hemisphere, dynamic
+// Rays are scheduled one per lane from an atomic queue: whenever at least
+// `refill` lanes of a warp are idle, one elected lane takes that many ray ids
+// with a single atomicAdd and the idle lanes (ranked by ballot) start them.
+// Lanes therefore stay busy while long rays of the same texel finish, and the
+// per-ray closest distances land in a scratch array.  A second kernel folds
+// each texel's samples in sample order, exactly as the *_step2 shaders do.
+
+struct DynArgs {
+  SceneDev s;
+  const float4* __restrict__ samples;
+  const float4* __restrict__ coords;
+  const uint32_t* __restrict__ tidx;
+  uint32_t spp, perms, texel0;  // rays [0, total) cover texels texel0 ...
+  uint32_t total;
+  uint32_t refill;
+  float lo, hi;
+  float* __restrict__ scratch;  // one distance per ray
+  uint32_t* queue;
+  int* status;
+  unsigned long long* tally;
+};
+
+// Ordered traversal, one inner node per call.  Returns true when finished.
+template <int STOP, bool COUNT>
+__device__ __forceinline__ bool ordered_step(const SceneDev& s, f3 o, f3 d, float lo, float hi, float& best,
+                                             int32_t& cur, int& sp, int32_t* stack_node, float* stack_dist,
+                                             int* status, Tally& tally) {
+  const float4* w = s.wide + 4 * (size_t)cur;
+  float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
+  float dist[2];
+  dist[0] = ray_box(o, d, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y));
+  dist[1] = ray_box(o, d, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w));
+  if (COUNT) tally.box += 2;
+  int32_t ref[2] = {__float_as_int(w3.x), __float_as_int(w3.y)};
+  int32_t cnt[2] = {__float_as_int(w3.z), __float_as_int(w3.w)};
+  int first = dist[1] < dist[0] ? 1 : 0;
+  int32_t next = -1;
+#pragma unroll
+  for (int q = 0; q < 2; ++q) {
+    int c = q == 0 ? first : 1 - first;
+    if (!(dist[c] < fminf(best, hi))) continue;
+    if (cnt[c] > 0) {
+      uint32_t t0 = (uint32_t)ref[c];
+      if (COUNT) tally.tri += (uint32_t)cnt[c];
+      for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s.rec, t, o, d, lo, best);
+      if (settled<STOP>(best, hi)) return true;
+    } else if (next < 0) {
+      next = ref[c];
+    } else {
+      if (sp >= kStack) {
+        atomicOr(status, 1);
+        return true;
+      }
+      stack_node[sp] = ref[c];
+      stack_dist[sp] = dist[c];
+      ++sp;
+    }
+  }
+  if (next >= 0) {
+    cur = next;
+    return false;
+  }
+  while (sp > 0) {
+    --sp;
+    if (stack_dist[sp] < fminf(best, hi)) {
+      cur = stack_node[sp];
+      return false;
+    }
+  }
+  return true;
+}
+
+// Skip-pointer walk, one flattened node per call.
+template <int STOP, bool COUNT>
+__device__ __forceinline__ bool skip_step(const SceneDev& s, f3 o, f3 d, float lo, float hi, float& best, int32_t& cur,
+                                          Tally& tally) {
+  uint32_t i = (uint32_t)cur;
+  float4 L = __ldg(s.node_lo + i), H = __ldg(s.node_hi + i);
+  float a = ray_box(o, d, xyz(L), xyz(H));
+  if (COUNT) tally.box++;
+  if (a < best && a < hi) {
+    uint32_t e = as_u32(H.w);
+    if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
+    for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
+    if (settled<STOP>(best, hi)) return true;
+    ++i;
+  } else {
+    i = __ldg(s.node_jump + i);
+  }
+  cur = (int32_t)i;
+  return i >= s.node_count;
+}
+
+template <int KIND, int TRAV, bool COUNT>
+__global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
+  constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lower = (1u << lane) - 1u;
+  int32_t stack_node[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
+  float stack_dist[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
+  Tally tally;
+  bool active = false, exhausted = false;
+  uint32_t r = 0;
+  f3 o = mk3(0.0f, 0.0f, 0.0f), dir = o;
+  float best = FLT_MAX;
+  int32_t cur = 0;
+  int sp = 0;
+  for (;;) {
+    unsigned idle = __ballot_sync(full, !active);
+    if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
+      const uint32_t n_idle = __popc(idle);
+      const int leader = __ffs(idle) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(p.queue, n_idle);
+      base = __shfl_sync(full, base, leader);
+      if (base + n_idle >= p.total) exhausted = true;
+      if (!active) {
+        r = base + __popc(idle & lower);
+        if (r < p.total) {
+          const uint32_t g = p.texel0 + r / p.spp, k = r % p.spp;
+          const uint32_t id = __ldg(p.tidx + g);
+          best = FLT_MAX;
+          bool done = true;
+          if (id != kMiss && valid_hit(id, p.s.corner_count)) {
+            f3 d, tx, ty;
+            texel_frame(p.s, __ldg(p.coords + g), id, o, d, tx, ty);
+            if (KIND == FK_THICK) d = neg(d);
+            float4 rs = __ldg(p.samples + (size_t)(g % p.perms) * p.spp + k);
+            dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+            if (TRAV == FK_TRAVERSE_ORDERED) {
+              float4 L = __ldg(p.s.node_lo), H = __ldg(p.s.node_hi);
+              float a = ray_box(o, dir, xyz(L), xyz(H));
+              if (COUNT) tally.box++;
+              if (a < p.hi) {
+                if (p.s.root_is_leaf) {
+                  uint32_t e = as_u32(H.w);
+                  if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
+                  for (uint32_t q = as_u32(L.w); q < e; q += 3) tri_sample(p.s.rec, q / 3, o, dir, p.lo, best);
+                } else {
+                  cur = 0;
+                  sp = 0;
+                  done = false;
+                }
+              }
+            } else {
+              cur = 0;
+              done = false;
+            }
+          } else if (id != kMiss) {
+            atomicOr(p.status, 2);
+          }
+          if (done) p.scratch[r] = best;
+          else active = true;
+        }
+      }
+      idle = __ballot_sync(full, !active);
+    }
+    if (exhausted && idle == full) break;
+    if (active) {
+      bool fin = TRAV == FK_TRAVERSE_ORDERED
+                     ? ordered_step<STOP, COUNT>(p.s, o, dir, p.lo, p.hi, best, cur, sp, stack_node, stack_dist,
+                                                 p.status, tally)
+                     : skip_step<STOP, COUNT>(p.s, o, dir, p.lo, p.hi, best, cur, tally);
+      if (fin) {
+        p.scratch[r] = best;
+        active = false;
+      }
+    }
+  }
+  if (COUNT) {
+    unsigned long long b = tally.box, t = tally.tri;
+    for (int off = 16; off > 0; off >>= 1) {
+      b += __shfl_down_sync(full, b, off);
+      t += __shfl_down_sync(full, t, off);
+    }
+    if (lane == 0) {
+      atomicAdd(p.tally, b);
+      atomicAdd(p.tally + 1, t);
+    }
+  }
+}
+
+// Folds each texel's per-sample distances in sample order (the *_step2
+// shaders' sequential sums), one warp per texel.
+template <int KIND>
+__global__ void __launch_bounds__(256) hemi_reduce_kernel(HemiArgs p, const float* __restrict__ scratch,
+                                                          uint32_t texel0) {
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < p.count; item += warps) {
+    const uint32_t g = texel0 + item;
+    uint32_t id = __ldg(p.tidx + g);
+    if (id != kMiss && !valid_hit(id, p.s.corner_count)) id = kMiss;
+    if (id == kMiss) {
+      if (lane == 0) {
+        if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = 1.0f;
+        if (KIND == FK_THICK) p.out0[g] = p.hi;
+        float* bn = KIND == FK_BN ? p.out0 : (KIND == FK_AO_BN ? p.out1 : nullptr);
+        if (bn) { bn[3 * (size_t)g] = 0.0f; bn[3 * (size_t)g + 1] = 0.0f; bn[3 * (size_t)g + 2] = 0.0f; }
+        if (p.hits0) p.hits0[g] = 0;
+        if (p.hits1) p.hits1[g] = 0;
+      }
+      continue;
+    }
+    f3 o, d, tx, ty;
+    if (KIND == FK_BN || KIND == FK_AO_BN) texel_frame(p.s, __ldg(p.coords + g), id, o, d, tx, ty);
+    const float4* row = p.samples + (size_t)(g % p.perms) * p.spp;
+    const float* ts = scratch + (size_t)item * p.spp;
+    uint32_t occ = 0, anyhit = 0;
+    float acc = 0.0f;
+    f3 vacc = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t k0 = 0; k0 < p.spp; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      const bool active = k < p.spp;
+      const float t = active ? ts[k] : FLT_MAX;
+      const bool hit = active && t != FLT_MAX;
+      if (KIND == FK_AO || KIND == FK_AO_BN) occ += __popc(__ballot_sync(full, hit && t < p.hi));
+      anyhit += __popc(__ballot_sync(full, hit));
+      const int nact = (int)min(32u, p.spp - k0);
+      if (KIND == FK_BN || KIND == FK_AO_BN) {
+        f3 v = mk3(0.0f, 0.0f, 0.0f);
+        if (active && !hit) {
+          float4 rs = __ldg(row + k);
+          v = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+        }
+        for (int j = 0; j < nact; ++j) {
+          vacc.x = __fadd_rn(vacc.x, __shfl_sync(full, v.x, j));
+          vacc.y = __fadd_rn(vacc.y, __shfl_sync(full, v.y, j));
+          vacc.z = __fadd_rn(vacc.z, __shfl_sync(full, v.z, j));
+        }
+      }
+      if (KIND == FK_THICK) {
+        float v = hit ? t : p.hi;
+        for (int j = 0; j < nact; ++j) acc = __fadd_rn(acc, __shfl_sync(full, v, j));
+      }
+    }
+    if (lane == 0) {
+      const float fs = (float)p.spp;
+      if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = __fsub_rn(1.0f, __fdiv_rn((float)occ, fs));
+      if (KIND == FK_THICK) p.out0[g] = __fdiv_rn(acc, fs);
+      if (KIND == FK_BN || KIND == FK_AO_BN) {
+        float* bn = KIND == FK_BN ? p.out0 : p.out1;
+        f3 v = normalize(vacc);
+        bn[3 * (size_t)g] = v.x;
+        bn[3 * (size_t)g + 1] = v.y;
+        bn[3 * (size_t)g + 2] = v.z;
+      }
+      if (KIND == FK_AO_BN) {
+        if (p.hits0) p.hits0[g] = occ;
+        if (p.hits1) p.hits1[g] = anyhit;
+      } else if (p.hits0) {
+        p.hits0[g] = KIND == FK_AO ? occ : anyhit;
+      }
+    }
+  }
+}
+
+template <int KIND, int TRAV>
+static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill) {
+  auto trace = a.tally ? hemi_trace_kernel<KIND, TRAV, true> : hemi_trace_kernel<KIND, TRAV, false>;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace, 256, 0);
+  if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "occupancy");
+  if (per_sm < 1) per_sm = 1;
+  // Scratch: one float per ray, texels processed in chunks that fit it.
+  const uint64_t max_rays = 1ull << 27;  // 512 MB of distances
+  uint32_t chunk = (uint32_t)std::min<uint64_t>(a.count, std::max<uint64_t>(1, max_rays / a.spp));
+  float* scratch = (float*)fk_scratch(ctx, (size_t)chunk * a.spp * sizeof(float));
+  if (!scratch) return fk_fail(ctx, FK_ERR_NOMEM, "hemisphere scratch allocation failed");
+  for (uint32_t done = 0; done < a.count; done += chunk) {
+    uint32_t n = std::min(chunk, a.count - done);
+    DynArgs d;
+    d.s = a.s;
+    d.samples = a.samples;
+    d.coords = a.coords;
+    d.tidx = a.tidx;
+    d.spp = a.spp;
+    d.perms = a.perms;
+    d.texel0 = a.offset + done;
+    d.total = n * a.spp;
+    d.refill = refill;
+    d.lo = a.lo;
+    d.hi = a.hi;
+    d.scratch = scratch;
+    d.queue = fk_take_counter(ctx);
+    d.status = a.status;
+    d.tally = a.tally;
+    uint32_t blocks = (uint32_t)ctx->sm_count * (uint32_t)per_sm;
+    uint32_t need = (d.total + 255) / 256;
+    if (blocks > need) blocks = need;
+    trace<<<blocks, 256, 0, ctx->stream>>>(d);
+    int rc = fk_after_launch(ctx, "hemi_trace_kernel");
+    if (rc != FK_OK) return rc;
+    HemiArgs r = a;
+    r.count = n;
+    uint32_t rblocks = std::min<uint32_t>((n + 7) / 8, (uint32_t)ctx->sm_count * 8);
+    hemi_reduce_kernel<KIND><<<rblocks, 256, 0, ctx->stream>>>(r, scratch, d.texel0);
+    rc = fk_after_launch(ctx, "hemi_reduce_kernel");
+    if (rc != FK_OK) return rc;
+  }
+  return FK_OK;
 }
 
 // ------------------------------------------------------------------ mesh mapping

@@ -191,6 +191,11 @@ typedef struct fk_sample_params {
 #define FK_TRAVERSE_AUTO 0    /* tuned choice for the scene */
 #define FK_TRAVERSE_ORDERED 1 /* near-first stack traversal over the BVH2 layout */
 #define FK_TRAVERSE_SKIP 2    /* the reference's skip-pointer walk, node order */
+#define FK_TRAVERSE_MASK 0x0F
+/* Ray scheduling, or-ed into the traversal argument (0 = tuned choice). */
+#define FK_SCHEDULE_STATIC 0x10  /* one warp per texel, lanes = samples */
+#define FK_SCHEDULE_DYNAMIC 0x20 /* lanes refilled with rays from a queue */
+#define FK_SCHEDULE_MASK 0xF0
 
 /* Hemisphere sampling for texels [offset, offset + count) (global indices
  * into coords / tidx).  Outputs, indexed by texel:

@@ -58,7 +58,12 @@ def pixt12(cmap):
 
 
 def bits(a):
-    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+    """Bit patterns with every NaN mapped to one value: x86 and CUDA produce
+    different NaN payloads for the same invalid operation (e.g. 0 * inf in
+    normalize of a zero tangent), which carries no information."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).copy()
+    u[np.isnan(np.asarray(a, np.float32))] = 0x7FC00000
+    return u
 
 
 def same_bits(a, b):

@@ -110,11 +110,12 @@ def oracle_hemi(oracle, c, mm, kind, samples, spp, lo, hi):
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK])
 @pytest.mark.parametrize("spp", [16, 40])
-def test_hemisphere_skip_is_bit_exact(ctx, oracle, name, kind, spp):
+@pytest.mark.parametrize("sched", [api.SCHEDULE_STATIC, api.SCHEDULE_DYNAMIC])
+def test_hemisphere_skip_is_bit_exact(ctx, oracle, name, kind, spp, sched):
     c = case(name)
     _, _, mm = mapped(ctx, oracle, c)
     lo, hi = 0.001, 0.3
-    samples, (out, hits) = run_hemi(ctx, mm, kind, spp, lo, hi, api.TRAVERSE_SKIP)
+    samples, (out, hits) = run_hemi(ctx, mm, kind, spp, lo, hi, api.TRAVERSE_SKIP | sched)
     ref, rhits, tidx = oracle_hemi(oracle, c, mm, kind, samples, spp, lo, hi)
     hit = tidx != api.MISS
     assert hit.mean() > 0.5
@@ -127,11 +128,12 @@ def test_hemisphere_skip_is_bit_exact(ctx, oracle, name, kind, spp):
 
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK])
-def test_hemisphere_ordered_matches(ctx, oracle, name, kind):
+@pytest.mark.parametrize("sched", [api.SCHEDULE_STATIC, api.SCHEDULE_DYNAMIC])
+def test_hemisphere_ordered_matches(ctx, oracle, name, kind, sched):
     c = case(name)
     _, _, mm = mapped(ctx, oracle, c)
     spp, lo, hi = 32, 0.001, 0.3
-    samples, (out, hits) = run_hemi(ctx, mm, kind, spp, lo, hi, api.TRAVERSE_ORDERED)
+    samples, (out, hits) = run_hemi(ctx, mm, kind, spp, lo, hi, api.TRAVERSE_ORDERED | sched)
     ref, rhits, tidx = oracle_hemi(oracle, c, mm, kind, samples, spp, lo, hi)
     hit = tidx != api.MISS
     exact_hits = hits[hit] == rhits[hit]
@@ -148,11 +150,12 @@ def test_ao_bn_fused_equals_separate(ctx, oracle):
     c = case("plane")
     _, _, mm = mapped(ctx, oracle, c)
     spp, lo, hi = 48, 0.001, 0.3
-    _, (ao, aoh) = run_hemi(ctx, mm, api.AO, spp, lo, hi, api.TRAVERSE_SKIP)
-    _, (bn, bnh) = run_hemi(ctx, mm, api.BN, spp, lo, hi, api.TRAVERSE_SKIP)
-    _, (fa, fah, fb, fbh) = run_hemi(ctx, mm, api.AO_BN, spp, lo, hi, api.TRAVERSE_SKIP)
-    assert same_bits(ao, fa) and np.array_equal(aoh, fah)
-    assert same_bits(bn, fb) and np.array_equal(bnh, fbh)
+    for sched in (api.SCHEDULE_STATIC, api.SCHEDULE_DYNAMIC):
+        _, (ao, aoh) = run_hemi(ctx, mm, api.AO, spp, lo, hi, api.TRAVERSE_SKIP | sched)
+        _, (bn, bnh) = run_hemi(ctx, mm, api.BN, spp, lo, hi, api.TRAVERSE_SKIP | sched)
+        _, (fa, fah, fb, fbh) = run_hemi(ctx, mm, api.AO_BN, spp, lo, hi, api.TRAVERSE_SKIP | sched)
+        assert same_bits(ao, fa) and np.array_equal(aoh, fah)
+        assert same_bits(bn, fb) and np.array_equal(bnh, fbh)
 
 
 @pytest.mark.parametrize("name", list(CASES))
