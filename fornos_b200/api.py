@@ -20,6 +20,7 @@ MISS = 0xFFFFFFFF
 AO, BN, THICK, AO_BN = 0, 1, 2, 3
 TRAVERSE_AUTO, TRAVERSE_ORDERED, TRAVERSE_SKIP = 0, 1, 2
 SCHEDULE_STATIC, SCHEDULE_DYNAMIC = 0x10, 0x20  # or-ed into `traverse`
+EXACT_BOX_TESTS = 0x100  # or-ed into `traverse`: divide in every box test
 GATHER_HEIGHT, GATHER_POSITION, GATHER_NORMAL = 0, 1, 2
 MAP_SMOOTH, MAP_LOWPOLY_NORMALS, MAP_HYBRID = 0, 1, 2
 SOLVER_HEIGHT, SOLVER_POSITION, SOLVER_NORMALS, SOLVER_AO, SOLVER_BENT_NORMALS, SOLVER_THICKNESS = range(6)

@@ -37,7 +37,8 @@ int fk_hemisphere(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk
     return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: null argument");
   if (kind < FK_AO || kind > FK_AO_BN) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown kind");
   if (prm->sample_count == 0 || prm->perm_count == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: zero samples");
-  if ((traverse & ~(FK_TRAVERSE_MASK | FK_SCHEDULE_MASK)) || (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_SKIP ||
+  if ((traverse & ~(FK_TRAVERSE_MASK | FK_SCHEDULE_MASK | FK_EXACT_BOX_TESTS)) ||
+      (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_SKIP ||
       (traverse & FK_SCHEDULE_MASK) > FK_SCHEDULE_DYNAMIC)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown traversal or schedule");
   uint64_t end = (uint64_t)offset + count;

@@ -2,6 +2,7 @@
 // (include/fornos_gpu.h).  Replaces the GL buffer layer: ComputeBuffer<T>
 // (Src/compute.h:37-87) and the uploads of MeshMapping::init
 // (Src/meshmapping.cpp:128-184).
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <vector>
@@ -247,6 +248,18 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   s->leaf_count = leaves;
   s->wide_count = nw;
   s->root_is_leaf = nodes[0].jump == 1;
+  // The filtered box test assumes |box - origin| < 2^26; ray origins lie on
+  // the scene's triangles, so box and corner coordinates below 2^24 suffice.
+  {
+    const float lim = 16777216.0f;
+    bool ok = true;
+    for (uint32_t i = 0; i < nn && ok; ++i)
+      for (int a = 0; a < 3; ++a)
+        ok = ok && std::fabs(nodes[i].aabb_min[a]) < lim && std::fabs(nodes[i].aabb_max[a]) < lim;
+    for (size_t i = 0; i < (size_t)nc && ok; ++i)
+      for (int a = 0; a < 3; ++a) ok = ok && std::fabs(pos4[4 * i + a]) < lim;
+    s->filter_ok = ok ? 1 : 0;
+  }
   size_t nb = sizeof(float4) * nn, cb = sizeof(float4) * (size_t)nc;
   int rc = FK_OK;
   auto up = [&](void** dst, const void* src, size_t bytes) {

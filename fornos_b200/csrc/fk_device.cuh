@@ -51,6 +51,65 @@ __device__ __forceinline__ float ray_box(f3 o, f3 d, f3 lo, f3 hi) {
   return (b >= 0.0f && a <= b) ? a : FLT_MAX;
 }
 
+// Filtered form of ray_box for a ray traced many times against boxes: the
+// six slab quotients q = fl(num / d) are replaced by q' = fl(num * fl(1 / d)).
+// For d != 0 with |d| >= 2^-100 and |num| < 2^26, |q' - q| <= 2^-22 |q'| +
+// 2^-125 (two roundings of relative size 2^-24 each, one more for q itself,
+// and an absolute term for subnormal quotients); for d = 0 both forms give
+// the same +-inf or NaN.  min / max keep that bound for the entry and exit
+// distances a, b.  A decision (b >= 0, a <= b, a < thr) is taken from a', b'
+// only when it holds with those margins; otherwise the exact quotients decide.
+// The outcome is therefore always that of ray_box(o, d, lo, hi) < thr.
+struct RayPre {
+  f3 o, d, inv;
+  bool exact_only;  // some |d| is nonzero but below 2^-100: always divide
+};
+
+__device__ __forceinline__ RayPre ray_pre(f3 o, f3 d) {
+  RayPre r;
+  r.o = o;
+  r.d = d;
+  r.inv = mk3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+  const float tiny = 7.8886091e-31f;  // 2^-100
+  r.exact_only = (d.x != 0.0f && fabsf(d.x) < tiny) || (d.y != 0.0f && fabsf(d.y) < tiny) ||
+                 (d.z != 0.0f && fabsf(d.z) < tiny);
+  return r;
+}
+
+__device__ __forceinline__ float slack(float v) {
+  // bound on |exact - filtered| for a filtered slab value v (0 when v is inf / NaN,
+  // where both forms agree exactly)
+  float s = __fadd_rn(__fmul_rn(fabsf(v), 4.76837158e-07f), 2.3509887e-38f);  // 2^-21 |v| + 2^-125
+  return isfinite(v) ? s : 0.0f;
+}
+
+// Returns ray_box(o, d, lo, hi) < thr exactly, and in `entry` the filtered
+// entry distance (for ordering / deferred culling only).
+__device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
+  f3 n1 = sub(lo, r.o), n2 = sub(hi, r.o);
+  if (!r.exact_only) {
+    f3 t1 = mk3(__fmul_rn(n1.x, r.inv.x), __fmul_rn(n1.y, r.inv.y), __fmul_rn(n1.z, r.inv.z));
+    f3 t2 = mk3(__fmul_rn(n2.x, r.inv.x), __fmul_rn(n2.y, r.inv.y), __fmul_rn(n2.z, r.inv.z));
+    f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
+    float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
+    float b = fminf(tx.x, fminf(tx.y, tx.z));
+    entry = a;
+    float sa = slack(a), sb = slack(b);
+    // certain rejections
+    if (__fadd_rn(b, sb) < 0.0f) return false;
+    if (__fsub_rn(a, sa) > __fadd_rn(b, sb)) return false;
+    if (__fsub_rn(a, sa) >= thr) return false;
+    // certain acceptance (NaN a or b never qualifies)
+    if (__fsub_rn(b, sb) >= 0.0f && __fadd_rn(a, sa) <= __fsub_rn(b, sb) && __fadd_rn(a, sa) < thr) return true;
+  }
+  f3 t1 = divv(n1, r.d), t2 = divv(n2, r.d);
+  f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
+  float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
+  float b = fminf(tx.x, fminf(tx.y, tx.z));
+  entry = a;
+  return ((b >= 0.0f && a <= b) ? a : FLT_MAX) < thr;
+}
+
 // Binary64 barycentric of Shaders/meshmapping_nobackfaces.comp:48-62.
 __device__ __forceinline__ f3 bary_f64(f3 p, f3 a, f3 b, f3 c) {
   double ax = a.x, ay = a.y, az = a.z;

@@ -53,6 +53,7 @@ struct fk_scene {
   uint32_t wide_count = 0;
   float4* tri_rec = nullptr;
   uint32_t root_is_leaf = 0;
+  uint32_t filter_ok = 0;        // every coordinate below 2^24 in magnitude
   size_t bytes = 0;
 };
 

@@ -35,6 +35,7 @@ struct SceneDev {
   uint32_t node_count;
   uint32_t root_is_leaf;
   uint32_t corner_count;
+  uint32_t filter_ok;  // scene coordinates small enough for the filtered box test
 };
 
 // A hit index read from a caller's buffer: a miss, or the first corner of a
@@ -55,6 +56,7 @@ static SceneDev dev_of(const fk_scene* s) {
   d.node_count = s->node_count;
   d.root_is_leaf = s->root_is_leaf;
   d.corner_count = s->corner_count;
+  d.filter_ok = s->filter_ok;
   return d;
 }
 
@@ -370,7 +372,7 @@ static int run_hemi(fk_ctx* ctx, const HemiArgs& a) {
 }
 
 template <int KIND, int TRAV>
-static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill);
+static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter);
 
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   HemiArgs a;
@@ -398,11 +400,12 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
     return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 64; use FK_TRAVERSE_SKIP");
   if (sched == 0) sched = FK_SCHEDULE_DYNAMIC;
   const uint32_t refill = h.refill ? h.refill : 8;
+  const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
 #define FK_HEMI_CASE(K)                                                                              \
   case K:                                                                                            \
     if (sched == FK_SCHEDULE_DYNAMIC)                                                                \
-      return trav == FK_TRAVERSE_ORDERED ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill)  \
-                                         : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill);    \
+      return trav == FK_TRAVERSE_ORDERED ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill, filter) \
+                                         : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill, filter);   \
     return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a)                    \
                                        : run_hemi<K, FK_TRAVERSE_SKIP>(ctx, a);
   switch (h.kind) {
@@ -439,16 +442,37 @@ struct DynArgs {
   unsigned long long* tally;
 };
 
+// Child box test of the traversal kernels: exact quotients, or the filtered
+// form (fk_device.cuh: box_hit) whose decision is provably the same.
+template <bool FILTER>
+__device__ __forceinline__ bool child_hit(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
+  if (FILTER) return box_hit(r, lo, hi, thr, entry);
+  entry = ray_box(r.o, r.d, lo, hi);
+  return entry < thr;
+}
+
+// Deferred node still worth visiting: exact distances compare directly;
+// filtered ones only cull when certainly at or beyond the threshold.
+template <bool FILTER>
+__device__ __forceinline__ bool still_open(float entry, float thr) {
+  if (FILTER) return __fsub_rn(entry, slack(entry)) < thr;
+  return entry < thr;
+}
+
 // Ordered traversal, one inner node per call.  Returns true when finished.
-template <int STOP, bool COUNT>
-__device__ __forceinline__ bool ordered_step(const SceneDev& s, f3 o, f3 d, float lo, float hi, float& best,
+template <int STOP, bool COUNT, bool FILTER>
+__device__ __forceinline__ bool ordered_step(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
                                              int32_t& cur, int& sp, int32_t* stack_node, float* stack_dist,
                                              int* status, Tally& tally) {
   const float4* w = s.wide + 4 * (size_t)cur;
   float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
+  const f3 blo[2] = {mk3(w0.x, w0.z, w2.x), mk3(w1.x, w1.z, w2.z)};
+  const f3 bhi[2] = {mk3(w0.y, w0.w, w2.y), mk3(w1.y, w1.w, w2.w)};
+  const float thr0 = fminf(best, hi);
   float dist[2];
-  dist[0] = ray_box(o, d, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y));
-  dist[1] = ray_box(o, d, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w));
+  bool hit[2];
+  hit[0] = child_hit<FILTER>(rp, blo[0], bhi[0], thr0, dist[0]);
+  hit[1] = child_hit<FILTER>(rp, blo[1], bhi[1], thr0, dist[1]);
   if (COUNT) tally.box += 2;
   int32_t ref[2] = {__float_as_int(w3.x), __float_as_int(w3.y)};
   int32_t cnt[2] = {__float_as_int(w3.z), __float_as_int(w3.w)};
@@ -457,11 +481,13 @@ __device__ __forceinline__ bool ordered_step(const SceneDev& s, f3 o, f3 d, floa
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     int c = q == 0 ? first : 1 - first;
-    if (!(dist[c] < fminf(best, hi))) continue;
+    if (!hit[c]) continue;
+    // the threshold may have dropped while the nearer child was processed
+    if (q == 1 && fminf(best, hi) < thr0 && !child_hit<FILTER>(rp, blo[c], bhi[c], fminf(best, hi), dist[c])) continue;
     if (cnt[c] > 0) {
       uint32_t t0 = (uint32_t)ref[c];
       if (COUNT) tally.tri += (uint32_t)cnt[c];
-      for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s.rec, t, o, d, lo, best);
+      for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s.rec, t, rp.o, rp.d, lo, best);
       if (settled<STOP>(best, hi)) return true;
     } else if (next < 0) {
       next = ref[c];
@@ -481,7 +507,7 @@ __device__ __forceinline__ bool ordered_step(const SceneDev& s, f3 o, f3 d, floa
   }
   while (sp > 0) {
     --sp;
-    if (stack_dist[sp] < fminf(best, hi)) {
+    if (still_open<FILTER>(stack_dist[sp], fminf(best, hi))) {
       cur = stack_node[sp];
       return false;
     }
@@ -490,17 +516,18 @@ __device__ __forceinline__ bool ordered_step(const SceneDev& s, f3 o, f3 d, floa
 }
 
 // Skip-pointer walk, one flattened node per call.
-template <int STOP, bool COUNT>
-__device__ __forceinline__ bool skip_step(const SceneDev& s, f3 o, f3 d, float lo, float hi, float& best, int32_t& cur,
-                                          Tally& tally) {
+template <int STOP, bool COUNT, bool FILTER>
+__device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
+                                          int32_t& cur, Tally& tally) {
   uint32_t i = (uint32_t)cur;
   float4 L = __ldg(s.node_lo + i), H = __ldg(s.node_hi + i);
-  float a = ray_box(o, d, xyz(L), xyz(H));
+  float entry;
+  bool h = child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry);
   if (COUNT) tally.box++;
-  if (a < best && a < hi) {
+  if (h) {
     uint32_t e = as_u32(H.w);
     if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
-    for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
+    for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, rp.o, rp.d, lo, best);
     if (settled<STOP>(best, hi)) return true;
     ++i;
   } else {
@@ -510,7 +537,7 @@ __device__ __forceinline__ bool skip_step(const SceneDev& s, f3 o, f3 d, float l
   return i >= s.node_count;
 }
 
-template <int KIND, int TRAV, bool COUNT>
+template <int KIND, int TRAV, bool COUNT, bool FILTER>
 __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
   constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
   const unsigned full = 0xFFFFFFFFu;
@@ -521,7 +548,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t r = 0;
-  f3 o = mk3(0.0f, 0.0f, 0.0f), dir = o;
+  RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX;
   int32_t cur = 0;
   int sp = 0;
@@ -542,11 +569,13 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
           best = FLT_MAX;
           bool done = true;
           if (id != kMiss && valid_hit(id, p.s.corner_count)) {
-            f3 d, tx, ty;
+            f3 o, d, tx, ty;
             texel_frame(p.s, __ldg(p.coords + g), id, o, d, tx, ty);
             if (KIND == FK_THICK) d = neg(d);
             float4 rs = __ldg(p.samples + (size_t)(g % p.perms) * p.spp + k);
-            dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+            f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+            rp = ray_pre(o, dir);
+            if (!p.s.filter_ok) rp.exact_only = true;
             if (TRAV == FK_TRAVERSE_ORDERED) {
               float4 L = __ldg(p.s.node_lo), H = __ldg(p.s.node_hi);
               float a = ray_box(o, dir, xyz(L), xyz(H));
@@ -578,9 +607,9 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
     if (exhausted && idle == full) break;
     if (active) {
       bool fin = TRAV == FK_TRAVERSE_ORDERED
-                     ? ordered_step<STOP, COUNT>(p.s, o, dir, p.lo, p.hi, best, cur, sp, stack_node, stack_dist,
-                                                 p.status, tally)
-                     : skip_step<STOP, COUNT>(p.s, o, dir, p.lo, p.hi, best, cur, tally);
+                     ? ordered_step<STOP, COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, cur, sp, stack_node, stack_dist,
+                                                         p.status, tally)
+                     : skip_step<STOP, COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, cur, tally);
       if (fin) {
         p.scratch[r] = best;
         active = false;
@@ -677,8 +706,9 @@ __global__ void __launch_bounds__(256) hemi_reduce_kernel(HemiArgs p, const floa
 }
 
 template <int KIND, int TRAV>
-static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill) {
-  auto trace = a.tally ? hemi_trace_kernel<KIND, TRAV, true> : hemi_trace_kernel<KIND, TRAV, false>;
+static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter) {
+  auto trace = a.tally ? (filter ? hemi_trace_kernel<KIND, TRAV, true, true> : hemi_trace_kernel<KIND, TRAV, true, false>)
+                       : (filter ? hemi_trace_kernel<KIND, TRAV, false, true> : hemi_trace_kernel<KIND, TRAV, false, false>);
   int per_sm = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace, 256, 0);
   if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "occupancy");

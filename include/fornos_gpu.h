@@ -196,6 +196,9 @@ typedef struct fk_sample_params {
 #define FK_SCHEDULE_STATIC 0x10  /* one warp per texel, lanes = samples */
 #define FK_SCHEDULE_DYNAMIC 0x20 /* lanes refilled with rays from a queue */
 #define FK_SCHEDULE_MASK 0xF0
+/* Divide for every ray-box slab instead of the filtered reciprocal form (the
+ * dynamic schedule's default), which takes the same decisions. */
+#define FK_EXACT_BOX_TESTS 0x100
 
 /* Hemisphere sampling for texels [offset, offset + count) (global indices
  * into coords / tidx).  Outputs, indexed by texel:

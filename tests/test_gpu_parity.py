@@ -110,7 +110,8 @@ def oracle_hemi(oracle, c, mm, kind, samples, spp, lo, hi):
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK])
 @pytest.mark.parametrize("spp", [16, 40])
-@pytest.mark.parametrize("sched", [api.SCHEDULE_STATIC, api.SCHEDULE_DYNAMIC])
+@pytest.mark.parametrize("sched", [api.SCHEDULE_STATIC, api.SCHEDULE_DYNAMIC,
+                                   api.SCHEDULE_DYNAMIC | api.EXACT_BOX_TESTS])
 def test_hemisphere_skip_is_bit_exact(ctx, oracle, name, kind, spp, sched):
     c = case(name)
     _, _, mm = mapped(ctx, oracle, c)
@@ -128,7 +129,8 @@ def test_hemisphere_skip_is_bit_exact(ctx, oracle, name, kind, spp, sched):
 
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK])
-@pytest.mark.parametrize("sched", [api.SCHEDULE_STATIC, api.SCHEDULE_DYNAMIC])
+@pytest.mark.parametrize("sched", [api.SCHEDULE_STATIC, api.SCHEDULE_DYNAMIC,
+                                   api.SCHEDULE_DYNAMIC | api.EXACT_BOX_TESTS])
 def test_hemisphere_ordered_matches(ctx, oracle, name, kind, sched):
     c = case(name)
     _, _, mm = mapped(ctx, oracle, c)
@@ -248,3 +250,18 @@ def test_errors_are_reported_not_fatal(ctx):
     mm.run()
     s.run()
     assert np.isfinite(s.get_results()[: tm.count]).all()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK, api.AO_BN])
+@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_SKIP])
+def test_filtered_box_tests_equal_exact(ctx, oracle, name, kind, trav):
+    """The reciprocal-filtered box test must take every decision the divided
+    one takes: outputs and counts are identical bit for bit."""
+    c = case(name)
+    _, _, mm = mapped(ctx, oracle, c)
+    spp, lo, hi = 24, 0.001, 0.3
+    _, a = run_hemi(ctx, mm, kind, spp, lo, hi, trav | api.SCHEDULE_DYNAMIC)
+    _, b = run_hemi(ctx, mm, kind, spp, lo, hi, trav | api.SCHEDULE_DYNAMIC | api.EXACT_BOX_TESTS)
+    for x, y in zip(a, b):
+        assert same_bits(x, y) if x.dtype == np.float32 else np.array_equal(x, y)
