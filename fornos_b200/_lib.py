@@ -38,6 +38,10 @@ class SolverParams(ctypes.Structure):
                 ("tangent_space", c_int), ("normalize_output", c_int), ("seed", c_u32), ("traverse", c_int)]
 
 
+class Tuning(ctypes.Structure):
+    _fields_ = [("refill", c_u32), ("leaf_batch", c_u32), ("speculate", c_u32), ("reserved", c_u32)]
+
+
 class SceneInfo(ctypes.Structure):
     _fields_ = [("node_count", c_u32), ("corner_count", c_u32), ("depth", c_u32), ("leaf_count", c_u32),
                 ("device_bytes", c_u64)]
@@ -71,6 +75,8 @@ _SIGS = {
     "fk_ctx_stream": (c_vp, [c_vp]),
     "fk_sync": (c_int, [c_vp]),
     "fk_launch_count": (c_u64, [c_vp]),
+    "fk_ctx_set_tuning": (c_int, [c_vp, ctypes.POINTER(Tuning)]),
+    "fk_ctx_get_tuning": (c_int, [c_vp, ctypes.POINTER(Tuning)]),
     "fk_buf_alloc": (c_int, [c_vp, c_size, ctypes.POINTER(c_vp)]),
     "fk_buf_upload": (c_int, [c_vp, c_vp, c_size, c_vp, c_size]),
     "fk_buf_download": (c_int, [c_vp, c_vp, c_size, c_vp, c_size]),

@@ -85,6 +85,15 @@ class Context:
     def launches(self):
         return int(self.lib.fk_launch_count(self.handle))
 
+    def set_tuning(self, refill=8, leaf_batch=16, speculate=0):
+        t = L.Tuning(refill, leaf_batch, speculate, 0)
+        _check(self.lib.fk_ctx_set_tuning(self.handle, ctypes.byref(t)), self, "fk_ctx_set_tuning")
+
+    def get_tuning(self):
+        t = L.Tuning()
+        _check(self.lib.fk_ctx_get_tuning(self.handle, ctypes.byref(t)), self)
+        return {"refill": t.refill, "leaf_batch": t.leaf_batch, "speculate": t.speculate}
+
     def buffer(self, nbytes):
         return Buffer(self, nbytes)
 

@@ -124,6 +124,20 @@ int fk_sync(fk_ctx* ctx) {
 
 uint64_t fk_launch_count(const fk_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
+int fk_ctx_set_tuning(fk_ctx* ctx, const fk_tuning* t) {
+  if (!ctx || !t) return FK_ERR_INVALID;
+  if (t->refill < 1 || t->refill > 32 || t->leaf_batch < 1 || t->leaf_batch > 32 || t->speculate > 1)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_ctx_set_tuning: refill and leaf_batch in 1..32, speculate 0 or 1");
+  ctx->tuning = *t;
+  return FK_OK;
+}
+
+int fk_ctx_get_tuning(const fk_ctx* ctx, fk_tuning* t) {
+  if (!ctx || !t) return FK_ERR_INVALID;
+  *t = ctx->tuning;
+  return FK_OK;
+}
+
 // ------------------------------------------------------------------ buffers
 int fk_buf_alloc(fk_ctx* ctx, size_t bytes, fk_buf** out) {
   if (!ctx || !out || bytes == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_alloc: zero size or null");
@@ -225,8 +239,10 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     int32_t ref[2], cnt[2];
     for (int k = 0; k < 2; ++k) {
       const fk_bvh_node& n = nodes[c[k]];
+      // inner child: its record index; leaf child: -(flattened node index + 1),
+      // the triangle range being that node's [start, end)
       if (wide_of[c[k]] >= 0) { ref[k] = wide_of[c[k]]; cnt[k] = 0; }
-      else { ref[k] = (int32_t)(n.start / 3); cnt[k] = (int32_t)((n.end - n.start) / 3); }
+      else { ref[k] = -(int32_t)c[k] - 1; cnt[k] = (int32_t)((n.end - n.start) / 3); }
     }
     const fk_bvh_node& L = nodes[c[0]];
     const fk_bvh_node& R = nodes[c[1]];

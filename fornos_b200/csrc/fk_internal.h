@@ -26,6 +26,7 @@ struct fk_ctx {
   int* status = nullptr;          // device status word (limits a kernel could not honour)
   void* scratch = nullptr;        // see fk_scratch
   size_t scratch_bytes = 0;
+  fk_tuning tuning = {8, 16, 0, 0};  // dynamic-schedule knobs (fk_ctx_set_tuning)
   std::set<fk_buf*> bufs;
   std::set<fk_scene*> scenes;
   std::set<fk_texel_map*> maps;
@@ -107,7 +108,9 @@ struct HemiLaunch {
   uint32_t* hits0;
   uint32_t* hits1;
   unsigned long long* tally = nullptr;  // non-null: counting variant
-  uint32_t refill = 0;                  // dynamic schedule: idle lanes that trigger a refill (0 = default)
+  uint32_t refill = 0;                  // dynamic schedule: idle lanes that trigger a refill (0 = context tuning)
+  uint32_t leaf_batch = 0;              // postponed leaves that start a leaf phase (0 = context tuning)
+  uint32_t speculate = 0;
 };
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h);
 int launch_gather(fk_ctx* ctx, const fk_scene* s, int kind, const float4* coords, const uint32_t* tidx,

@@ -151,6 +151,7 @@ __device__ float trace_skip(const SceneDev& s, f3 o, f3 d, float lo, float hi, T
 }
 
 static constexpr int kStack = 64;
+static constexpr uint32_t kMaxOrderedDepth = 48;  // deeper trees use the skip walk
 
 // Near-first traversal of the children-in-parent layout with the same
 // pruning rule.  The host selects it only when the tree depth fits kStack;
@@ -189,8 +190,8 @@ __device__ float trace_ordered(const SceneDev& s, f3 o, f3 d, float lo, float hi
     for (int q = 0; q < 2; ++q) {
       int c = q == 0 ? first : 1 - first;
       if (!(dist[c] < fminf(best, hi))) continue;
-      if (cnt[c] > 0) {
-        uint32_t t0 = (uint32_t)ref[c];
+      if (ref[c] < 0) {
+        uint32_t t0 = as_u32(__ldg(s.node_lo + (-ref[c] - 1)).w) / 3;
         if (COUNT) tally.tri += (uint32_t)cnt[c];
         for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s.rec, t, o, d, lo, best);
         if (settled<STOP>(best, hi)) return best;
@@ -372,7 +373,8 @@ static int run_hemi(fk_ctx* ctx, const HemiArgs& a) {
 }
 
 template <int KIND, int TRAV>
-static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter);
+static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter, uint32_t leaf_batch,
+                            uint32_t speculate);
 
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   HemiArgs a;
@@ -395,17 +397,20 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   a.tally = h.tally;
   int trav = h.traverse & FK_TRAVERSE_MASK;
   int sched = h.traverse & FK_SCHEDULE_MASK;
-  if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= (uint32_t)kStack ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
-  if (trav == FK_TRAVERSE_ORDERED && s->depth > (uint32_t)kStack)
-    return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 64; use FK_TRAVERSE_SKIP");
+  if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
+  if (trav == FK_TRAVERSE_ORDERED && s->depth > kMaxOrderedDepth)
+    return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 48; use FK_TRAVERSE_SKIP");
   if (sched == 0) sched = FK_SCHEDULE_DYNAMIC;
-  const uint32_t refill = h.refill ? h.refill : 8;
+  const uint32_t refill = h.refill ? h.refill : ctx->tuning.refill;
   const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
+  const uint32_t leaf_batch = h.leaf_batch ? h.leaf_batch : ctx->tuning.leaf_batch;
+  const uint32_t speculate = h.speculate ? h.speculate : ctx->tuning.speculate;
 #define FK_HEMI_CASE(K)                                                                              \
   case K:                                                                                            \
     if (sched == FK_SCHEDULE_DYNAMIC)                                                                \
-      return trav == FK_TRAVERSE_ORDERED ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill, filter) \
-                                         : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill, filter);   \
+      return trav == FK_TRAVERSE_ORDERED                                                            \
+                 ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill, filter, leaf_batch, speculate)   \
+                 : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill, filter, leaf_batch, speculate);     \
     return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a)                    \
                                        : run_hemi<K, FK_TRAVERSE_SKIP>(ctx, a);
   switch (h.kind) {
@@ -435,6 +440,8 @@ struct DynArgs {
   uint32_t spp, perms, texel0;  // rays [0, total) cover texels texel0 ...
   uint32_t total;
   uint32_t refill;
+  uint32_t leaf_batch;  // postponed leaves that start a leaf phase early
+  uint32_t speculate;   // lanes holding a leaf keep visiting inner records
   float lo, hi;
   float* __restrict__ scratch;  // one distance per ray
   uint32_t* queue;
@@ -459,60 +466,94 @@ __device__ __forceinline__ bool still_open(float entry, float thr) {
   return entry < thr;
 }
 
-// Ordered traversal, one inner node per call.  Returns true when finished.
-template <int STOP, bool COUNT, bool FILTER>
-__device__ __forceinline__ bool ordered_step(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
-                                             int32_t& cur, int& sp, int32_t* stack_node, float* stack_dist,
-                                             int* status, Tally& tally) {
-  const float4* w = s.wide + 4 * (size_t)cur;
+// Lane state of the ordered traversal in the dynamic schedule.  A lane holds
+// the next inner record to visit (cur) and at most one postponed leaf (pend,
+// a flattened node index); the warp alternates between an inner phase and a
+// leaf phase so that its lanes run the same kind of work together (Aila and
+// Laine's while-while structure with postponed leaves).  Leaves are tested
+// only after their box passed against a threshold no smaller than the
+// current one, and re-checked against the current threshold before their
+// triangles run, so the leaf set is that of the ordered traversal.
+struct OState {
+  int32_t cur, pend;
+  float pend_dist;
+  int sp;
+};
+
+template <bool FILTER>
+__device__ __forceinline__ bool push(int32_t* sn, float* sd, int& sp, int32_t ref, float dist, int* status) {
+  if (sp >= kStack) {
+    atomicOr(status, 1);
+    return false;
+  }
+  sn[sp] = ref;
+  sd[sp] = dist;
+  ++sp;
+  return true;
+}
+
+// Inner phase: tests both children of record `cur` against `thr`.
+template <bool COUNT, bool FILTER>
+__device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, float thr, OState& st, int32_t* sn,
+                                            float* sd, int* status, Tally& tally) {
+  const float4* w = s.wide + 4 * (size_t)st.cur;
   float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
-  const f3 blo[2] = {mk3(w0.x, w0.z, w2.x), mk3(w1.x, w1.z, w2.z)};
-  const f3 bhi[2] = {mk3(w0.y, w0.w, w2.y), mk3(w1.y, w1.w, w2.w)};
-  const float thr0 = fminf(best, hi);
   float dist[2];
   bool hit[2];
-  hit[0] = child_hit<FILTER>(rp, blo[0], bhi[0], thr0, dist[0]);
-  hit[1] = child_hit<FILTER>(rp, blo[1], bhi[1], thr0, dist[1]);
+  hit[0] = child_hit<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, dist[0]);
+  hit[1] = child_hit<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, dist[1]);
   if (COUNT) tally.box += 2;
   int32_t ref[2] = {__float_as_int(w3.x), __float_as_int(w3.y)};
-  int32_t cnt[2] = {__float_as_int(w3.z), __float_as_int(w3.w)};
   int first = dist[1] < dist[0] ? 1 : 0;
   int32_t next = -1;
 #pragma unroll
   for (int q = 0; q < 2; ++q) {
     int c = q == 0 ? first : 1 - first;
     if (!hit[c]) continue;
-    // the threshold may have dropped while the nearer child was processed
-    if (q == 1 && fminf(best, hi) < thr0 && !child_hit<FILTER>(rp, blo[c], bhi[c], fminf(best, hi), dist[c])) continue;
-    if (cnt[c] > 0) {
-      uint32_t t0 = (uint32_t)ref[c];
-      if (COUNT) tally.tri += (uint32_t)cnt[c];
-      for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s.rec, t, rp.o, rp.d, lo, best);
-      if (settled<STOP>(best, hi)) return true;
+    if (ref[c] < 0) {
+      if (st.pend < 0) {
+        st.pend = -ref[c] - 1;
+        st.pend_dist = dist[c];
+      } else if (!push<FILTER>(sn, sd, st.sp, ref[c], dist[c], status)) {
+        return false;
+      }
     } else if (next < 0) {
       next = ref[c];
-    } else {
-      if (sp >= kStack) {
-        atomicOr(status, 1);
-        return true;
-      }
-      stack_node[sp] = ref[c];
-      stack_dist[sp] = dist[c];
-      ++sp;
-    }
-  }
-  if (next >= 0) {
-    cur = next;
-    return false;
-  }
-  while (sp > 0) {
-    --sp;
-    if (still_open<FILTER>(stack_dist[sp], fminf(best, hi))) {
-      cur = stack_node[sp];
+    } else if (!push<FILTER>(sn, sd, st.sp, ref[c], dist[c], status)) {
       return false;
     }
   }
+  st.cur = next;
   return true;
+}
+
+// Leaf phase: the postponed leaf's triangles, if its box still passes.
+template <bool COUNT, bool FILTER>
+__device__ __forceinline__ void leaf_visit(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
+                                           OState& st, Tally& tally) {
+  if (still_open<FILTER>(st.pend_dist, fminf(best, hi))) {
+    const uint32_t b = as_u32(__ldg(s.node_lo + st.pend).w), e = as_u32(__ldg(s.node_hi + st.pend).w);
+    if (COUNT) tally.tri += (e - b) / 3;
+    for (uint32_t k = b; k < e; k += 3) tri_sample(s.rec, k / 3, rp.o, rp.d, lo, best);
+  }
+  st.pend = -1;
+}
+
+// Takes the nearest still-open deferred entry; false when none is left.
+template <bool FILTER>
+__device__ __forceinline__ bool pop(OState& st, const int32_t* sn, const float* sd, float thr) {
+  while (st.sp > 0) {
+    --st.sp;
+    if (!still_open<FILTER>(sd[st.sp], thr)) continue;
+    if (sn[st.sp] < 0) {
+      st.pend = -sn[st.sp] - 1;
+      st.pend_dist = sd[st.sp];
+    } else {
+      st.cur = sn[st.sp];
+    }
+    return true;
+  }
+  return false;
 }
 
 // Skip-pointer walk, one flattened node per call.
@@ -550,8 +591,8 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
   uint32_t r = 0;
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX;
-  int32_t cur = 0;
-  int sp = 0;
+  int32_t cur = 0;  // skip walk: node index
+  OState st = {-1, -1, 0.0f, 0};
   for (;;) {
     unsigned idle = __ballot_sync(full, !active);
     if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
@@ -581,15 +622,11 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
               float a = ray_box(o, dir, xyz(L), xyz(H));
               if (COUNT) tally.box++;
               if (a < p.hi) {
-                if (p.s.root_is_leaf) {
-                  uint32_t e = as_u32(H.w);
-                  if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
-                  for (uint32_t q = as_u32(L.w); q < e; q += 3) tri_sample(p.s.rec, q / 3, o, dir, p.lo, best);
-                } else {
-                  cur = 0;
-                  sp = 0;
-                  done = false;
-                }
+                st.sp = 0;
+                st.cur = p.s.root_is_leaf ? -1 : 0;
+                st.pend = p.s.root_is_leaf ? 0 : -1;
+                st.pend_dist = a;
+                done = false;
               }
             } else {
               cur = 0;
@@ -605,12 +642,31 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
       idle = __ballot_sync(full, !active);
     }
     if (exhausted && idle == full) break;
-    if (active) {
-      bool fin = TRAV == FK_TRAVERSE_ORDERED
-                     ? ordered_step<STOP, COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, cur, sp, stack_node, stack_dist,
-                                                         p.status, tally)
-                     : skip_step<STOP, COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, cur, tally);
-      if (fin) {
+    if (TRAV == FK_TRAVERSE_ORDERED) {
+      // phase choice, uniform across the warp
+      const bool spec_ok = st.sp < kStack - 4;
+      const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
+      const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
+      const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
+      if (active) {
+        bool fin = false;
+        if (leaf_phase) {
+          if (st.pend >= 0) {
+            leaf_visit<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, tally);
+            fin = settled<STOP>(best, p.hi);
+          }
+        } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
+          if (!inner_visit<COUNT, FILTER>(p.s, rp, fminf(best, p.hi), st, stack_node, stack_dist, p.status, tally))
+            fin = true;
+        }
+        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stack_node, stack_dist, fminf(best, p.hi));
+        if (fin) {
+          p.scratch[r] = best;
+          active = false;
+        }
+      }
+    } else if (active) {
+      if (skip_step<STOP, COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, cur, tally)) {
         p.scratch[r] = best;
         active = false;
       }
@@ -706,7 +762,8 @@ __global__ void __launch_bounds__(256) hemi_reduce_kernel(HemiArgs p, const floa
 }
 
 template <int KIND, int TRAV>
-static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter) {
+static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter, uint32_t leaf_batch,
+                            uint32_t speculate) {
   auto trace = a.tally ? (filter ? hemi_trace_kernel<KIND, TRAV, true, true> : hemi_trace_kernel<KIND, TRAV, true, false>)
                        : (filter ? hemi_trace_kernel<KIND, TRAV, false, true> : hemi_trace_kernel<KIND, TRAV, false, false>);
   int per_sm = 0;
@@ -730,6 +787,8 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
     d.texel0 = a.offset + done;
     d.total = n * a.spp;
     d.refill = refill;
+    d.leaf_batch = leaf_batch;
+    d.speculate = speculate;
     d.lo = a.lo;
     d.hi = a.hi;
     d.scratch = scratch;

@@ -68,6 +68,17 @@ int fk_sync(fk_ctx* ctx);
 /* Kernel launches issued by this context so far. */
 uint64_t fk_launch_count(const fk_ctx* ctx);
 
+/* Knobs of the dynamically scheduled hemisphere traversal (defaults 8, 16,
+ * 0, 0); fk_tune_hemisphere picks them by measurement. */
+typedef struct fk_tuning {
+  uint32_t refill;      /* idle lanes of a warp that trigger a batch fetch (1..32) */
+  uint32_t leaf_batch;  /* lanes holding a postponed leaf that start a leaf phase (1..32) */
+  uint32_t speculate;   /* lanes holding a leaf keep visiting inner records (0 / 1) */
+  uint32_t reserved;
+} fk_tuning;
+int fk_ctx_set_tuning(fk_ctx* ctx, const fk_tuning* tuning);
+int fk_ctx_get_tuning(const fk_ctx* ctx, fk_tuning* tuning);
+
 /* ------------------------------------------------------------ buffers
  * Replaces ComputeBuffer<T> (Src/compute.h:37-87).  New buffers are
  * zero-filled like ComputeBuffer(count, usage) (Src/compute.h:57-65). */
