@@ -26,7 +26,7 @@ struct fk_ctx {
   int* status = nullptr;          // device status word (limits a kernel could not honour)
   void* scratch = nullptr;        // see fk_scratch
   size_t scratch_bytes = 0;
-  fk_tuning tuning = {8, 16, 0, 0};  // dynamic-schedule knobs (fk_ctx_set_tuning)
+  fk_tuning tuning = {8, 8, 0, 0};   // dynamic-schedule knobs (fk_ctx_set_tuning)
   std::set<fk_buf*> bufs;
   std::set<fk_scene*> scenes;
   std::set<fk_texel_map*> maps;

@@ -68,7 +68,7 @@ int fk_sync(fk_ctx* ctx);
 /* Kernel launches issued by this context so far. */
 uint64_t fk_launch_count(const fk_ctx* ctx);
 
-/* Knobs of the dynamically scheduled hemisphere traversal (defaults 8, 16,
+/* Knobs of the dynamically scheduled hemisphere traversal (defaults 8, 8,
  * 0, 0); fk_tune_hemisphere picks them by measurement. */
 typedef struct fk_tuning {
   uint32_t refill;      /* idle lanes of a warp that trigger a batch fetch (1..32) */
