@@ -50,6 +50,13 @@ WORKLOADS = {
              "thickness 1024 spp, max 0.5",
         gen=lambda seed: W.icosphere_pair(seed=seed),
         tex=4096, spp=1024, min_d=0.001, max_d=0.5, bakers=("ao", "bn", "thick")),
+    # profiling case: the plane workload's scene (381 MB, larger than L2) at 250x250 texels, 16 spp, so one
+    # hemisphere launch lasts milliseconds under ncu
+    "plane250": dict(
+        desc="profiling case: the 1024x1024-quad heightfield scene of plane2048 at 250x250 texels, AO / bent "
+             "normals / thickness 16 spp, min 0.001, max 0.3",
+        gen=lambda seed: W.plane_pair(seed=seed, lo_quads=64, hi_quads=1024, bumps=200),
+        tex=250, spp=16, min_d=0.001, max_d=0.3, bakers=("ao", "bn", "thick")),
 }
 TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2}
 SCHEDULE = {"auto": 0, "static": 0x10, "dynamic": 0x20}
@@ -135,6 +142,24 @@ class Prepared:
         self.triangles = hi.triangle_count
 
 
+def reduce_over_ranks(ms, rays, world, device):
+    """Max of the per-rank step times and sum of the per-rank rays (every
+    rank takes this same collective step)."""
+    if world == 1:
+        return float(ms), float(rays)
+    import torch
+    t = torch.tensor([float(ms)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    r = torch.tensor([float(rays)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(r)
+    return float(t.item()), float(r.item())
+
+
+def replica_seed(base, rank):
+    """Each rank bakes its own seeded replica of the workload."""
+    return base + rank
+
+
 def pinned(shape, dtype):
     import torch
     t = torch.empty(int(np.prod(shape)) * np.dtype(dtype).itemsize, dtype=torch.uint8, pin_memory=True)
@@ -153,7 +178,7 @@ def run_fornos(args, wl, rank, world):
     ctx = api.Context(dev)
     ctx.set_stream(stream.cuda_stream)
     trav = TRAVERSE[args.traverse] | SCHEDULE[args.schedule]
-    prep = Prepared(wl, args.seed + rank)
+    prep = Prepared(wl, replica_seed(args.seed, rank))
     tex, spp, lo_d, hi_d = wl["tex"], wl["spp"], wl["min_d"], wl["max_d"]
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -230,16 +255,7 @@ def run_fornos(args, wl, rank, world):
         for a, b, kind in launches:
             hemi_ms.setdefault(kind, []).append(a.elapsed_time(b))
     rays = rays_per_texel(wl) * n
-    ms_max = ms
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_max = float(t.item())
-        tot = torch.tensor([float(rays)], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(tot)
-        rays_all = float(tot.item())
-    else:
-        rays_all = float(rays)
+    ms_max, rays_all = reduce_over_ranks(ms, rays, world, "cuda")
 
     # ---- end to end through fk_bake from pinned host memory
     keep = []
@@ -277,10 +293,7 @@ def run_fornos(args, wl, rank, world):
     for _ in range(args.steps):
         e2e_step()
     e2e_ms = (time.perf_counter() - w0) * 1e3 / args.steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms, _ = reduce_over_ranks(e2e_ms, 0, world, "cuda")
     h2d = sum(a.nbytes for a in (h_nodes, h_pos, h_nrm, h_pix, h_pixt, h_idx)) + samples.nbytes
     d2h = sum(a.nbytes for k, a in out_arrays.items()
               if (k == "height" and "height" in bakers) or (k == "position3" and "position" in bakers)
