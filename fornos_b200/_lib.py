@@ -109,6 +109,8 @@ _SIGS = {
                               c_int, c_vp, c_vp, c_vp, c_vp]),
     "fk_gather": (c_int, [c_vp, c_vp, c_int, c_vp, c_vp, c_u32, c_u32, c_vp]),
     "fk_tangent_space": (c_int, [c_vp, c_vp, c_u32, c_u32, c_vp]),
+    "fk_hemisphere_noalloc": (c_int, [c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32, c_u32,
+                                      c_int, c_vp, c_vp, c_vp, c_vp, c_vp]),
     "fk_meshmapping_create": (c_int, [c_vp, ctypes.POINTER(c_vp)]),
     "fk_meshmapping_init": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int]),
     "fk_meshmapping_init_scene": (c_int, [c_vp, c_vp, c_vp, c_int]),

@@ -113,6 +113,10 @@ struct HemiLaunch {
   uint32_t speculate = 0;
 };
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h);
+// Same kernels over caller-provided scratch: `dist` holds count x spp floats,
+// `queue` and `status` are zeroed words.  Allocates nothing.
+int launch_hemisphere_external(const fk_scene* s, const HemiLaunch& h, cudaStream_t stream, int sm_count,
+                               const fk_tuning& tun, float* dist, uint32_t* queue, int* status, std::string& err);
 int launch_gather(fk_ctx* ctx, const fk_scene* s, int kind, const float4* coords, const uint32_t* tidx,
                   uint32_t offset, uint32_t count, float* out);
 int launch_tangent_space(fk_ctx* ctx, const fk_texel_map* m, uint32_t offset, uint32_t count, float* io3);

@@ -811,6 +811,98 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
   return FK_OK;
 }
 
+// ------------------------------------------------------------------ hemisphere, caller scratch
+// The dynamic trace + reduce pair over scratch the caller supplies (one float
+// per ray, a queue word and a status word, both already zero), in a single
+// pass: the caller guarantees count x spp fits its scratch.  Nothing here
+// allocates; errors come back as a CUDA error code.
+template <int KIND, int TRAV>
+static cudaError_t run_hemi_external(const HemiArgs& a, cudaStream_t stream, int sm_count, const fk_tuning& tun,
+                                     bool filter, float* dist, uint32_t* queue) {
+  auto trace = filter ? hemi_trace_kernel<KIND, TRAV, false, true> : hemi_trace_kernel<KIND, TRAV, false, false>;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace, 256, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  DynArgs d;
+  d.s = a.s;
+  d.samples = a.samples;
+  d.coords = a.coords;
+  d.tidx = a.tidx;
+  d.spp = a.spp;
+  d.perms = a.perms;
+  d.texel0 = a.offset;
+  d.total = a.count * a.spp;
+  d.refill = tun.refill;
+  d.leaf_batch = tun.leaf_batch;
+  d.speculate = tun.speculate;
+  d.lo = a.lo;
+  d.hi = a.hi;
+  d.scratch = dist;
+  d.queue = queue;
+  d.status = a.status;
+  d.tally = nullptr;
+  uint32_t blocks = (uint32_t)sm_count * (uint32_t)per_sm;
+  uint32_t need = (d.total + 255) / 256;
+  if (blocks > need) blocks = need;
+  trace<<<blocks, 256, 0, stream>>>(d);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  uint32_t rblocks = std::min<uint32_t>((a.count + 7) / 8, (uint32_t)sm_count * 8);
+  hemi_reduce_kernel<KIND><<<rblocks, 256, 0, stream>>>(a, dist, a.offset);
+  return cudaGetLastError();
+}
+
+int launch_hemisphere_external(const fk_scene* s, const HemiLaunch& h, cudaStream_t stream, int sm_count,
+                               const fk_tuning& tun, float* dist, uint32_t* queue, int* status, std::string& err) {
+  HemiArgs a;
+  a.s = dev_of(s);
+  a.samples = h.samples;
+  a.coords = h.coords;
+  a.tidx = h.tidx;
+  a.spp = h.spp;
+  a.perms = h.perms;
+  a.offset = h.offset;
+  a.count = h.count;
+  a.lo = h.min_d;
+  a.hi = h.max_d;
+  a.out0 = h.out0;
+  a.out1 = h.out1;
+  a.hits0 = h.hits0;
+  a.hits1 = h.hits1;
+  a.queue = queue;
+  a.status = status;
+  a.tally = nullptr;
+  int trav = h.traverse & FK_TRAVERSE_MASK;
+  if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
+  if (trav == FK_TRAVERSE_ORDERED && s->depth > kMaxOrderedDepth) {
+    err = "ordered traversal needs tree depth <= 48; use FK_TRAVERSE_SKIP";
+    return FK_ERR_INVALID;
+  }
+  const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
+  cudaError_t e = cudaSuccess;
+#define FK_EXT_CASE(K)                                                                                     \
+  case K:                                                                                                  \
+    e = trav == FK_TRAVERSE_ORDERED                                                                        \
+            ? run_hemi_external<K, FK_TRAVERSE_ORDERED>(a, stream, sm_count, tun, filter, dist, queue)    \
+            : run_hemi_external<K, FK_TRAVERSE_SKIP>(a, stream, sm_count, tun, filter, dist, queue);      \
+    break;
+  switch (h.kind) {
+    FK_EXT_CASE(FK_AO)
+    FK_EXT_CASE(FK_BN)
+    FK_EXT_CASE(FK_THICK)
+    FK_EXT_CASE(FK_AO_BN)
+    default:
+      err = "unknown kind";
+      return FK_ERR_INVALID;
+  }
+#undef FK_EXT_CASE
+  if (e != cudaSuccess) {
+    err = std::string("hemisphere launch: ") + cudaGetErrorName(e);
+    return FK_ERR_CUDA;
+  }
+  return FK_OK;
+}
+
 // ------------------------------------------------------------------ mesh mapping
 __device__ __forceinline__ bool bary_ok_map(f3 w) {
   return w.x >= -1e-5f && w.y >= -1e-5f && w.y <= 1.0f && w.z >= -1e-5f && w.z <= 1.0f;

@@ -232,6 +232,27 @@ int fk_hemisphere(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, cons
 int fk_gather(fk_ctx* ctx, const fk_scene* scene, int kind, const fk_buf* coords, const fk_buf* tidx,
               uint32_t offset, uint32_t count, fk_buf* out);
 
+/* No counterpart in the reference.  fk_hemisphere for callers that must not
+ * allocate device memory during a bake (a host running one bake chunk per
+ * interactive frame, or one that budgets all GPU memory through its own
+ * allocator): cudaMalloc / cudaFree would stall such a caller's frame and can
+ * fail under memory pressure.  It allocates nothing; its per-ray scratch is a
+ * fixed array compiled into the library, held by every GPU that loads it
+ * until the process exits, so one call takes at most FK_NOALLOC_MAX_RAYS
+ * texels x samples (16 MiB of distances); larger requests are refused with
+ * FK_ERR_INVALID and should be split over calls.  All pointers are device
+ * pointers owned by the caller (coords4 / tidx as fk_meshmap writes them,
+ * samples4 as fk_samples_cosine fills them, outputs as fk_hemisphere writes
+ * them); `stream` is a cudaStream_t (NULL = default stream).  The scene's
+ * device must be current.  The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress), so make it before any stream capture.
+ * Every call reuses the same array: calls whose work may overlap on the GPU
+ * race on it and must be serialised by the caller. */
+#define FK_NOALLOC_MAX_RAYS (1u << 22)
+int fk_hemisphere_noalloc(const fk_scene* scene, const float* coords4, const uint32_t* tidx, int kind,
+                          const fk_sample_params* params, const float* samples4, uint32_t offset, uint32_t count,
+                          int traverse, float* out0, float* out1, uint32_t* hits0, uint32_t* hits1, void* stream);
+
 /* Shaders/tangentspace.comp in place over 3-float values [offset, offset+count). */
 int fk_tangent_space(fk_ctx* ctx, const fk_texel_map* map, uint32_t offset, uint32_t count, fk_buf* io3);
 
