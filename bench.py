@@ -61,7 +61,9 @@ WORKLOADS = {
 TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2}
 SCHEDULE = {"auto": 0, "static": 0x10, "dynamic": 0x20}
 # DRAM bytes per hemisphere-kernel launch from ncu captures (profiles/), by workload.
-NCU_TRAFFIC = {}
+# plane250: measured for one AO+BN trace launch (984,064 rays); plane2048: the same 364.5 B per ray scaled to one
+# chunk launch of 134,217,728 rays (traffic grows with rays).  Source: profiles/hemi_trace_kernel_plane250.md.
+NCU_TRAFFIC = {"plane250": 358.7e6, "plane2048": 48.9e9}
 
 
 def rays_per_texel(wl):
@@ -328,7 +330,7 @@ def run_fornos(args, wl, rank, world):
         "e2e": {"value": round(rays_all / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
                 "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(gpu_launches),
-        "roofline": {"bound": "fp32", "kernel": "hemi_kernel", "achieved": round(achieved / 1e12, 3),
+        "roofline": {"bound": "fp32", "kernel": "hemi_trace_kernel", "achieved": round(achieved / 1e12, 3),
                      "peak": round(peak / 1e12, 3), "unit": "TFLOP/s", "frac": round(achieved / peak, 4),
                      "traffic": NCU_TRAFFIC.get(args.workload),
                      "peak_source": "measured in-run: fk_diag_fp32_peak (add/mul/min chains, 1 op per instruction)",
