@@ -435,19 +435,120 @@ def run_reference_arm(args, wl):
     }
 
 
+def batch_jobs(seed, count):
+    """The batched-bake workload: `count` jobs, each a sphere-style or
+    plane-style pair from its own seed, high-poly triangle count log-uniform in
+    10k..2M, texture from {256, 512, 1024, 2048}, AO spp from {32, 128, 512}."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for i in range(count):
+        tris = float(np.exp(rng.uniform(np.log(1e4), np.log(2e6))))
+        tex = int(rng.choice([256, 512, 1024, 2048]))
+        spp = int(rng.choice([32, 128, 512]))
+        if i % 2 == 0:
+            hq = max(8, int(round((tris / 2) ** 0.5)))
+            gen = (lambda s, hq=hq: W.plane_pair(seed=s, lo_quads=64, hi_quads=hq, bumps=200))
+            lo_d, hi_d = 0.001, 0.3
+        else:
+            u = max(16, int(round(tris ** 0.5)))
+            gen = (lambda s, u=u: W.sphere_pair(seed=s, hi_seg=(u, max(8, u // 2))))
+            lo_d, hi_d = 0.001, 0.5
+        jobs.append(dict(gen=gen, seed=seed * 1000 + i, tex=tex, spp=spp, min_d=lo_d, max_d=hi_d))
+    return jobs
+
+
+def run_batch_bench(args):
+    """64 jobs: per-job fk_hemisphere launches vs one batched persistent launch
+    (default schedule, autotuned, and autotuned + CUDA graph).  AO only."""
+    import torch
+
+    from fornos_b200 import api
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    ctx = api.Context(0)
+    ctx.set_stream(stream.cuda_stream)
+    specs = batch_jobs(args.seed, args.batch_jobs)
+    jobs, keep = [], []
+    tables = {}
+    for s in specs:
+        wl = dict(gen=s["gen"], tex=s["tex"])
+        prep = Prepared(wl, s["seed"])
+        tm = api.TexelMap.from_meshes(ctx, prep.lm, prep.dm, s["tex"], s["tex"])
+        scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
+        n = tm.count
+        coords, tidx = ctx.buffer(16 * n), ctx.buffer(4 * n)
+        api.meshmap(ctx, scene, tm, True, coords, tidx)
+        if s["spp"] not in tables:
+            tables[s["spp"]] = ctx.upload(api.samples_cosine(s["spp"], api.PERMS, args.seed))
+        jobs.append(dict(scene=scene, coords=coords, tidx=tidx, texel_count=n, spp=s["spp"], min_distance=s["min_d"],
+                         max_distance=s["max_d"], samples=tables[s["spp"]], out0=ctx.buffer(4 * n),
+                         hits0=ctx.buffer(4 * n), triangles=prep.triangles, tex=s["tex"]))
+        keep.append((tm, prep))
+    ctx.sync()
+    rays = sum(j["texel_count"] * j["spp"] for j in jobs)
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            fn()  # warm-up
+            stream.synchronize()
+            a.record(stream)
+            fn()
+            b.record(stream)
+        stream.synchronize()
+        return a.elapsed_time(b)
+
+    def per_job():
+        for j in jobs:
+            api.hemisphere(ctx, j["scene"], j["coords"], j["tidx"], api.AO, j["spp"], j["min_distance"],
+                           j["max_distance"], j["samples"], j["out0"], None, j["hits0"], None, 0, j["texel_count"])
+
+    t_jobs = timed(per_job)
+    want = [(j["out0"].download(np.float32, j["texel_count"]), j["hits0"].download(np.uint32, j["texel_count"]))
+            for j in jobs]
+    outs = [dict(out0=ctx.buffer(4 * j["texel_count"]), hits0=ctx.buffer(4 * j["texel_count"])) for j in jobs]
+    batch = api.Batch(ctx, [dict(j, **o) for j, o in zip(jobs, outs)], api.AO)
+    t_batch = timed(lambda: batch.run())
+    tuned = batch.tune()
+    t_tuned = timed(lambda: batch.run())
+    batch.capture()
+    t_graph = timed(lambda: batch.replay())
+    identical = all(np.array_equal(o["out0"].download(np.float32, j["texel_count"]).view(np.uint32), w[0].view(np.uint32))
+                    and np.array_equal(o["hits0"].download(np.uint32, j["texel_count"]), w[1])
+                    for j, o, w in zip(jobs, outs, want))
+    mr = lambda ms: round(rays / (ms * 1e-3) / 1e6, 2)
+    return {
+        "metric": "Mrays/s (batched AO bake of %d jobs)" % len(jobs), "value": mr(t_graph), "unit": "Mrays/s",
+        "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generated meshes)",
+        "config": {"workload": "batch%d" % len(jobs), "rays": rays,
+                   "texels": sum(j["texel_count"] for j in jobs),
+                   "triangles": [j["triangles"] for j in jobs], "textures": [j["tex"] for j in jobs],
+                   "spp": [j["spp"] for j in jobs]},
+        "per_job_launches": {"ms": round(t_jobs, 2), "mrays": mr(t_jobs)},
+        "batch_default": {"ms": round(t_batch, 2), "mrays": mr(t_batch)},
+        "batch_tuned": {"ms": round(t_tuned, 2), "mrays": mr(t_tuned), "tuning": tuned},
+        "batch_tuned_graph": {"ms": round(t_graph, 2), "mrays": mr(t_graph), "info": batch.info()},
+        "batch_equals_per_job": bool(identical),
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fornos", choices=["fornos", "reference"])
-    ap.add_argument("--workload", default="plane2048", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="plane2048", choices=list(WORKLOADS) + ["batch"])
+    ap.add_argument("--batch-jobs", type=int, default=64)
     ap.add_argument("--traverse", default="auto", choices=list(TRAVERSE))
     ap.add_argument("--schedule", default="auto", choices=list(SCHEDULE))
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.workload == "batch":
+        print(json.dumps(run_batch_bench(args)))
+        return 0
     wl = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))

@@ -61,6 +61,12 @@ class BakeDesc(ctypes.Structure):
                 ("thickness", BakeSampler), ("traverse", c_int)]
 
 
+class BatchJob(ctypes.Structure):
+    _fields_ = [("scene", c_vp), ("coords", c_vp), ("tidx", c_vp), ("texel_count", c_u32),
+                ("params", SampleParams), ("samples", c_vp), ("out0", c_vp), ("out1", c_vp), ("hits0", c_vp),
+                ("hits1", c_vp)]
+
+
 class BakeOut(ctypes.Structure):
     _fields_ = [("coords4", f32p), ("tidx", u32p), ("height", f32p), ("position3", f32p), ("normals3", f32p),
                 ("ao", f32p), ("bent_normals3", f32p), ("thickness", f32p)]
@@ -133,6 +139,15 @@ _SIGS = {
     "fk_solver_result_buffer": (c_vp, [c_vp]),
     "fk_solver_free": (c_int, [c_vp]),
     "fk_bake": (c_int, [c_vp, ctypes.POINTER(BakeDesc), ctypes.POINTER(BakeOut)]),
+    "fk_batch_create": (c_int, [c_vp, ctypes.POINTER(BatchJob), c_u32, c_int, ctypes.POINTER(c_vp)]),
+    "fk_batch_info": (c_int, [c_vp, ctypes.POINTER(c_u64), u32p, u32p]),
+    "fk_batch_tune": (c_int, [c_vp, c_u64, ctypes.POINTER(Tuning), ctypes.POINTER(c_int)]),
+    "fk_batch_run": (c_int, [c_vp, c_int]),
+    "fk_batch_capture": (c_int, [c_vp, c_int]),
+    "fk_batch_replay": (c_int, [c_vp]),
+    "fk_batch_free": (c_int, [c_vp]),
+    "fk_tune_hemisphere": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32, c_u32,
+                                   c_u64, ctypes.POINTER(Tuning), ctypes.POINTER(c_int)]),
     "fk_diag_fp32_peak": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double)]),
     "fk_diag_traversal_counts": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32,
                                          c_u32, c_int, ctypes.POINTER(c_u64)]),

@@ -569,3 +569,67 @@ def bake(ctx, nodes, pos4, nrm4, width, height, pix8, pixt12, indices, outputs, 
         if a is not None:
             setattr(o, name, a.ctypes.data_as(ctype))
     _check(ctx.lib.fk_bake(ctx.handle, ctypes.byref(d), ctypes.byref(o)), ctx, "fk_bake")
+
+
+# ------------------------------------------------------------------ batches and tuning
+class Batch:
+    """Batched hemisphere jobs in one persistent launch (fk_batch_*).
+    jobs: list of dicts with scene, coords, tidx, texel_count, spp, min_distance, max_distance, samples, out0
+    (and out1, hits0, hits1); perms defaults to 4096."""
+
+    def __init__(self, ctx, jobs, kind=AO):
+        self.ctx = ctx
+        arr = (L.BatchJob * len(jobs))()
+        hv = lambda b: b.handle if b is not None else None
+        for i, j in enumerate(jobs):
+            arr[i] = L.BatchJob(j["scene"].handle, j["coords"].handle, j["tidx"].handle, j["texel_count"],
+                                L.SampleParams(j["spp"], j.get("perms", PERMS), j["min_distance"], j["max_distance"]),
+                                j["samples"].handle, j["out0"].handle, hv(j.get("out1")), hv(j.get("hits0")),
+                                hv(j.get("hits1")))
+        h = L.c_vp()
+        _check(ctx.lib.fk_batch_create(ctx.handle, arr, len(jobs), kind, ctypes.byref(h)), ctx, "fk_batch_create")
+        self.handle = h.value
+
+    def info(self):
+        rays, texels, launches = L.c_u64(), L.c_u32(), L.c_u32()
+        _check(self.ctx.lib.fk_batch_info(self.handle, ctypes.byref(rays), ctypes.byref(texels),
+                                          ctypes.byref(launches)))
+        return {"rays": rays.value, "texels": texels.value, "launches_per_run": launches.value}
+
+    def tune(self, sample_rays=0):
+        t, trav = L.Tuning(), L.c_int()
+        _check(self.ctx.lib.fk_batch_tune(self.handle, sample_rays, ctypes.byref(t), ctypes.byref(trav)), self.ctx,
+               "fk_batch_tune")
+        return {"refill": t.refill, "leaf_batch": t.leaf_batch, "traverse": trav.value}
+
+    def run(self, traverse=0):
+        _check(self.ctx.lib.fk_batch_run(self.handle, traverse), self.ctx, "fk_batch_run")
+
+    def capture(self, traverse=0):
+        _check(self.ctx.lib.fk_batch_capture(self.handle, traverse), self.ctx, "fk_batch_capture")
+
+    def replay(self):
+        _check(self.ctx.lib.fk_batch_replay(self.handle), self.ctx, "fk_batch_replay")
+
+    def free(self):
+        if self.handle and self.ctx.handle:
+            self.ctx.lib.fk_batch_free(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def tune_hemisphere(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, offset=0, count=0, perms=PERMS,
+                    sample_rays=0):
+    """Autotunes the dynamic traversal for one fk_hemisphere call; returns
+    (tuning dict, traverse flags).  Apply with ctx.set_tuning(**...)."""
+    p = L.SampleParams(spp, perms, min_d, max_d)
+    t, trav = L.Tuning(), L.c_int()
+    _check(ctx.lib.fk_tune_hemisphere(ctx.handle, scene.handle, coords.handle, tidx.handle, kind, ctypes.byref(p),
+                                      samples.handle, offset, count, sample_rays, ctypes.byref(t),
+                                      ctypes.byref(trav)), ctx, "fk_tune_hemisphere")
+    return {"refill": t.refill, "leaf_batch": t.leaf_batch, "speculate": t.speculate}, trav.value

@@ -1,0 +1,357 @@
+// Batched bakes and the traversal autotuner.
+//
+// A batch is a set of hemisphere-sampling jobs, each with its own scene,
+// mapped texels, sample table, parameters and output buffers, that share
+// one persistent launch: their rays are laid end to end in one 64-bit ray
+// space (chunked at texel boundaries to fit the scratch), and every lane maps
+// its ray back to its job.  The launches of a run can be recorded once into a
+// CUDA graph and replayed.  The autotuner times a strided sample of the
+// batch's rays (every job represented) for each candidate schedule and keeps
+// the fastest: ordered vs skip-pointer traversal, filtered vs divided box
+// tests, the refill threshold and the postponed-leaf batch.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "fk_internal.h"
+
+namespace {
+
+struct Chunk {
+  unsigned long long r0, r1;
+  uint32_t t0, t1;
+};
+
+constexpr unsigned long long kMaxChunkRays = 1ull << 27;  // 512 MB of distances
+
+}  // namespace
+
+struct fk_batch {
+  fk_ctx* ctx = nullptr;
+  int kind = FK_AO;
+  uint32_t njobs = 0;
+  unsigned long long total_rays = 0;
+  uint32_t total_texels = 0;
+  fk::BatchJobDev* jobs = nullptr;        // device job table
+  unsigned long long* queues = nullptr;   // one counter per chunk (and one for calibration)
+  float* scratch = nullptr;
+  unsigned long long scratch_rays = 0;
+  std::vector<Chunk> chunks;
+  int traverse = FK_TRAVERSE_ORDERED;     // tuned choice
+  bool filter = true;
+  fk_tuning tuning = {8, 8, 0, 0};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+static bool fits(const fk_buf* b, uint64_t bytes) { return b && b->bytes >= bytes; }
+
+static int batch_run_chunks(fk_batch* b, int trav, bool filter, const fk_tuning& tun) {
+  fk_ctx* ctx = b->ctx;
+  for (size_t c = 0; c < b->chunks.size(); ++c) {
+    const Chunk& ch = b->chunks[c];
+    FK_CUDA(ctx, cudaMemsetAsync(b->queues + c, 0, sizeof(unsigned long long), ctx->stream));
+    fk::BatchArgs a;
+    a.jobs = b->jobs;
+    a.njobs = b->njobs;
+    a.r0 = ch.r0;
+    a.r1 = ch.r1;
+    a.t0 = ch.t0;
+    a.t1 = ch.t1;
+    a.stride = 1;
+    a.scratch = b->scratch;
+    a.queue = b->queues + c;
+    a.status = ctx->status;
+    a.refill = tun.refill;
+    a.leaf_batch = tun.leaf_batch;
+    cudaError_t e = fk::launch_batch(a, b->kind, trav, filter, ctx->stream, ctx->sm_count, true);
+    if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "batch launch");
+    ctx->launches += 2;
+  }
+  return FK_OK;
+}
+
+static void batch_drop_graph(fk_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  b->exec = nullptr;
+  b->graph = nullptr;
+}
+
+// Times the trace of every `stride`-th ray of the batch under one schedule.
+static int batch_time(fk_batch* b, unsigned long long stride, int trav, bool filter, const fk_tuning& tun,
+                      float* ms) {
+  fk_ctx* ctx = b->ctx;
+  unsigned long long* q = b->queues + b->chunks.size();
+  fk::BatchArgs a;
+  a.jobs = b->jobs;
+  a.njobs = b->njobs;
+  a.r0 = 0;
+  a.r1 = b->total_rays;
+  a.t0 = a.t1 = 0;
+  a.stride = stride;
+  a.scratch = b->scratch;
+  a.queue = q;
+  a.status = ctx->status;
+  a.refill = tun.refill;
+  a.leaf_batch = tun.leaf_batch;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int rc = FK_OK;
+  for (int rep = 0; rep < 2 && rc == FK_OK; ++rep) {
+    cudaMemsetAsync(q, 0, sizeof(unsigned long long), ctx->stream);
+    cudaEventRecord(e0, ctx->stream);
+    cudaError_t e = fk::launch_batch(a, b->kind, trav, filter, ctx->stream, ctx->sm_count, false);
+    cudaEventRecord(e1, ctx->stream);
+    if (e != cudaSuccess) rc = fk_cuda_fail(ctx, e, "batch calibration");
+    else if ((e = cudaEventSynchronize(e1)) != cudaSuccess) rc = fk_cuda_fail(ctx, e, "batch calibration sync");
+    float t = 0.0f;
+    cudaEventElapsedTime(&t, e0, e1);
+    best = std::min(best, t);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = best;
+  return rc;
+}
+
+extern "C" {
+
+int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int kind, fk_batch** out) {
+  if (!ctx || !jobs || !out || njobs == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_batch_create: no jobs");
+  if (njobs > fk::kMaxBatchJobs)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_batch_create: at most " + std::to_string(fk::kMaxBatchJobs) + " jobs");
+  if (kind < FK_AO || kind > FK_AO_BN) return fk_fail(ctx, FK_ERR_INVALID, "fk_batch_create: unknown kind");
+  std::vector<fk::BatchJobDev> table(njobs);
+  unsigned long long rays = 0;
+  uint64_t texels = 0;
+  for (uint32_t i = 0; i < njobs; ++i) {
+    const fk_batch_job& J = jobs[i];
+    const uint64_t n = J.texel_count;
+    const std::string who = "fk_batch_create: job " + std::to_string(i);
+    if (!J.scene || !ctx->scenes.count(const_cast<fk_scene*>(J.scene)))
+      return fk_fail(ctx, FK_ERR_INVALID, who + " has no scene of this context");
+    if (J.params.sample_count == 0 || J.params.perm_count == 0)
+      return fk_fail(ctx, FK_ERR_INVALID, who + " has zero samples");
+    if (!fits(J.coords, 16 * n) || !fits(J.tidx, 4 * n) ||
+        !fits(J.samples, 16ull * J.params.sample_count * J.params.perm_count) ||
+        !fits(J.out0, (kind == FK_BN ? 12 : 4) * n) || (kind == FK_AO_BN && !fits(J.out1, 12 * n)) ||
+        (J.hits0 && !fits(J.hits0, 4 * n)) || (J.hits1 && !fits(J.hits1, 4 * n)))
+      return fk_fail(ctx, FK_ERR_INVALID, who + " has a buffer too small for its texels");
+    if ((unsigned long long)J.params.sample_count > kMaxChunkRays)
+      return fk_fail(ctx, FK_ERR_INVALID, who + " has too many samples per texel");
+    fk::BatchJobDev& d = table[i];
+    std::memset(&d, 0, sizeof(d));
+    d.s = fk::scene_dev(J.scene);
+    d.samples = (const float4*)J.samples->ptr;
+    d.coords = (const float4*)J.coords->ptr;
+    d.tidx = (const uint32_t*)J.tidx->ptr;
+    d.out0 = (float*)J.out0->ptr;
+    d.out1 = kind == FK_AO_BN ? (float*)J.out1->ptr : nullptr;
+    d.hits0 = J.hits0 ? (uint32_t*)J.hits0->ptr : nullptr;
+    d.hits1 = (kind == FK_AO_BN && J.hits1) ? (uint32_t*)J.hits1->ptr : nullptr;
+    d.ray_base = rays;
+    d.texel_base = (uint32_t)texels;
+    d.texels = J.texel_count;
+    d.spp = J.params.sample_count;
+    d.perms = J.params.perm_count;
+    d.lo = J.params.min_distance;
+    d.hi = J.params.max_distance;
+    rays += n * J.params.sample_count;
+    texels += n;
+    if (texels > 0xFFFFFFFFull) return fk_fail(ctx, FK_ERR_INVALID, "fk_batch_create: more than 2^32 texels");
+  }
+  fk_batch* b = new (std::nothrow) fk_batch();
+  if (!b) return FK_ERR_NOMEM;
+  b->ctx = ctx;
+  b->kind = kind;
+  b->njobs = njobs;
+  b->total_rays = rays;
+  b->total_texels = (uint32_t)texels;
+  // chunks at texel boundaries, at most kMaxChunkRays rays each
+  Chunk cur = {0, 0, 0, 0};
+  for (uint32_t i = 0; i < njobs; ++i) {
+    const fk::BatchJobDev& d = table[i];
+    uint32_t t = 0;
+    while (t < d.texels) {
+      unsigned long long room = (kMaxChunkRays - (cur.r1 - cur.r0)) / d.spp;
+      if (room == 0) {
+        b->chunks.push_back(cur);
+        cur = {cur.r1, cur.r1, cur.t1, cur.t1};
+        continue;
+      }
+      uint32_t take = (uint32_t)std::min<unsigned long long>(room, d.texels - t);
+      cur.r1 += (unsigned long long)take * d.spp;
+      cur.t1 += take;
+      t += take;
+    }
+  }
+  if (cur.t1 > cur.t0) b->chunks.push_back(cur);
+  b->scratch_rays = std::min<unsigned long long>(std::max<unsigned long long>(rays, 1), kMaxChunkRays);
+  int rc = fk_dev_alloc(ctx, (void**)&b->jobs, sizeof(fk::BatchJobDev) * njobs);
+  if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->queues, sizeof(unsigned long long) * (b->chunks.size() + 1));
+  if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->scratch, sizeof(float) * b->scratch_rays);
+  if (rc == FK_OK) {
+    cudaError_t e = cudaMemcpyAsync(b->jobs, table.data(), sizeof(fk::BatchJobDev) * njobs, cudaMemcpyHostToDevice,
+                                    ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) rc = fk_cuda_fail(ctx, e, "fk_batch_create upload");
+  }
+  if (rc != FK_OK) {
+    fk_batch_free(b);
+    return rc;
+  }
+  // default schedule: ordered when every scene's tree is shallow enough
+  for (uint32_t i = 0; i < njobs; ++i)
+    if (jobs[i].scene->depth > 48) b->traverse = FK_TRAVERSE_SKIP;
+  b->tuning = ctx->tuning;
+  *out = b;
+  return FK_OK;
+}
+
+int fk_batch_info(const fk_batch* b, uint64_t* rays, uint32_t* texels, uint32_t* launches_per_run) {
+  if (!b) return FK_ERR_INVALID;
+  if (rays) *rays = b->total_rays;
+  if (texels) *texels = b->total_texels;
+  if (launches_per_run) *launches_per_run = (uint32_t)(2 * b->chunks.size());
+  return FK_OK;
+}
+
+int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse) {
+  if (!b) return FK_ERR_INVALID;
+  fk_ctx* ctx = b->ctx;
+  if (sample_rays == 0) sample_rays = 1ull << 22;
+  sample_rays = std::min<uint64_t>(sample_rays, b->scratch_rays);
+  unsigned long long stride = std::max<unsigned long long>(1, (b->total_rays + sample_rays - 1) / sample_rays);
+  struct Cand {
+    int trav;
+    bool filter;
+    fk_tuning t;
+  };
+  std::vector<Cand> cands;
+  bool ordered_ok = b->traverse == FK_TRAVERSE_ORDERED;
+  for (uint32_t refill : {4u, 8u, 16u}) {
+    if (ordered_ok)
+      for (uint32_t lb : {1u, 4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED, true, {refill, lb, 0, 0}});
+    cands.push_back({FK_TRAVERSE_SKIP, true, {refill, 8, 0, 0}});
+  }
+  if (ordered_ok) cands.push_back({FK_TRAVERSE_ORDERED, false, {8, 8, 0, 0}});
+  cands.push_back({FK_TRAVERSE_SKIP, false, {8, 8, 0, 0}});
+  float best_ms = 1e30f;
+  Cand best = cands[0];
+  float warm = 0.0f;
+  int rc = batch_time(b, stride, cands[0].trav, cands[0].filter, cands[0].t, &warm);  // warms caches and code
+  for (const Cand& c : cands) {
+    if (rc != FK_OK) break;
+    float ms = 0.0f;
+    rc = batch_time(b, stride, c.trav, c.filter, c.t, &ms);
+    if (rc == FK_OK && ms < best_ms) {
+      best_ms = ms;
+      best = c;
+    }
+  }
+  if (rc != FK_OK) return rc;
+  b->traverse = best.trav;
+  b->filter = best.filter;
+  b->tuning = best.t;
+  batch_drop_graph(b);
+  if (best_tuning) *best_tuning = best.t;
+  if (best_traverse) *best_traverse = best.trav | FK_SCHEDULE_DYNAMIC | (best.filter ? 0 : FK_EXACT_BOX_TESTS);
+  return FK_OK;
+}
+
+int fk_batch_run(fk_batch* b, int traverse) {
+  if (!b) return FK_ERR_INVALID;
+  int trav = traverse & FK_TRAVERSE_MASK;
+  bool filter = b->filter && !(traverse & FK_EXACT_BOX_TESTS);
+  if (trav == FK_TRAVERSE_AUTO) trav = b->traverse;
+  if (trav == FK_TRAVERSE_ORDERED && b->traverse == FK_TRAVERSE_SKIP && !(traverse & FK_TRAVERSE_MASK))
+    trav = FK_TRAVERSE_SKIP;
+  return batch_run_chunks(b, trav, filter, b->tuning);
+}
+
+int fk_batch_capture(fk_batch* b, int traverse) {
+  if (!b) return FK_ERR_INVALID;
+  fk_ctx* ctx = b->ctx;
+  batch_drop_graph(b);
+  FK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = fk_batch_run(b, traverse);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+  if (rc != FK_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "cudaStreamEndCapture");
+  b->graph = g;
+  e = cudaGraphInstantiate(&b->exec, g, 0);
+  if (e != cudaSuccess) {
+    batch_drop_graph(b);
+    return fk_cuda_fail(ctx, e, "cudaGraphInstantiate");
+  }
+  return FK_OK;
+}
+
+int fk_batch_replay(fk_batch* b) {
+  if (!b) return FK_ERR_INVALID;
+  if (!b->exec) return fk_fail(b->ctx, FK_ERR_STATE, "fk_batch_replay: nothing captured");
+  FK_CUDA(b->ctx, cudaGraphLaunch(b->exec, b->ctx->stream));
+  b->ctx->launches += 2 * b->chunks.size();
+  return FK_OK;
+}
+
+int fk_batch_free(fk_batch* b) {
+  if (!b) return FK_ERR_INVALID;
+  if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
+  batch_drop_graph(b);
+  fk_dev_free(b->jobs);
+  fk_dev_free(b->queues);
+  fk_dev_free(b->scratch);
+  delete b;
+  return FK_OK;
+}
+
+// Tuner for a single fk_hemisphere call: a one-job batch over the same
+// arguments, calibrated on a strided sample of its rays.
+int fk_tune_hemisphere(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
+                       const fk_sample_params* params, const fk_buf* samples, uint32_t offset, uint32_t count,
+                       uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse) {
+  if (!ctx || !scene || !coords || !tidx || !params || !samples || !best_tuning || !best_traverse)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: null argument");
+  uint64_t end = (uint64_t)offset + count;
+  if (!fits(coords, 16 * end) || !fits(tidx, 4 * end))
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: mapping buffers too small");
+  if (count == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: no texels");
+  // views of the caller's buffers at `offset` (no copies), outputs to scratch
+  fk_buf c_view = *coords, t_view = *tidx;
+  c_view.ptr = (char*)coords->ptr + 16 * (size_t)offset;
+  c_view.bytes = 16 * (size_t)count;
+  t_view.ptr = (char*)tidx->ptr + 4 * (size_t)offset;
+  t_view.bytes = 4 * (size_t)count;
+  fk_buf *o0 = nullptr, *o1 = nullptr;
+  int rc = fk_buf_alloc(ctx, 12 * (size_t)count, &o0);
+  if (rc == FK_OK) rc = fk_buf_alloc(ctx, 12 * (size_t)count, &o1);
+  fk_batch* b = nullptr;
+  if (rc == FK_OK) {
+    fk_batch_job j;
+    std::memset(&j, 0, sizeof(j));
+    j.scene = scene;
+    j.coords = &c_view;
+    j.tidx = &t_view;
+    j.texel_count = count;
+    j.params = *params;
+    j.samples = samples;
+    j.out0 = o0;
+    j.out1 = o1;
+    rc = fk_batch_create(ctx, &j, 1, kind, &b);
+  }
+  if (rc == FK_OK) rc = fk_batch_tune(b, sample_rays, best_tuning, best_traverse);
+  if (b) fk_batch_free(b);
+  if (o0) fk_buf_free(ctx, o0);
+  if (o1) fk_buf_free(ctx, o1);
+  return rc;
+}
+
+}  // extern "C"

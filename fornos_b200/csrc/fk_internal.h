@@ -92,6 +92,53 @@ void* fk_scratch(fk_ctx* ctx, size_t bytes);
 
 // Kernel launchers (fk_*.cu).
 namespace fk {
+
+// Device view of a scene, passed to kernels by value or kept in shared memory.
+struct SceneDev {
+  const float4* __restrict__ node_lo;
+  const float4* __restrict__ node_hi;
+  const uint32_t* __restrict__ node_jump;
+  const float4* __restrict__ pos4;
+  const float4* __restrict__ nrm4;
+  const float4* __restrict__ wide;
+  const float4* __restrict__ rec;
+  uint32_t node_count;
+  uint32_t root_is_leaf;
+  uint32_t corner_count;
+  uint32_t filter_ok;  // scene coordinates small enough for the filtered box test
+};
+SceneDev scene_dev(const fk_scene* s);
+
+// One job of a batched hemisphere launch (device-side job table entry).
+static constexpr uint32_t kMaxBatchJobs = 64;
+struct BatchJobDev {
+  SceneDev s;
+  const float4* samples;
+  const float4* coords;
+  const uint32_t* tidx;
+  float* out0;
+  float* out1;
+  uint32_t* hits0;
+  uint32_t* hits1;
+  unsigned long long ray_base;  // first ray of the job in the batch's ray space
+  uint32_t texel_base;          // first texel of the job in the batch's texel space
+  uint32_t texels, spp, perms;
+  float lo, hi;
+  uint32_t pad[2];
+};
+struct BatchArgs {
+  const BatchJobDev* jobs;
+  uint32_t njobs;
+  unsigned long long r0, r1;  // rays of this launch
+  uint32_t t0, t1;            // texels folded by this launch
+  unsigned long long stride;  // trace every stride-th ray (calibration), 1 otherwise
+  float* scratch;             // one distance per traced ray, indexed from r0 / stride
+  unsigned long long* queue;  // zeroed before the launch
+  int* status;
+  uint32_t refill, leaf_batch;
+};
+cudaError_t launch_batch(const BatchArgs& a, int kind, int trav, bool filter, cudaStream_t stream, int sm_count,
+                         bool reduce);
 int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, uint32_t offset, uint32_t count,
                    float4* coords, uint32_t* tidx);
 struct HemiLaunch {

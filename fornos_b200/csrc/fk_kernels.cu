@@ -24,20 +24,6 @@
 
 namespace fk {
 
-struct SceneDev {
-  const float4* __restrict__ node_lo;
-  const float4* __restrict__ node_hi;
-  const uint32_t* __restrict__ node_jump;
-  const float4* __restrict__ pos4;
-  const float4* __restrict__ nrm4;
-  const float4* __restrict__ wide;
-  const float4* __restrict__ rec;
-  uint32_t node_count;
-  uint32_t root_is_leaf;
-  uint32_t corner_count;
-  uint32_t filter_ok;  // scene coordinates small enough for the filtered box test
-};
-
 // A hit index read from a caller's buffer: a miss, or the first corner of a
 // triangle inside the scene.  Anything else is reported and treated as a miss.
 __device__ __forceinline__ bool valid_hit(uint32_t id, uint32_t corners) {
@@ -809,6 +795,250 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
     if (rc != FK_OK) return rc;
   }
   return FK_OK;
+}
+
+// ------------------------------------------------------------------ hemisphere, batched jobs
+// Many bake jobs (each its own scene, texels, sample table, parameters and
+// outputs) share one persistent launch.  The global ray space is the jobs'
+// rays end to end (64-bit ids); a lane maps its ray to a job by binary search
+// over the job table, which every block keeps in shared memory, and traverses
+// that job's scene in place.  `stride` > 1 traces every stride-th ray only
+// (the autotuner's calibration sample).
+template <int KIND, int TRAV, bool FILTER>
+__global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
+  constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
+  __shared__ BatchJobDev jobs[kMaxBatchJobs];
+  for (uint32_t i = threadIdx.x; i < p.njobs * (uint32_t)(sizeof(BatchJobDev) / 4); i += blockDim.x)
+    ((uint32_t*)jobs)[i] = ((const uint32_t*)p.jobs)[i];
+  __syncthreads();
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lower = (1u << lane) - 1u;
+  const unsigned long long total = (p.r1 - p.r0 + p.stride - 1) / p.stride;
+  int32_t stack_node[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
+  float stack_dist[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
+  Tally tally;
+  bool active = false, exhausted = false;
+  unsigned long long q = 0;
+  int j = 0;
+  RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
+  float best = FLT_MAX, lo = 0.0f, hi = 0.0f;
+  int32_t cur = 0;
+  uint32_t end = 0;  // skip walk: one past the job's last node
+  OState st = {-1, -1, 0.0f, 0};
+  for (;;) {
+    unsigned idle = __ballot_sync(full, !active);
+    if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
+      const uint32_t n_idle = __popc(idle);
+      const int leader = __ffs(idle) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(p.queue, (unsigned long long)n_idle);
+      base = __shfl_sync(full, base, leader);
+      if (base + n_idle >= total) exhausted = true;
+      if (!active) {
+        q = base + __popc(idle & lower);
+        if (q < total) {
+          const unsigned long long r = p.r0 + q * p.stride;
+          int a = 0, b = (int)p.njobs - 1;  // last job whose ray_base <= r
+          while (a < b) {
+            int m = (a + b + 1) >> 1;
+            if (jobs[m].ray_base <= r) a = m; else b = m - 1;
+          }
+          j = a;
+          const BatchJobDev& J = jobs[j];
+          const unsigned long long local = r - J.ray_base;
+          const uint32_t g = (uint32_t)(local / J.spp), k = (uint32_t)(local % J.spp);
+          const uint32_t id = __ldg(J.tidx + g);
+          best = FLT_MAX;
+          lo = J.lo;
+          hi = J.hi;
+          bool done = true;
+          if (id != kMiss && valid_hit(id, J.s.corner_count)) {
+            f3 o, d, tx, ty;
+            texel_frame(J.s, __ldg(J.coords + g), id, o, d, tx, ty);
+            if (KIND == FK_THICK) d = neg(d);
+            float4 rs = __ldg(J.samples + (size_t)(g % J.perms) * J.spp + k);
+            f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+            rp = ray_pre(o, dir);
+            if (!J.s.filter_ok) rp.exact_only = true;
+            if (TRAV == FK_TRAVERSE_ORDERED) {
+              float4 L = __ldg(J.s.node_lo), H = __ldg(J.s.node_hi);
+              float aa = ray_box(o, dir, xyz(L), xyz(H));
+              if (aa < hi) {
+                st.sp = 0;
+                st.cur = J.s.root_is_leaf ? -1 : 0;
+                st.pend = J.s.root_is_leaf ? 0 : -1;
+                st.pend_dist = aa;
+                done = false;
+              }
+            } else {
+              cur = 0;
+              end = J.s.node_count;
+              done = false;
+            }
+          } else if (id != kMiss) {
+            atomicOr(p.status, 2);
+          }
+          if (done) p.scratch[q] = best;
+          else active = true;
+        }
+      }
+      idle = __ballot_sync(full, !active);
+    }
+    if (exhausted && idle == full) break;
+    const SceneDev& s = jobs[j].s;
+    if (TRAV == FK_TRAVERSE_ORDERED) {
+      const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
+      const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
+      const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
+      if (active) {
+        bool fin = false;
+        if (leaf_phase) {
+          if (st.pend >= 0) {
+            leaf_visit<false, FILTER>(s, rp, lo, hi, best, st, tally);
+            fin = settled<STOP>(best, hi);
+          }
+        } else if (st.cur >= 0 && st.pend < 0) {
+          if (!inner_visit<false, FILTER>(s, rp, fminf(best, hi), st, stack_node, stack_dist, p.status, tally))
+            fin = true;
+        }
+        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stack_node, stack_dist, fminf(best, hi));
+        if (fin) {
+          p.scratch[q] = best;
+          active = false;
+        }
+      }
+    } else if (active) {
+      if (skip_step<STOP, false, FILTER>(s, rp, lo, hi, best, cur, tally) || (uint32_t)cur >= end) {
+        p.scratch[q] = best;
+        active = false;
+      }
+    }
+  }
+}
+
+// Per-texel folds for a batch chunk: global texels [t0, t1), one warp each.
+template <int KIND>
+__global__ void __launch_bounds__(256) batch_reduce_kernel(BatchArgs p) {
+  __shared__ BatchJobDev jobs[kMaxBatchJobs];
+  for (uint32_t i = threadIdx.x; i < p.njobs * (uint32_t)(sizeof(BatchJobDev) / 4); i += blockDim.x)
+    ((uint32_t*)jobs)[i] = ((const uint32_t*)p.jobs)[i];
+  __syncthreads();
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t t = p.t0 + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < p.t1; t += warps) {
+    int a = 0, b = (int)p.njobs - 1;
+    while (a < b) {
+      int m = (a + b + 1) >> 1;
+      if (jobs[m].texel_base <= t) a = m; else b = m - 1;
+    }
+    const BatchJobDev& J = jobs[a];
+    const uint32_t g = t - J.texel_base;
+    const float* ts = p.scratch + (J.ray_base + (unsigned long long)g * J.spp - p.r0);
+    uint32_t id = __ldg(J.tidx + g);
+    if (id != kMiss && !valid_hit(id, J.s.corner_count)) id = kMiss;
+    if (id == kMiss) {
+      if (lane == 0) {
+        if (KIND == FK_AO || KIND == FK_AO_BN) J.out0[g] = 1.0f;
+        if (KIND == FK_THICK) J.out0[g] = J.hi;
+        float* bn = KIND == FK_BN ? J.out0 : (KIND == FK_AO_BN ? J.out1 : nullptr);
+        if (bn) { bn[3 * (size_t)g] = 0.0f; bn[3 * (size_t)g + 1] = 0.0f; bn[3 * (size_t)g + 2] = 0.0f; }
+        if (J.hits0) J.hits0[g] = 0;
+        if (J.hits1) J.hits1[g] = 0;
+      }
+      continue;
+    }
+    f3 o, d, tx, ty;
+    if (KIND == FK_BN || KIND == FK_AO_BN) texel_frame(J.s, __ldg(J.coords + g), id, o, d, tx, ty);
+    const float4* row = J.samples + (size_t)(g % J.perms) * J.spp;
+    uint32_t occ = 0, anyhit = 0;
+    float acc = 0.0f;
+    f3 vacc = mk3(0.0f, 0.0f, 0.0f);
+    for (uint32_t k0 = 0; k0 < J.spp; k0 += 32) {
+      const uint32_t k = k0 + lane;
+      const bool on = k < J.spp;
+      const float tk = on ? ts[k] : FLT_MAX;
+      const bool hit = on && tk != FLT_MAX;
+      if (KIND == FK_AO || KIND == FK_AO_BN) occ += __popc(__ballot_sync(full, hit && tk < J.hi));
+      anyhit += __popc(__ballot_sync(full, hit));
+      const int nact = (int)min(32u, J.spp - k0);
+      if (KIND == FK_BN || KIND == FK_AO_BN) {
+        f3 v = mk3(0.0f, 0.0f, 0.0f);
+        if (on && !hit) {
+          float4 rs = __ldg(row + k);
+          v = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+        }
+        for (int i = 0; i < nact; ++i) {
+          vacc.x = __fadd_rn(vacc.x, __shfl_sync(full, v.x, i));
+          vacc.y = __fadd_rn(vacc.y, __shfl_sync(full, v.y, i));
+          vacc.z = __fadd_rn(vacc.z, __shfl_sync(full, v.z, i));
+        }
+      }
+      if (KIND == FK_THICK) {
+        float v = hit ? tk : J.hi;
+        for (int i = 0; i < nact; ++i) acc = __fadd_rn(acc, __shfl_sync(full, v, i));
+      }
+    }
+    if (lane == 0) {
+      const float fs = (float)J.spp;
+      if (KIND == FK_AO || KIND == FK_AO_BN) J.out0[g] = __fsub_rn(1.0f, __fdiv_rn((float)occ, fs));
+      if (KIND == FK_THICK) J.out0[g] = __fdiv_rn(acc, fs);
+      if (KIND == FK_BN || KIND == FK_AO_BN) {
+        float* bn = KIND == FK_BN ? J.out0 : J.out1;
+        f3 v = normalize(vacc);
+        bn[3 * (size_t)g] = v.x;
+        bn[3 * (size_t)g + 1] = v.y;
+        bn[3 * (size_t)g + 2] = v.z;
+      }
+      if (KIND == FK_AO_BN) {
+        if (J.hits0) J.hits0[g] = occ;
+        if (J.hits1) J.hits1[g] = anyhit;
+      } else if (J.hits0) {
+        J.hits0[g] = KIND == FK_AO ? occ : anyhit;
+      }
+    }
+  }
+}
+
+SceneDev scene_dev(const fk_scene* s) { return dev_of(s); }
+
+template <int KIND, int TRAV, bool FILTER>
+static cudaError_t batch_launch(const BatchArgs& a, cudaStream_t stream, int sm_count, bool reduce) {
+  auto trace = batch_trace_kernel<KIND, TRAV, FILTER>;
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace, 256, 0);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  const unsigned long long rays = (a.r1 - a.r0 + a.stride - 1) / a.stride;
+  unsigned long long blocks = (unsigned long long)sm_count * per_sm;
+  if (blocks > (rays + 255) / 256) blocks = (rays + 255) / 256;
+  if (blocks == 0) return cudaSuccess;
+  trace<<<(uint32_t)blocks, 256, 0, stream>>>(a);
+  if ((e = cudaGetLastError()) != cudaSuccess || !reduce) return e;
+  uint32_t rblocks = std::min<uint32_t>((a.t1 - a.t0 + 7) / 8, (uint32_t)sm_count * 8);
+  if (rblocks) batch_reduce_kernel<KIND><<<rblocks, 256, 0, stream>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch(const BatchArgs& a, int kind, int trav, bool filter, cudaStream_t stream, int sm_count,
+                         bool reduce) {
+#define FK_BATCH_CASE(K)                                                                                   \
+  case K:                                                                                                  \
+    if (trav == FK_TRAVERSE_ORDERED)                                                                       \
+      return filter ? batch_launch<K, FK_TRAVERSE_ORDERED, true>(a, stream, sm_count, reduce)             \
+                    : batch_launch<K, FK_TRAVERSE_ORDERED, false>(a, stream, sm_count, reduce);           \
+    return filter ? batch_launch<K, FK_TRAVERSE_SKIP, true>(a, stream, sm_count, reduce)                  \
+                  : batch_launch<K, FK_TRAVERSE_SKIP, false>(a, stream, sm_count, reduce);
+  switch (kind) {
+    FK_BATCH_CASE(FK_AO)
+    FK_BATCH_CASE(FK_BN)
+    FK_BATCH_CASE(FK_THICK)
+    FK_BATCH_CASE(FK_AO_BN)
+    default:
+      return cudaErrorInvalidValue;
+  }
+#undef FK_BATCH_CASE
 }
 
 // ------------------------------------------------------------------ hemisphere, caller scratch

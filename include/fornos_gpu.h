@@ -312,6 +312,47 @@ int fk_solver_hits(fk_solver* s, uint32_t* host_out, size_t count);
 const fk_buf* fk_solver_result_buffer(const fk_solver* s);
 int fk_solver_free(fk_solver* s);
 
+/* ------------------------------------------------------------ batched bakes
+ * No counterpart in the reference (which bakes one mesh pair at a time, one
+ * chunk per UI frame).  Up to 64 hemisphere jobs, each with its own scene,
+ * mapped texels, sample table, parameters and outputs, share one persistent
+ * launch: their rays are laid end to end and every lane maps its ray back to
+ * its job, so small and large jobs keep the whole GPU busy together.  Results
+ * are those fk_hemisphere gives per job. */
+typedef struct fk_batch fk_batch;
+typedef struct fk_batch_job {
+  const fk_scene* scene;
+  const fk_buf* coords;      /* fk_meshmap output for the job's texels 0 .. texel_count-1 */
+  const fk_buf* tidx;
+  uint32_t texel_count;
+  fk_sample_params params;
+  const fk_buf* samples;     /* perm_count x sample_count table (fk_samples_cosine) */
+  fk_buf* out0;              /* outputs as fk_hemisphere writes them for the batch's kind */
+  fk_buf* out1;
+  fk_buf* hits0;
+  fk_buf* hits1;
+} fk_batch_job;
+
+int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t job_count, int kind, fk_batch** out);
+int fk_batch_info(const fk_batch* batch, uint64_t* rays, uint32_t* texels, uint32_t* launches_per_run);
+/* Autotuner: times a strided sample of about sample_rays rays of every job
+ * (0 = 4M) under each candidate schedule (ordered vs skip-pointer traversal,
+ * filtered vs divided box tests, refill threshold, postponed-leaf batch) and
+ * keeps the fastest for later runs; reports it. */
+int fk_batch_tune(fk_batch* batch, uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse);
+/* One run on the context's stream; traverse 0 = the tuned schedule. */
+int fk_batch_run(fk_batch* batch, int traverse);
+/* Records fk_batch_run into a CUDA graph; fk_batch_replay launches it. */
+int fk_batch_capture(fk_batch* batch, int traverse);
+int fk_batch_replay(fk_batch* batch);
+int fk_batch_free(fk_batch* batch);
+
+/* The autotuner for one fk_hemisphere call (same arguments); apply the result
+ * with fk_ctx_set_tuning and the returned traverse flags. */
+int fk_tune_hemisphere(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
+                       const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
+                       uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse);
+
 /* ------------------------------------------------------------ one-shot bake
  * FornosRunner::start + run (Src/fornos.cpp:53-251) from host arrays, after
  * the host preprocessing (mesh loading, normals, BVH build, texel map): uploads
