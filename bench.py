@@ -488,9 +488,10 @@ def run_batch_bench(args):
     rays = sum(j["texel_count"] * j["spp"] for j in jobs)
 
     def timed(fn):
+        # one pass each: a pass is tens of seconds of GPU work, and every job's
+        # scene and texels are already resident
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with torch.cuda.stream(stream):
-            fn()  # warm-up
             stream.synchronize()
             a.record(stream)
             fn()
