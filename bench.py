@@ -487,16 +487,19 @@ def run_batch_bench(args):
     ctx.sync()
     rays = sum(j["texel_count"] * j["spp"] for j in jobs)
 
-    def timed(fn):
-        # one pass each: a pass is tens of seconds of GPU work, and every job's
-        # scene and texels are already resident
+    clocks = {}
+
+    def timed(fn, name):
+        # one pass per call (tens of seconds of GPU work, every job's scene and
+        # texels already resident), with the SM clock sampled during it
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
+        with ClockSampler(0) as clk, torch.cuda.stream(stream):
             stream.synchronize()
             a.record(stream)
             fn()
             b.record(stream)
-        stream.synchronize()
+            stream.synchronize()
+        clocks.setdefault(name, []).append(clk.summary())
         return a.elapsed_time(b)
 
     def per_job():
@@ -504,16 +507,21 @@ def run_batch_bench(args):
             api.hemisphere(ctx, j["scene"], j["coords"], j["tidx"], api.AO, j["spp"], j["min_distance"],
                            j["max_distance"], j["samples"], j["out0"], None, j["hits0"], None, 0, j["texel_count"])
 
-    t_jobs = timed(per_job)
-    want = [(j["out0"].download(np.float32, j["texel_count"]), j["hits0"].download(np.uint32, j["texel_count"]))
-            for j in jobs]
     outs = [dict(out0=ctx.buffer(4 * j["texel_count"]), hits0=ctx.buffer(4 * j["texel_count"])) for j in jobs]
     batch = api.Batch(ctx, [dict(j, **o) for j, o in zip(jobs, outs)], api.AO)
-    t_batch = timed(lambda: batch.run())
+    # per-job and batched passes alternate, twice, so that neither arm runs on
+    # a cooler GPU than the other; each arm keeps its faster pass
+    t_jobs, t_batch = [], []
+    for _ in range(2):
+        t_jobs.append(timed(per_job, "per_job_launches"))
+        t_batch.append(timed(lambda: batch.run(), "batch_default"))
+    want = [(j["out0"].download(np.float32, j["texel_count"]), j["hits0"].download(np.uint32, j["texel_count"]))
+            for j in jobs]
     tuned = batch.tune()
-    t_tuned = timed(lambda: batch.run())
+    t_tuned = timed(lambda: batch.run(), "batch_tuned")
     batch.capture()
-    t_graph = timed(lambda: batch.replay())
+    t_graph = timed(lambda: batch.replay(), "batch_tuned_graph")
+    t_jobs, t_batch = min(t_jobs), min(t_batch)
     identical = all(np.array_equal(o["out0"].download(np.float32, j["texel_count"]).view(np.uint32), w[0].view(np.uint32))
                     and np.array_equal(o["hits0"].download(np.uint32, j["texel_count"]), w[1])
                     for j, o, w in zip(jobs, outs, want))
@@ -530,6 +538,7 @@ def run_batch_bench(args):
         "batch_tuned": {"ms": round(t_tuned, 2), "mrays": mr(t_tuned), "tuning": tuned},
         "batch_tuned_graph": {"ms": round(t_graph, 2), "mrays": mr(t_graph), "info": batch.info()},
         "batch_equals_per_job": bool(identical),
+        "clocks": clocks,
     }
 
 

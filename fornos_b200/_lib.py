@@ -72,6 +72,21 @@ class BakeOut(ctypes.Structure):
                 ("ao", f32p), ("bent_normals3", f32p), ("thickness", f32p)]
 
 
+class Adam(ctypes.Structure):
+    _fields_ = [("learning_rate", c_float), ("beta1", c_float), ("beta2", c_float), ("eps", c_float)]
+
+
+class DenoiseParams(ctypes.Structure):
+    _fields_ = [("low_samples", c_u32), ("full_samples", c_u32), ("perm_count", c_u32), ("min_distance", c_float),
+                ("max_distance", c_float), ("tile", c_u32), ("verify_cells", c_u32), ("max_tile_error", c_float),
+                ("traverse", c_int)]
+
+
+class DenoiseStats(ctypes.Structure):
+    _fields_ = [("tiles", c_u32), ("tiles_failed", c_u32), ("spot_checks", c_u32), ("texels_rebaked", c_u32),
+                ("rays", c_u64), ("worst_tile_error", c_float)]
+
+
 # name: (restype, argtypes)
 _SIGS = {
     "fk_ctx_create": (c_int, [c_int, ctypes.POINTER(c_vp)]),
@@ -113,6 +128,9 @@ _SIGS = {
     "fk_meshmap": (c_int, [c_vp, c_vp, c_vp, c_int, c_u32, c_u32, c_vp, c_vp]),
     "fk_hemisphere": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32, c_u32,
                               c_int, c_vp, c_vp, c_vp, c_vp]),
+    "fk_hemisphere_texels": (c_int, [c_vp, c_vp, c_vp, c_vp, c_u32, c_int, ctypes.POINTER(SampleParams), c_vp, c_vp,
+                                     c_u32, c_u32, c_int, c_vp, c_vp, c_vp, c_vp]),
+    "fk_ctx_check": (c_int, [c_vp]),
     "fk_gather": (c_int, [c_vp, c_vp, c_int, c_vp, c_vp, c_u32, c_u32, c_vp]),
     "fk_tangent_space": (c_int, [c_vp, c_vp, c_u32, c_u32, c_vp]),
     "fk_hemisphere_noalloc": (c_int, [c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32, c_u32,
@@ -151,6 +169,20 @@ _SIGS = {
     "fk_diag_fp32_peak": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double)]),
     "fk_diag_traversal_counts": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32,
                                          c_u32, c_int, ctypes.POINTER(c_u64)]),
+    "fk_denoiser_create": (c_int, [c_vp, ctypes.POINTER(c_vp)]),
+    "fk_denoiser_free": (c_int, [c_vp]),
+    "fk_denoiser_set_params": (c_int, [c_vp, f32p, c_u32]),
+    "fk_denoiser_get_params": (c_int, [c_vp, f32p, c_u32]),
+    "fk_denoise_features": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_float, c_vp]),
+    "fk_denoise_rows": (c_int, [c_vp, c_vp, c_u32, c_u32, c_vp, c_u32, c_vp]),
+    "fk_denoiser_train_step": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_u32, c_u32, ctypes.POINTER(Adam)]),
+    "fk_denoiser_last_loss": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double)]),
+    "fk_denoiser_gradient": (c_int, [c_vp, c_vp, c_vp, c_u32, c_vp, c_u32, c_u32, f32p,
+                                     ctypes.POINTER(ctypes.c_double)]),
+    "fk_denoiser_forward": (c_int, [c_vp, c_vp, c_u32, c_vp]),
+    "fk_denoise_apply": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_u32, c_u32, c_vp, c_vp]),
+    "fk_denoise_bake": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(DenoiseParams), c_vp, c_vp, c_vp, c_vp,
+                                ctypes.POINTER(DenoiseStats)]),
 }
 
 _lib = None

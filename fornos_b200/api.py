@@ -81,6 +81,11 @@ class Context:
     def sync(self):
         _check(self.lib.fk_sync(self.handle), self)
 
+    def check(self):
+        """Waits for the stream; raises FornosError when a kernel flagged an
+        error since the last check (fk_ctx_check)."""
+        _check(self.lib.fk_ctx_check(self.handle), self, "fk_ctx_check")
+
     @property
     def launches(self):
         return int(self.lib.fk_launch_count(self.handle))
@@ -360,6 +365,18 @@ def hemisphere(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, out0,
            ctx, "fk_hemisphere")
 
 
+def hemisphere_texels(ctx, scene, coords, tidx, texel_count, kind, spp, min_d, max_d, samples, ids, out0, out1=None,
+                      hits0=None, hits1=None, offset=0, count=None, perms=PERMS, traverse=TRAVERSE_AUTO):
+    """fk_hemisphere over the texels listed in `ids` (u32 buffer); each listed
+    texel gets exactly the value a whole-map pass gives it."""
+    count = ids.nbytes // 4 - offset if count is None else count
+    p = L.SampleParams(spp, perms, min_d, max_d)
+    hv = lambda b: b.handle if b is not None else None
+    _check(ctx.lib.fk_hemisphere_texels(ctx.handle, scene.handle, coords.handle, tidx.handle, texel_count, kind,
+                                        ctypes.byref(p), samples.handle, ids.handle, offset, count, traverse,
+                                        out0.handle, hv(out1), hv(hits0), hv(hits1)), ctx, "fk_hemisphere_texels")
+
+
 def gather(ctx, scene, kind, coords, tidx, out, offset=0, count=0):
     _check(ctx.lib.fk_gather(ctx.handle, scene.handle, kind, coords.handle, tidx.handle, offset, count, out.handle),
            ctx, "fk_gather")
@@ -633,3 +650,111 @@ def tune_hemisphere(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, 
                                       samples.handle, offset, count, sample_rays, ctypes.byref(t),
                                       ctypes.byref(trav)), ctx, "fk_tune_hemisphere")
     return {"refill": t.refill, "leaf_batch": t.leaf_batch, "speculate": t.speculate}, trav.value
+
+
+# ------------------------------------------------------------------ learned denoiser
+DN_INPUTS = 250
+DN_PARAMS = 20868
+DN_ROW_BYTES = 512
+DN_TILE_ROWS = 128
+DN_HIDDEN = 64
+DN_OUT = 4
+# parameter blocks: name -> (offset, shape)
+DN_LAYOUT = {"w1": (0, (64, 256)), "b1": (16384, (64,)), "w2": (16448, (64, 64)), "b2": (20544, (64,)),
+             "w3": (20608, (4, 64)), "b3": (20864, (4,))}
+
+
+def denoise_features(ctx, tmap, coords, tidx, ao, bn3, pos3, nrm3, max_distance, image=None):
+    """Dense feature image (3 planes of W x H float4) of a texel map."""
+    if image is None:
+        image = ctx.buffer(48 * tmap.width * tmap.height)
+    _check(ctx.lib.fk_denoise_features(ctx.handle, tmap.handle, coords.handle, tidx.handle, ao.handle, bn3.handle,
+                                       pos3.handle, nrm3.handle, max_distance, image.handle), ctx,
+           "fk_denoise_features")
+    return image
+
+
+def denoise_rows(ctx, image, width, height, pixels, count, rows=None):
+    """Network input rows (256 bf16 each) for `count` pixel indices."""
+    if rows is None:
+        rows = ctx.buffer(max(count, 1) * DN_ROW_BYTES)
+    _check(ctx.lib.fk_denoise_rows(ctx.handle, image.handle, width, height, pixels.handle, count, rows.handle), ctx,
+           "fk_denoise_rows")
+    return rows
+
+
+class Denoiser:
+    """The learned AO + bent-normal denoiser (fk_denoiser)."""
+
+    def __init__(self, ctx, params=None):
+        self.ctx = ctx
+        h = L.c_vp()
+        _check(ctx.lib.fk_denoiser_create(ctx.handle, ctypes.byref(h)), ctx, "fk_denoiser_create")
+        self.handle = h.value
+        if params is not None:
+            self.set_params(params)
+
+    def set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32).reshape(-1)
+        _check(self.ctx.lib.fk_denoiser_set_params(self.handle, _f32(p), p.size), self.ctx, "fk_denoiser_set_params")
+
+    def get_params(self):
+        p = np.empty(DN_PARAMS, np.float32)
+        _check(self.ctx.lib.fk_denoiser_get_params(self.handle, _f32(p), p.size), self.ctx, "fk_denoiser_get_params")
+        return p
+
+    def train_step(self, rows, targets, n_rows, batch, row_ids=None, offset=0, lr=1e-3, beta1=0.9, beta2=0.999,
+                   eps=1e-8):
+        a = L.Adam(lr, beta1, beta2, eps)
+        _check(self.ctx.lib.fk_denoiser_train_step(self.handle, rows.handle, targets.handle, n_rows,
+                                                   row_ids.handle if row_ids is not None else None, offset, batch,
+                                                   ctypes.byref(a)), self.ctx, "fk_denoiser_train_step")
+
+    def last_loss(self):
+        v = ctypes.c_double()
+        _check(self.ctx.lib.fk_denoiser_last_loss(self.handle, ctypes.byref(v)), self.ctx, "fk_denoiser_last_loss")
+        return v.value
+
+    def gradient(self, rows, targets, n_rows, batch, row_ids=None, offset=0):
+        g = np.empty(DN_PARAMS, np.float32)
+        v = ctypes.c_double()
+        _check(self.ctx.lib.fk_denoiser_gradient(self.handle, rows.handle, targets.handle, n_rows,
+                                                 row_ids.handle if row_ids is not None else None, offset, batch,
+                                                 _f32(g), ctypes.byref(v)), self.ctx, "fk_denoiser_gradient")
+        return g, v.value
+
+    def forward(self, rows, count, y4=None):
+        if y4 is None:
+            y4 = self.ctx.buffer(max(count, 1) * 16)
+        _check(self.ctx.lib.fk_denoiser_forward(self.handle, rows.handle, count, y4.handle), self.ctx,
+               "fk_denoiser_forward")
+        return y4
+
+    def apply(self, tmap, image, tidx, ao_in, bn_in, ao_out, bn_out, offset=0, count=None):
+        count = tmap.count - offset if count is None else count
+        _check(self.ctx.lib.fk_denoise_apply(self.handle, tmap.handle, image.handle, tidx.handle, ao_in.handle,
+                                             bn_in.handle, offset, count, ao_out.handle, bn_out.handle), self.ctx,
+               "fk_denoise_apply")
+
+    def bake(self, scene, tmap, coords, tidx, samples_low, samples_full, ao_out, bn_out, low_samples=16,
+             full_samples=1024, min_distance=0.001, max_distance=0.3, perms=PERMS, tile=64, verify_cells=4,
+             max_tile_error=0.02, traverse=TRAVERSE_AUTO):
+        """The verified denoised AO + bent-normal bake; returns its statistics."""
+        p = L.DenoiseParams(low_samples, full_samples, perms, min_distance, max_distance, tile, verify_cells,
+                            max_tile_error, traverse)
+        st = L.DenoiseStats()
+        _check(self.ctx.lib.fk_denoise_bake(self.handle, scene.handle, tmap.handle, coords.handle, tidx.handle,
+                                            ctypes.byref(p), samples_low.handle, samples_full.handle, ao_out.handle,
+                                            bn_out.handle, ctypes.byref(st)), self.ctx, "fk_denoise_bake")
+        return {k: getattr(st, k) for k, _ in L.DenoiseStats._fields_}
+
+    def free(self):
+        if self.handle and self.ctx.handle:
+            self.ctx.lib.fk_denoiser_free(self.handle)
+        self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

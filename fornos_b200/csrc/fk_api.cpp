@@ -70,6 +70,52 @@ int fk_hemisphere(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk
   return fk::launch_hemisphere(ctx, s, h);
 }
 
+int fk_hemisphere_texels(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk_buf* tidx,
+                         uint32_t texel_count, int kind, const fk_sample_params* prm, const fk_buf* samples,
+                         const fk_buf* ids, uint32_t offset, uint32_t count, int traverse, fk_buf* out0, fk_buf* out1,
+                         fk_buf* hits0, fk_buf* hits1) {
+  if (!ctx || !s || !coords || !tidx || !prm || !samples || !ids || !out0)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: null argument");
+  if (kind < FK_AO || kind > FK_AO_BN) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: unknown kind");
+  if (prm->sample_count == 0 || prm->perm_count == 0)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: zero samples");
+  if ((traverse & ~(FK_TRAVERSE_MASK | FK_SCHEDULE_MASK | FK_EXACT_BOX_TESTS)) ||
+      (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_SKIP || (traverse & FK_SCHEDULE_MASK) > FK_SCHEDULE_DYNAMIC)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: unknown traversal or schedule");
+  if ((traverse & FK_SCHEDULE_MASK) == FK_SCHEDULE_STATIC)
+    return fk_fail(ctx, FK_ERR_UNSUPPORTED, "fk_hemisphere_texels: texel lists run on the dynamic schedule only");
+  const uint64_t n = texel_count;
+  if (!fits(ids, 4 * ((uint64_t)offset + count))) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: id list too small");
+  if (!fits(coords, 16 * n) || !fits(tidx, 4 * n))
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: mapping buffers smaller than texel_count");
+  if (!fits(samples, 16ull * prm->sample_count * prm->perm_count))
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: sample table smaller than perm_count x sample_count");
+  if (!fits(out0, (kind == FK_BN ? 12 : 4) * n) || (kind == FK_AO_BN && !fits(out1, 12 * n)))
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: output buffers smaller than texel_count");
+  if ((hits0 && !fits(hits0, 4 * n)) || (kind == FK_AO_BN && hits1 && !fits(hits1, 4 * n)))
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: hit buffers smaller than texel_count");
+  if (count == 0) return FK_OK;
+  fk::HemiLaunch h;
+  h.kind = kind;
+  h.spp = prm->sample_count;
+  h.perms = prm->perm_count;
+  h.min_d = prm->min_distance;
+  h.max_d = prm->max_distance;
+  h.samples = (const float4*)samples->ptr;
+  h.coords = (const float4*)coords->ptr;
+  h.tidx = (const uint32_t*)tidx->ptr;
+  h.offset = offset;
+  h.count = count;
+  h.traverse = traverse;
+  h.out0 = (float*)out0->ptr;
+  h.out1 = kind == FK_AO_BN ? (float*)out1->ptr : nullptr;
+  h.hits0 = hits0 ? (uint32_t*)hits0->ptr : nullptr;
+  h.hits1 = (kind == FK_AO_BN && hits1) ? (uint32_t*)hits1->ptr : nullptr;
+  h.ids = (const uint32_t*)ids->ptr;
+  h.texel_limit = texel_count;
+  return fk::launch_hemisphere(ctx, s, h);
+}
+
 int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk_buf* tidx, int kind,
                              const fk_sample_params* prm, const fk_buf* samples, uint32_t offset, uint32_t count,
                              int traverse, uint64_t* tests) {
@@ -381,15 +427,20 @@ size_t fk_solver_result_count(const fk_solver* s) {
   return s && s->ready ? (size_t)floats_per_texel(s->p.kind) * s->work_count : 0;
 }
 
-static int check_status(fk_ctx* ctx) {
+int fk_ctx_check(fk_ctx* ctx) {
+  if (!ctx) return FK_ERR_INVALID;
   int st = 0;
   FK_CUDA(ctx, cudaMemcpyAsync(&st, ctx->status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-  if (st) {
-    cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream);
-    return fk_fail(ctx, FK_ERR_DEVICE, "a traversal exceeded its stack; results are incomplete");
-  }
-  return FK_OK;
+  if (!st) return FK_OK;
+  cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream);
+  std::string msg;
+  if (st & 1) msg += "a traversal exceeded its stack; ";
+  if (st & 2) msg += "a texel names a triangle outside the scene; ";
+  if (st & 4) msg += "a texel list holds an id beyond texel_count; ";
+  if (st & 8) msg += "a training batch names a row beyond n_rows; ";
+  msg += "results are incomplete";
+  return fk_fail(ctx, FK_ERR_DEVICE, msg.c_str());
 }
 
 // getResults (e.g. Src/solver_ao.cpp:70-75): the whole padded result buffer.
@@ -398,7 +449,7 @@ int fk_solver_results(fk_solver* s, float* out, size_t floats) {
   if (!s->ready) return fk_fail(s->ctx, FK_ERR_STATE, "fk_solver_results: not initialised");
   size_t n = fk_solver_result_count(s);
   if (floats < n) return fk_fail(s->ctx, FK_ERR_INVALID, "fk_solver_results: host buffer too small");
-  int rc = check_status(s->ctx);
+  int rc = fk_ctx_check(s->ctx);
   if (rc != FK_OK) return rc;
   return fk_buf_download(s->ctx, s->result, 0, out, 4 * n);
 }

@@ -158,6 +158,11 @@ struct HemiLaunch {
   uint32_t refill = 0;                  // dynamic schedule: idle lanes that trigger a refill (0 = context tuning)
   uint32_t leaf_batch = 0;              // postponed leaves that start a leaf phase (0 = context tuning)
   uint32_t speculate = 0;
+  // Texel list (dynamic schedule only): ray texel g is texel ids[g] for the
+  // mapping inputs, the sample permutation and the outputs; ids at or above
+  // texel_limit are skipped and flag status bit 4.
+  const uint32_t* ids = nullptr;
+  uint32_t texel_limit = 0;
 };
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h);
 // Same kernels over caller-provided scratch: `dist` holds count x spp floats,
@@ -169,6 +174,52 @@ int launch_gather(fk_ctx* ctx, const fk_scene* s, int kind, const float4* coords
 int launch_tangent_space(fk_ctx* ctx, const fk_texel_map* m, uint32_t offset, uint32_t count, float* io3);
 int launch_tri_records(fk_ctx* ctx, fk_scene* s);
 struct RasterTri;  // defined in fk_raster.cu
+
+// Learned denoiser: parameter layout (fp32, row-major) and kernel launchers.
+namespace dn {
+constexpr int kInputs = 250, kK1 = 256, kHidden = 64, kOut = 4, kRows = 128;
+constexpr int kW1 = 0;                        // [64][256], columns 250..255 zero
+constexpr int kB1 = kW1 + kHidden * kK1;      // [64]
+constexpr int kW2 = kB1 + kHidden;            // [64 out][64 in]
+constexpr int kB2 = kW2 + kHidden * kHidden;  // [64]
+constexpr int kW3 = kB2 + kHidden;            // [4 out][64 in]
+constexpr int kB3 = kW3 + kOut * kHidden;     // [4]
+constexpr int kParams = kB3 + kOut;
+}  // namespace dn
+// fp32 parameters (biases are read from here) and bf16 working copies:
+// w1 [64][256], w2 [64][64] (out, in), w2t (in, out), w3 [8][64] (rows 4..7
+// zero), w3t [64][8].
+struct DnWeights {
+  const float* params;
+  const void *w1, *w2, *w2t, *w3, *w3t;
+};
+namespace dn {
+size_t train_smem_bytes();
+size_t apply_smem_bytes();
+cudaError_t launch_features(cudaStream_t st, uint32_t n, uint32_t w, uint32_t h, const uint32_t* indices,
+                            const uint32_t* tidx, const float4* coords, const float* ao, const float* bn3,
+                            const float* pos3, const float* nrm3, float max_d, float4* image);
+cudaError_t launch_rows(cudaStream_t st, const float4* image, uint32_t w, uint32_t h, const uint32_t* pixels,
+                        uint32_t n, uint32_t* rows);
+cudaError_t launch_train(cudaStream_t st, const uint32_t* rows, const float4* targets, const uint32_t* row_ids,
+                         uint32_t nrows, uint32_t offset, uint32_t batch, const DnWeights& wt, float* partials,
+                         float* loss, int* status);
+cudaError_t launch_adam(cudaStream_t st, const float* partials, uint32_t tiles, float* params, float* m, float* v,
+                        float* grad_out, int update, float lr, float beta1, float beta2, float eps, float c1, float c2,
+                        const DnWeights& wt);
+cudaError_t launch_refresh(cudaStream_t st, const DnWeights& wt);
+cudaError_t launch_apply(cudaStream_t st, int sm_count, const float4* image, uint32_t w, uint32_t h,
+                         const uint32_t* indices, const uint32_t* tidx, const float* ao_in, const float* bn_in,
+                         uint32_t offset, uint32_t count, const DnWeights& wt, float* ao_out, float* bn_out,
+                         const uint32_t* rows, float4* y_out);
+cudaError_t launch_inverse(cudaStream_t st, uint32_t n, const uint32_t* indices, uint32_t pixels, uint32_t* inv);
+cudaError_t launch_verify_slots(cudaStream_t st, uint32_t w, uint32_t h, uint32_t tile, uint32_t cells,
+                                const uint32_t* inv, const uint32_t* tidx, uint32_t* slots);
+cudaError_t launch_tile_error(cudaStream_t st, uint32_t tiles, uint32_t per, const uint32_t* slots, const float* ao_d,
+                              const float* bn_d, const float* ao_v, const float* bn_v, float* err);
+cudaError_t launch_fallback_list(cudaStream_t st, uint32_t n, uint32_t w, uint32_t tile, const uint32_t* indices,
+                                 const uint32_t* tidx, const uint8_t* failed, uint32_t* list, uint32_t* count);
+}  // namespace dn
 }  // namespace fk
 
 // Host mesh (Src/mesh.h:35-63).

@@ -233,6 +233,8 @@ struct HemiArgs {
   uint32_t* queue;
   int* status;
   unsigned long long* tally;  // counting variant: total box tests, triangle tests
+  const uint32_t* __restrict__ ids;  // texel list (dynamic schedule), or null
+  uint32_t texel_limit;              // ids must stay below this
 };
 
 // Ray frame of Shaders/ao_step0.comp:39-50.
@@ -381,12 +383,16 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   a.queue = fk_take_counter(ctx);
   a.status = ctx->status;
   a.tally = h.tally;
+  a.ids = h.ids;
+  a.texel_limit = h.texel_limit;
   int trav = h.traverse & FK_TRAVERSE_MASK;
   int sched = h.traverse & FK_SCHEDULE_MASK;
   if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
   if (trav == FK_TRAVERSE_ORDERED && s->depth > kMaxOrderedDepth)
     return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 48; use FK_TRAVERSE_SKIP");
   if (sched == 0) sched = FK_SCHEDULE_DYNAMIC;
+  if (h.ids && sched != FK_SCHEDULE_DYNAMIC)
+    return fk_fail(ctx, FK_ERR_UNSUPPORTED, "texel lists run on the dynamic schedule only");
   const uint32_t refill = h.refill ? h.refill : ctx->tuning.refill;
   const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
   const uint32_t leaf_batch = h.leaf_batch ? h.leaf_batch : ctx->tuning.leaf_batch;
@@ -433,7 +439,22 @@ struct DynArgs {
   uint32_t* queue;
   int* status;
   unsigned long long* tally;
+  const uint32_t* __restrict__ ids;  // texel list, or null: ray texel g is ids[g]
+  uint32_t texel_limit;
 };
+
+// Texel of list position g: itself, or ids[g] for a texel list.  An id at or
+// beyond the limit is reported (status bit 4) and yields kMiss, so nothing is
+// read or written for it.
+__device__ __forceinline__ uint32_t list_texel(const uint32_t* ids, uint32_t limit, uint32_t g, int* status) {
+  if (!ids) return g;
+  const uint32_t t = __ldg(ids + g);
+  if (t >= limit) {
+    atomicOr(status, 4);
+    return kMiss;
+  }
+  return t;
+}
 
 // Child box test of the traversal kernels: exact quotients, or the filtered
 // form (fk_device.cuh: box_hit) whose decision is provably the same.
@@ -591,8 +612,9 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
       if (!active) {
         r = base + __popc(idle & lower);
         if (r < p.total) {
-          const uint32_t g = p.texel0 + r / p.spp, k = r % p.spp;
-          const uint32_t id = __ldg(p.tidx + g);
+          const uint32_t k = r % p.spp;
+          const uint32_t g = list_texel(p.ids, p.texel_limit, p.texel0 + r / p.spp, p.status);
+          const uint32_t id = g == kMiss ? kMiss : __ldg(p.tidx + g);
           best = FLT_MAX;
           bool done = true;
           if (id != kMiss && valid_hit(id, p.s.corner_count)) {
@@ -680,7 +702,11 @@ __global__ void __launch_bounds__(256) hemi_reduce_kernel(HemiArgs p, const floa
   const int lane = threadIdx.x & 31;
   const uint32_t warps = gridDim.x * (blockDim.x >> 5);
   for (uint32_t item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < p.count; item += warps) {
-    const uint32_t g = texel0 + item;
+    uint32_t g = texel0 + item;
+    if (p.ids) {
+      g = __ldg(p.ids + g);
+      if (g >= p.texel_limit) continue;  // reported by the trace kernel
+    }
     uint32_t id = __ldg(p.tidx + g);
     if (id != kMiss && !valid_hit(id, p.s.corner_count)) id = kMiss;
     if (id == kMiss) {
@@ -781,6 +807,8 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
     d.queue = fk_take_counter(ctx);
     d.status = a.status;
     d.tally = a.tally;
+    d.ids = a.ids;
+    d.texel_limit = a.texel_limit;
     uint32_t blocks = (uint32_t)ctx->sm_count * (uint32_t)per_sm;
     uint32_t need = (d.total + 255) / 256;
     if (blocks > need) blocks = need;
@@ -814,12 +842,13 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
-  const unsigned long long total = (p.r1 - p.r0 + p.stride - 1) / p.stride;
+  // a launch traces at most the scratch's 2^27 rays: lane indices fit 32 bits
+  const uint32_t total = (uint32_t)((p.r1 - p.r0 + p.stride - 1) / p.stride);
   int32_t stack_node[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
   float stack_dist[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
   Tally tally;
   bool active = false, exhausted = false;
-  unsigned long long q = 0;
+  uint32_t q = 0;
   int j = 0;
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX, lo = 0.0f, hi = 0.0f;
@@ -831,14 +860,14 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
     if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
       const uint32_t n_idle = __popc(idle);
       const int leader = __ffs(idle) - 1;
-      unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(p.queue, (unsigned long long)n_idle);
+      uint32_t base = 0;
+      if (lane == leader) base = (uint32_t)atomicAdd(p.queue, (unsigned long long)n_idle);
       base = __shfl_sync(full, base, leader);
-      if (base + n_idle >= total) exhausted = true;
+      if ((unsigned long long)base + n_idle >= total) exhausted = true;
       if (!active) {
         q = base + __popc(idle & lower);
         if (q < total) {
-          const unsigned long long r = p.r0 + q * p.stride;
+          const unsigned long long r = p.r0 + (unsigned long long)q * p.stride;
           int a = 0, b = (int)p.njobs - 1;  // last job whose ray_base <= r
           while (a < b) {
             int m = (a + b + 1) >> 1;
@@ -1072,6 +1101,8 @@ static cudaError_t run_hemi_external(const HemiArgs& a, cudaStream_t stream, int
   d.queue = queue;
   d.status = a.status;
   d.tally = nullptr;
+  d.ids = nullptr;
+  d.texel_limit = 0;
   uint32_t blocks = (uint32_t)sm_count * (uint32_t)per_sm;
   uint32_t need = (d.total + 255) / 256;
   if (blocks > need) blocks = need;
@@ -1102,6 +1133,8 @@ int launch_hemisphere_external(const fk_scene* s, const HemiLaunch& h, cudaStrea
   a.queue = queue;
   a.status = status;
   a.tally = nullptr;
+  a.ids = nullptr;
+  a.texel_limit = 0;
   int trav = h.traverse & FK_TRAVERSE_MASK;
   if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
   if (trav == FK_TRAVERSE_ORDERED && s->depth > kMaxOrderedDepth) {

@@ -223,6 +223,26 @@ int fk_hemisphere(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, cons
                   const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
                   int traverse, fk_buf* out0, fk_buf* out1, fk_buf* out_hits0, fk_buf* out_hits1);
 
+/* No counterpart in the reference.  fk_hemisphere over a texel list: the
+ * texels ids[offset .. offset + count) (u32 indices into coords / tidx and
+ * the outputs), each traced and written exactly as a whole-map fk_hemisphere
+ * call traces and writes it (same sample permutation: texel index modulo
+ * perm_count), other texels untouched.  Used for spot checks at full sample
+ * count and for re-baking selected tiles.  `texel_count` bounds the ids:
+ * coords / tidx / outputs must hold that many texels; the kernels skip ids
+ * at or above it and flag the context, so the next fk_ctx_check reports
+ * FK_ERR_DEVICE.  Dynamic schedule only (FK_SCHEDULE_STATIC is refused). */
+int fk_hemisphere_texels(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx,
+                         uint32_t texel_count, int kind, const fk_sample_params* params, const fk_buf* samples4,
+                         const fk_buf* ids, uint32_t offset, uint32_t count, int traverse, fk_buf* out0,
+                         fk_buf* out1, fk_buf* out_hits0, fk_buf* out_hits1);
+
+/* Waits for the context's stream and reads the kernels' error flags (then
+ * clears them): FK_ERR_DEVICE with a message when a traversal overflowed its
+ * stack, a texel named an invalid triangle or a texel list held an id out of
+ * range; FK_OK otherwise. */
+int fk_ctx_check(fk_ctx* ctx);
+
 /* Gathers, Shaders/heights.comp, positions.comp, normals.comp, over texels
  * [offset, offset + count).  HEIGHT: float; POSITION / NORMAL: 3 floats.
  * Missed texels: height 0 (the shader's rule), position / normal (0,0,0). */
@@ -415,6 +435,102 @@ int fk_diag_fp32_peak(fk_ctx* ctx, double* ops_per_second);
 int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
                              const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
                              int traverse, uint64_t* tests);
+
+/* ------------------------------------------------------------ learned denoiser
+ * No counterpart in the reference.  A per-texel MLP that turns a low-sample
+ * AO + bent-normal bake into an estimate of the full-sample one, from a 5 x 5
+ * texel neighbourhood of 10 features per texel: AO, bent normal (2-D
+ * octahedral), position relative to the centre texel / max distance (3),
+ * interpolated normal (octahedral, 2), mapping hit distance / max distance and
+ * coverage (mapping hit).  Network 250 -> 64 -> 64 -> 4 with tanh-form GELU,
+ * BF16 weights and activations, FP32 accumulation; outputs are residuals: AO =
+ * clamp(AO_low + y0, 0, 1), BN = normalize(BN_low + y1..3).
+ *
+ * Parameters (FK_DN_PARAMS fp32, row-major): W1 [64][256] (input columns
+ * 250..255 are padding and held at zero), b1 [64], W2 [64 out][64 in], b2
+ * [64], W3 [4][64], b3 [4].
+ *
+ * The feature image is 3 planes of W x H float4 (48 bytes per pixel); an input
+ * row is 256 bf16 (512 bytes).  Training runs the project's own kernels:
+ * forward, MSE loss on the residual targets (dAO, dBN.xyz), backward, and Adam
+ * with FP32 master weights and moments. */
+#define FK_DN_INPUTS 250
+#define FK_DN_ROW_BYTES 512
+#define FK_DN_PARAMS 20868
+#define FK_DN_TILE_ROWS 128 /* training batches are multiples of this */
+
+typedef struct fk_denoiser fk_denoiser;
+
+int fk_denoiser_create(fk_ctx* ctx, fk_denoiser** out);
+int fk_denoiser_free(fk_denoiser* d);
+/* Host fp32 parameters in the layout above (count = FK_DN_PARAMS); setting
+ * them zeroes W1's padding columns and resets the optimiser state. */
+int fk_denoiser_set_params(fk_denoiser* d, const float* params, uint32_t count);
+int fk_denoiser_get_params(fk_denoiser* d, float* params, uint32_t count);
+
+/* Dense feature image (48 x W x H bytes) of a texel map's texels from a
+ * low-sample AO (float) + bent normal (3 floats) bake, world positions and
+ * normals (fk_gather POSITION / NORMAL) and the mapping (coords / tidx);
+ * pixels without a mapping hit stay zero. */
+int fk_denoise_features(fk_ctx* ctx, const fk_texel_map* map, const fk_buf* coords, const fk_buf* tidx,
+                        const fk_buf* ao, const fk_buf* bn3, const fk_buf* pos3, const fk_buf* nrm3,
+                        float max_distance, fk_buf* image);
+/* Network input rows for `count` pixels (u32 pixel indices y * W + x). */
+int fk_denoise_rows(fk_ctx* ctx, const fk_buf* image, uint32_t width, uint32_t height, const fk_buf* pixels,
+                    uint32_t count, fk_buf* rows);
+
+typedef struct {
+  float learning_rate, beta1, beta2, eps;
+} fk_adam;
+/* One optimiser step over `batch` rows (a multiple of FK_DN_TILE_ROWS):
+ * dataset rows row_ids[offset .. offset + batch) (row_ids NULL: rows offset ..
+ * offset + batch) of `rows` (n_rows input rows) with float4 targets. */
+int fk_denoiser_train_step(fk_denoiser* d, const fk_buf* rows, const fk_buf* targets4, uint32_t n_rows,
+                           const fk_buf* row_ids, uint32_t offset, uint32_t batch, const fk_adam* adam);
+/* Mean squared error over the last train step's batch (waits for it). */
+int fk_denoiser_last_loss(fk_denoiser* d, double* loss);
+/* The gradient of the batch's mean squared error with respect to the
+ * parameters (FK_DN_PARAMS floats to the host) without updating them. */
+int fk_denoiser_gradient(fk_denoiser* d, const fk_buf* rows, const fk_buf* targets4, uint32_t n_rows,
+                         const fk_buf* row_ids, uint32_t offset, uint32_t batch, float* grad, double* loss);
+/* Raw network outputs (float4 per row) for `count` input rows. */
+int fk_denoiser_forward(fk_denoiser* d, const fk_buf* rows, uint32_t count, fk_buf* y4);
+/* Denoised AO / bent normals of texels [offset, offset + count) of `map`:
+ * reads the feature image and the low-sample values ao_in / bn_in (which may
+ * be the output buffers themselves); texels without a mapping hit get AO 1 and
+ * BN (0,0,0). */
+int fk_denoise_apply(fk_denoiser* d, const fk_texel_map* map, const fk_buf* image, const fk_buf* tidx,
+                     const fk_buf* ao_in, const fk_buf* bn_in, uint32_t offset, uint32_t count, fk_buf* ao_out,
+                     fk_buf* bn_out);
+
+/* The denoised AO + bent-normal bake with the plain bake as its judge:
+ *   1. AO + BN at low_samples over every texel;
+ *   2. features, network;
+ *   3. per tile of tile x tile texels, verify_cells^2 spot checks (the first
+ *      texel with a mapping hit of each cell) traced at full_samples exactly
+ *      as the plain bake traces them;
+ *   4. tiles whose error (the larger of the AO mean absolute error and the
+ *      bent normals' per-component one over the spot checks) exceeds
+ *      max_tile_error are re-baked at full_samples (the plain path's values).
+ * Samples tables: low_samples x perm_count and full_samples x perm_count. */
+typedef struct {
+  uint32_t low_samples, full_samples, perm_count;
+  float min_distance, max_distance;
+  uint32_t tile, verify_cells;
+  float max_tile_error;
+  int traverse;
+} fk_denoise_params;
+typedef struct {
+  uint32_t tiles;           /* tiles with at least one spot check */
+  uint32_t tiles_failed;    /* re-baked at full_samples */
+  uint32_t spot_checks;     /* texels traced at full_samples to verify */
+  uint32_t texels_rebaked;  /* texels of failed tiles */
+  uint64_t rays;            /* all rays traced */
+  float worst_tile_error;
+} fk_denoise_stats;
+int fk_denoise_bake(fk_denoiser* d, const fk_scene* scene, const fk_texel_map* map, const fk_buf* coords,
+                    const fk_buf* tidx, const fk_denoise_params* params, const fk_buf* samples_low,
+                    const fk_buf* samples_full, fk_buf* ao_out, fk_buf* bn_out, fk_denoise_stats* stats);
 
 #ifdef __cplusplus
 }
