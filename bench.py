@@ -340,7 +340,115 @@ def run_fornos(args, wl, rank, world):
                      "flop_model": "24 per ray-box test + 104 per ray-triangle test, tests counted on the GPU"},
         "clocks": clk.summary(),
     }
-    return result, (prep, tmap, B, n)
+    return result, (prep, tmap, B, n, ctx, stream, scene)
+
+
+# ---------------------------------------------------------------- denoised vs plain AO + BN
+def run_denoise_bench(args):
+    """The denoised-vs-plain comparison alone, on the plane workload's scene."""
+    import torch
+
+    from fornos_b200 import api
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    ctx = api.Context(0)
+    ctx.set_stream(stream.cuda_stream)
+    prep = Prepared(WORKLOADS["plane2048"], args.seed)
+    scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
+    r = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed)
+    if "unavailable" in r:
+        return dict(r, metric="AO + bent-normal texels/s, 16 spp + denoiser vs 1024 spp")
+    return {"metric": "AO + bent-normal texels/s at 4096x4096: 16 spp + denoiser (verified) vs plain 1024 spp",
+            "value": r["denoised"]["texels_per_s"], "unit": "texels/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32 traversal, bf16 network", "data": "synthetic (seeded generated meshes)",
+            "config": {"workload": "denoise4096", "scene": WORKLOADS["plane2048"]["desc"], "seed": args.seed},
+            "denoise": r}
+
+
+
+DENOISE = dict(tex=4096, low=16, full=1024, label=4096, min_d=0.001, max_d=0.3, tile=64, cells=4, max_err=0.02,
+               mae_texels=65536)
+
+
+def denoise_compare(ctx, stream, prep, scene, weights, seed):
+    """AO + bent normals of the plane workload's scene at 4096 x 4096 texels:
+    the plain 1024-sample bake against the verified 16-sample + network bake
+    (spot checks and per-tile fallback included), each timed with CUDA events
+    over one whole pass, and each scored by mean absolute error against
+    4096-sample values on 65,536 random texels with a mapping hit."""
+    import torch
+
+    from fornos_b200 import api
+    if not os.path.exists(weights):
+        return {"unavailable": "no trained denoiser weights at %s" % os.path.relpath(weights, ROOT)}
+    d = DENOISE
+    tex = d["tex"]
+    tm = api.TexelMap.from_meshes(ctx, prep.lm, prep.dm, tex, tex)
+    n = tm.count
+    coords, tidx = ctx.buffer(16 * n), ctx.buffer(4 * n)
+    api.meshmap(ctx, scene, tm, True, coords, tidx)
+    hit = np.nonzero(tidx.download(np.uint32, n) != api.MISS)[0]
+    low = ctx.upload(api.samples_cosine(d["low"], api.PERMS, seed + 11))
+    full = ctx.upload(api.samples_cosine(d["full"], api.PERMS, seed + 12))
+    label = ctx.upload(api.samples_cosine(d["label"], api.PERMS, seed + 13))
+    dn = api.Denoiser(ctx, np.load(weights)["params"])
+    args = (d["min_d"], d["max_d"])
+
+    def timed(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(0) as clk, torch.cuda.stream(stream):
+            stream.synchronize()
+            a.record(stream)
+            out = fn()
+            b.record(stream)
+            stream.synchronize()
+        return a.elapsed_time(b), out, clk.summary()
+
+    pao, pbn = ctx.buffer(4 * n), ctx.buffer(12 * n)
+    plain = lambda off, cnt: api.hemisphere(ctx, scene, coords, tidx, api.AO_BN, d["full"], *args, full, pao, pbn,
+                                            None, None, off, cnt)
+    plain(0, max(1, n // 100))  # warm-up on 1 % of the texels
+    t_plain, _, clk_plain = timed(lambda: plain(0, n))
+    dao, dbn = ctx.buffer(4 * n), ctx.buffer(12 * n)
+    bake = lambda: dn.bake(scene, tm, coords, tidx, low, full, dao, dbn, low_samples=d["low"],
+                           full_samples=d["full"], min_distance=d["min_d"], max_distance=d["max_d"], tile=d["tile"],
+                           verify_cells=d["cells"], max_tile_error=d["max_err"])
+    bake()  # warm-up
+    runs = [timed(bake) for _ in range(3)]
+    t_dn, stats, clk_dn = sorted(runs, key=lambda r: r[0])[1]
+    ctx.check()
+    # accuracy against 4096-sample values on random texels with a mapping hit
+    ids = np.sort(np.random.default_rng(seed).choice(hit, min(d["mae_texels"], len(hit)), replace=False))
+    ids = ids.astype(np.uint32)
+    lao, lbn = ctx.buffer(4 * n), ctx.buffer(12 * n)
+    api.hemisphere_texels(ctx, scene, coords, tidx, n, api.AO_BN, d["label"], *args, label, ctx.upload(ids), lao,
+                          lbn)
+    pick = lambda b, w: (b.download(np.float32, n) if w == 1 else b.download(np.float32, (n, 3)))[ids]
+    clean = lambda v: np.where(np.isfinite(v).all(1, keepdims=True), v, 0)
+    la, lb = pick(lao, 1), clean(pick(lbn, 3))
+
+    def score(ao_b, bn_b):
+        return {"mae_ao": round(float(np.abs(pick(ao_b, 1) - la).mean()), 5),
+                "mae_bn": round(float(np.abs(clean(pick(bn_b, 3)) - lb).mean()), 5)}
+
+    covered = len(hit)
+    res = {
+        "texture": tex, "texels_with_hit": covered, "train_meta": json.loads(str(np.load(weights)["meta"])).get(
+            "eval_mae"),
+        "plain": dict(samples=d["full"], ms=round(t_plain, 2), texels_per_s=round(covered / (t_plain * 1e-3), 1),
+                      clocks=clk_plain, **score(pao, pbn)),
+        "denoised": dict(samples=d["low"], ms=round(t_dn, 2), texels_per_s=round(covered / (t_dn * 1e-3), 1),
+                         clocks=clk_dn, stats=stats, **score(dao, dbn)),
+        "mae_reference": "%d-sample AO + bent normals on %d random texels with a mapping hit" % (
+            d["label"], len(ids)),
+        "fallback_rule": "tile %d x %d, %d spot checks at %d samples, re-bake if error > %.2f" % (
+            d["tile"], d["tile"], d["cells"] ** 2, d["full"], d["max_err"]),
+    }
+    res["speedup"] = round(t_plain / t_dn, 2)
+    for b in (tm, coords, tidx, low, full, label, pao, pbn, dao, dbn, lao, lbn):
+        b.free()
+    dn.free()
+    return res
 
 
 # ---------------------------------------------------------------- CPU arm
@@ -548,16 +656,21 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="fornos", choices=["fornos", "reference"])
-    ap.add_argument("--workload", default="plane2048", choices=list(WORKLOADS) + ["batch"])
+    ap.add_argument("--workload", default="plane2048", choices=list(WORKLOADS) + ["batch", "denoise"])
     ap.add_argument("--batch-jobs", type=int, default=64)
     ap.add_argument("--traverse", default="auto", choices=list(TRAVERSE))
     ap.add_argument("--schedule", default="auto", choices=list(SCHEDULE))
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-denoise", action="store_true", help="skip the denoised-vs-plain comparison")
+    ap.add_argument("--denoiser", default=os.path.join(ROOT, "fornos_b200", "data", "denoiser_plane2048.npz"))
     args = ap.parse_args()
     if args.workload == "batch":
         print(json.dumps(run_batch_bench(args)))
+        return 0
+    if args.workload == "denoise":
+        print(json.dumps(run_denoise_bench(args)))
         return 0
     wl = WORKLOADS[args.workload]
     rank = int(os.environ.get("RANK", 0))
@@ -577,12 +690,15 @@ def main():
                                              device_id=torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0))))
     result, state = run_fornos(args, wl, rank, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        prep, tmap, _, _ = state
+        prep, tmap = state[0], state[1]
         cpu = CpuBaseline(wl, args.seed, prep, tmap.download())
         cpu.calibrate(args.cpu_seconds)
         mr, rays, dt, m = cpu.run()
         result["cpu_baseline"] = {"value": round(mr, 4), "unit": "Mrays/s", "cores": cpu.cores, "kind": cpu.kind,
                                   "sample": cpu.describe(rays, m)}
+    if rank == 0 and world == 1 and args.workload == "plane2048" and not args.no_denoise:
+        prep, _, _, _, ctx, stream, scene = state
+        result["denoise"] = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed)
     if rank == 0:
         print(json.dumps(result))
     if world > 1:

@@ -3,8 +3,8 @@
 // the tensor cores (mma.sync m16n8k16, FP32 accumulation), over a 5 x 5 texel
 // neighbourhood of 10 features per texel:
 //   AO (1), bent normal as 2-D octahedral (2), position relative to the centre
-//   texel / max distance (3), interpolated normal as octahedral (2), mapping hit
-//   distance / max distance (1), coverage (1).
+//   texel in units of the centre's texel spacing (3), interpolated normal as
+//   octahedral (2), mapping hit distance / max distance (1), coverage (1).
 // Neighbours outside the texture or without a mapping hit contribute zeros.
 // The input width is padded from 250 to 256 with zero columns.
 //
@@ -97,12 +97,15 @@ __device__ __forceinline__ void assemble_row(const float4* __restrict__ f0, cons
         const float4 a = __ldg(f0 + q);
         if (a.w > 0.0f) {
           const float4 c = __ldg(f1 + p), b = __ldg(f1 + q), n = __ldg(f2 + q);
+          const float sp = __ldg(f2 + p).z;  // centre texel spacing
           v[0] = a.x;
           v[1] = a.y;
           v[2] = a.z;
-          v[3] = clamp4(b.x - c.x);
-          v[4] = clamp4(b.y - c.y);
-          v[5] = clamp4(b.z - c.z);
+          if (sp > 0.0f) {
+            v[3] = clamp4((b.x - c.x) / sp);
+            v[4] = clamp4((b.y - c.y) / sp);
+            v[5] = clamp4((b.z - c.z) / sp);
+          }
           v[6] = n.x;
           v[7] = n.y;
           v[8] = b.w;
@@ -232,6 +235,32 @@ __global__ void dn_features_kernel(uint32_t n, uint32_t w, uint32_t h, const uin
   f1[p] = make_float4(__ldg(pos3 + 3 * (size_t)i) / max_d, __ldg(pos3 + 3 * (size_t)i + 1) / max_d,
                       __ldg(pos3 + 3 * (size_t)i + 2) / max_d, __ldg(coords + i).x / max_d);
   f2[p] = make_float4(on.x, on.y, 0.0f, 0.0f);
+}
+
+// Texel spacing of each covered pixel: the mean distance (in position / max
+// distance units) to its covered 4-neighbours, right, left, down, up; 0 when
+// none is covered.  Stored in plane 2's z.
+__global__ void dn_spacing_kernel(uint32_t n, uint32_t w, uint32_t h, const uint32_t* __restrict__ indices,
+                                  const float4* __restrict__ f0, const float4* __restrict__ f1, float4* f2) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t p = __ldg(indices + i);
+  if (p >= w * h || !(__ldg(f0 + p).w > 0.0f)) return;
+  const int x = (int)(p % w), y = (int)(p / w);
+  const int nx[4] = {x + 1, x - 1, x, x}, ny[4] = {y, y, y + 1, y - 1};
+  const float4 c = __ldg(f1 + p);
+  float sum = 0.0f;
+  int k = 0;
+  for (int j = 0; j < 4; ++j) {
+    if (nx[j] < 0 || ny[j] < 0 || nx[j] >= (int)w || ny[j] >= (int)h) continue;
+    const uint32_t q = (uint32_t)ny[j] * w + (uint32_t)nx[j];
+    if (!(__ldg(f0 + q).w > 0.0f)) continue;
+    const float4 b = __ldg(f1 + q);
+    const float dx = b.x - c.x, dy = b.y - c.y, dz = b.z - c.z;
+    sum += sqrtf((dx * dx + dy * dy) + dz * dz);
+    ++k;
+  }
+  f2[p].z = k ? sum / (float)k : 0.0f;
 }
 
 // Input rows for a list of pixels (kNoTexel or out-of-image: an all-zero row).
@@ -742,6 +771,8 @@ cudaError_t launch_features(cudaStream_t st, uint32_t n, uint32_t w, uint32_t h,
   if (e != cudaSuccess || n == 0) return e;
   dn_features_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, w, h, indices, tidx, coords, ao, bn3, pos3, nrm3, max_d,
                                                        image, image + px, image + 2 * px);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  dn_spacing_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, w, h, indices, image, image + px, image + 2 * px);
   return cudaGetLastError();
 }
 

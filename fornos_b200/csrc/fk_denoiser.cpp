@@ -208,7 +208,7 @@ int fk_denoise_features(fk_ctx* ctx, const fk_texel_map* map, const fk_buf* coor
                                       (const uint32_t*)tidx->ptr, (const float4*)coords->ptr, (const float*)ao->ptr,
                                       (const float*)bn3->ptr, (const float*)pos3->ptr, (const float*)nrm3->ptr,
                                       max_distance, (float4*)image->ptr),
-                  "dn_features_kernel");
+                  "dn_features_kernel", 2);
 }
 
 int fk_denoise_rows(fk_ctx* ctx, const fk_buf* image, uint32_t width, uint32_t height, const fk_buf* pixels,
@@ -345,7 +345,7 @@ int fk_denoise_bake(fk_denoiser* d, const fk_scene* scene, const fk_texel_map* m
   rc = launched(ctx,
                 dn::launch_features(ctx->stream, n, w, h, map->indices, ti, c4, ao, bn, pos3, nrm3,
                                     prm->max_distance, image),
-                "dn_features_kernel");
+                "dn_features_kernel", 2);
   if (rc == FK_OK)
     rc = launched(ctx,
                   dn::launch_apply(ctx->stream, ctx->sm_count, image, w, h, map->indices, ti, ao, bn, 0, n,

@@ -440,9 +440,9 @@ int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* scene, const fk_buf* c
  * No counterpart in the reference.  A per-texel MLP that turns a low-sample
  * AO + bent-normal bake into an estimate of the full-sample one, from a 5 x 5
  * texel neighbourhood of 10 features per texel: AO, bent normal (2-D
- * octahedral), position relative to the centre texel / max distance (3),
- * interpolated normal (octahedral, 2), mapping hit distance / max distance and
- * coverage (mapping hit).  Network 250 -> 64 -> 64 -> 4 with tanh-form GELU,
+ * octahedral), position relative to the centre texel in units of the centre's
+ * texel spacing (3, clamped to +-4), interpolated normal (octahedral, 2),
+ * mapping hit distance / max distance and coverage (mapping hit).  Network 250 -> 64 -> 64 -> 4 with tanh-form GELU,
  * BF16 weights and activations, FP32 accumulation; outputs are residuals: AO =
  * clamp(AO_low + y0, 0, 1), BN = normalize(BN_low + y1..3).
  *
@@ -471,7 +471,10 @@ int fk_denoiser_get_params(fk_denoiser* d, float* params, uint32_t count);
 /* Dense feature image (48 x W x H bytes) of a texel map's texels from a
  * low-sample AO (float) + bent normal (3 floats) bake, world positions and
  * normals (fk_gather POSITION / NORMAL) and the mapping (coords / tidx);
- * pixels without a mapping hit stay zero. */
+ * pixels without a mapping hit stay zero.  Planes: (AO, octahedral BN, 1),
+ * (position / max distance, mapping distance / max distance), (octahedral
+ * normal, texel spacing, 0); the spacing is the mean distance to the covered
+ * 4-neighbours. */
 int fk_denoise_features(fk_ctx* ctx, const fk_texel_map* map, const fk_buf* coords, const fk_buf* tidx,
                         const fk_buf* ao, const fk_buf* bn3, const fk_buf* pos3, const fk_buf* nrm3,
                         float max_distance, fk_buf* image);

@@ -6,10 +6,11 @@ CUDA kernels (fornos_b200/csrc/fk_denoise.cu):
 
 * features: dense W x H image of 3 float4 planes per pixel,
   (AO, octahedral BN.xy, coverage), (position / R, mapping distance / R),
-  (octahedral normal.xy, 0, 0); float32 arithmetic in the kernel's order, so
-  the image is bit-exact;
-* rows: 25 neighbours x 10 features, bf16-rounded (round to nearest even),
-  padded to 256 columns; bit-exact;
+  (octahedral normal.xy, texel spacing, 0); float32 arithmetic in the
+  kernel's order, so the image is bit-exact;
+* rows: 25 neighbours x 10 features (positions relative to the centre in
+  units of its texel spacing, clamped to +-4), bf16-rounded (round to nearest
+  even), padded to 256 columns; bit-exact;
 * forward / backward of the MLP 250 -> 64 -> 64 -> 4 with tanh-form GELU.  With
   `bf16=True` the activations, the output gradient and the pre-activation
   gradients are rounded to bf16 at the points where the kernels feed them to
@@ -100,6 +101,21 @@ def features(w, h, indices, tidx, coords, ao, bn3, pos3, nrm3, max_d):
     f[1, p] = np.stack([pos[:, 0] / r, pos[:, 1] / r, pos[:, 2] / r,
                         np.asarray(coords, np.float32).reshape(-1, 4)[keep, 0] / r], 1)
     f[2, p] = np.stack([onx, ony, np.zeros_like(onx), np.zeros_like(onx)], 1)
+    # texel spacing: mean distance to the covered 4-neighbours (right, left, down, up)
+    x, y = (p % w).astype(np.int64), (p // w).astype(np.int64)
+    total = np.zeros(len(p), np.float32)
+    k = np.zeros(len(p), np.int64)
+    for dx, dy in ((1, 0), (-1, 0), (0, 1), (0, -1)):
+        nx, ny = x + dx, y + dy
+        ok = (nx >= 0) & (ny >= 0) & (nx < w) & (ny < h)
+        q = np.where(ok, ny * w + nx, 0)
+        ok &= f[0, q, 3] > 0
+        d = f[1, q, :3] - f[1, p, :3]
+        dist = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+        total = np.where(ok, total + dist, total).astype(np.float32)
+        k += ok
+    with np.errstate(all="ignore"):
+        f[2, p, 2] = np.where(k > 0, total / k.astype(np.float32), 0)
     return f
 
 
@@ -117,10 +133,11 @@ def rows(f, w, h, pixels):
         q = np.where(ok, y * w + x, 0)
         a = f[0, q]
         ok &= a[:, 3] > 0
-        b, n, c = f[1, q], f[2, q], f[1, np.where(valid, pixels, 0)]
-        v = np.stack([a[:, 0], a[:, 1], a[:, 2],
-                      np.clip(b[:, 0] - c[:, 0], f32(-4), f32(4)), np.clip(b[:, 1] - c[:, 1], f32(-4), f32(4)),
-                      np.clip(b[:, 2] - c[:, 2], f32(-4), f32(4)), n[:, 0], n[:, 1], b[:, 3],
+        pc = np.where(valid, pixels, 0)
+        b, n, c, sp = f[1, q], f[2, q], f[1, pc], f[2, pc, 2]
+        with np.errstate(all="ignore"):
+            rel = [np.where(sp > 0, np.clip((b[:, k] - c[:, k]) / sp, f32(-4), f32(4)), 0) for k in range(3)]
+        v = np.stack([a[:, 0], a[:, 1], a[:, 2], rel[0], rel[1], rel[2], n[:, 0], n[:, 1], b[:, 3],
                       np.ones(m, np.float32)], 1)
         out[:, j] = np.where(ok[:, None], v, 0)
     x = np.zeros((m, K1), np.float32)

@@ -78,7 +78,9 @@ def test_rows_neighbourhood_and_padding():
         dx, dy = j % 5 - 2, j // 5 - 2
         exp = (dy, dx) in inside
         assert (r[0, j, 9] == 1) == exp
-    # centre (2, 2) of pixel 14: relative position of neighbour (+1, +2) is (1, 2) / 0.5, clamped to 4
+    # centre (2, 2) of pixel 14: texel spacing 1 / 0.5 = 2 in position / R units, so neighbour (+1, +2) sits
+    # at (1, 2) spacings
+    assert f[2, 14, 2] == 2.0 and f[2, 8, 2] == 2.0  # pixel 8 = (2, 1) averages 3 covered neighbours
     j = (2 + 2) * 5 + (1 + 2)
-    assert np.allclose(r[1, j, 3:6], [2.0, 4.0, 0.0])
+    assert np.allclose(r[1, j, 3:6], [1.0, 2.0, 0.0])
     assert r[1, 12, 8] == D.bf16(np.float32(0.25) / np.float32(0.5))
