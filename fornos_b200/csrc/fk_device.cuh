@@ -76,11 +76,17 @@ __device__ __forceinline__ RayPre ray_pre(f3 o, f3 d) {
   return r;
 }
 
-__device__ __forceinline__ float slack(float v) {
-  // bound on |exact - filtered| for a filtered slab value v (0 when v is inf / NaN,
-  // where both forms agree exactly)
-  float s = __fadd_rn(__fmul_rn(fabsf(v), 4.76837158e-07f), 2.3509887e-38f);  // 2^-21 |v| + 2^-125
-  return isfinite(v) ? s : 0.0f;
+// Margins around a filtered slab value v: below(v) <= v - 2^-22 |v| - 2^-125
+// and above(v) >= v + 2^-22 |v| + 2^-125, each in two roundings (one fused
+// multiply-add with 2^-21, whose rounding costs at most 2^-24 |v|, then the
+// absolute term, which survives the rounding exactly where it matters: for
+// subnormal v).  For an infinite or NaN v both are NaN, so every comparison
+// with them fails and the exact quotients decide.
+__device__ __forceinline__ float below(float v) {
+  return __fsub_rn(__fmaf_rn(fabsf(v), -4.76837158e-07f, v), 2.3509887e-38f);
+}
+__device__ __forceinline__ float above(float v) {
+  return __fadd_rn(__fmaf_rn(fabsf(v), 4.76837158e-07f, v), 2.3509887e-38f);
 }
 
 // Returns ray_box(o, d, lo, hi) < thr exactly, and in `entry` the filtered
@@ -94,13 +100,12 @@ __device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr
     float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
     float b = fminf(tx.x, fminf(tx.y, tx.z));
     entry = a;
-    float sa = slack(a), sb = slack(b);
+    const float a_lo = below(a), b_hi = above(b);
     // certain rejections
-    if (__fadd_rn(b, sb) < 0.0f) return false;
-    if (__fsub_rn(a, sa) > __fadd_rn(b, sb)) return false;
-    if (__fsub_rn(a, sa) >= thr) return false;
-    // certain acceptance (NaN a or b never qualifies)
-    if (__fsub_rn(b, sb) >= 0.0f && __fadd_rn(a, sa) <= __fsub_rn(b, sb) && __fadd_rn(a, sa) < thr) return true;
+    if (b_hi < 0.0f || a_lo > b_hi || a_lo >= thr) return false;
+    // certain acceptance (never from a NaN margin)
+    const float a_hi = above(a), b_lo = below(b);
+    if (b_lo >= 0.0f && a_hi <= b_lo && a_hi < thr) return true;
   }
   f3 t1 = divv(n1, r.d), t2 = divv(n2, r.d);
   f3 tn = vmin(t1, t2), tx = vmax(t1, t2);

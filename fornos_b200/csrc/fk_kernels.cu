@@ -469,7 +469,7 @@ __device__ __forceinline__ bool child_hit(const RayPre& r, f3 lo, f3 hi, float t
 // filtered ones only cull when certainly at or beyond the threshold.
 template <bool FILTER>
 __device__ __forceinline__ bool still_open(float entry, float thr) {
-  if (FILTER) return __fsub_rn(entry, slack(entry)) < thr;
+  if (FILTER) return below(entry) < thr;
   return entry < thr;
 }
 
@@ -487,49 +487,54 @@ struct OState {
   int sp;
 };
 
-template <bool FILTER>
-__device__ __forceinline__ bool push(int32_t* sn, float* sd, int& sp, int32_t ref, float dist, int* status) {
+// Deferred entries are (ref, entry distance bits) pairs: one 8-byte access
+// per push or pop.
+__device__ __forceinline__ bool push(int2* stk, int& sp, int32_t ref, float dist, int* status) {
   if (sp >= kStack) {
     atomicOr(status, 1);
     return false;
   }
-  sn[sp] = ref;
-  sd[sp] = dist;
+  stk[sp] = make_int2(ref, __float_as_int(dist));
   ++sp;
   return true;
 }
 
-// Inner phase: tests both children of record `cur` against `thr`.
+// A child that passed its box test: the first leaf becomes the postponed
+// leaf, the first inner record the next one to visit, the rest are deferred.
+__device__ __forceinline__ bool place(OState& st, int32_t& next, int2* stk, int32_t ref, float dist, int* status) {
+  if (ref < 0) {
+    if (st.pend < 0) {
+      st.pend = -ref - 1;
+      st.pend_dist = dist;
+      return true;
+    }
+    return push(stk, st.sp, ref, dist, status);
+  }
+  if (next < 0) {
+    next = ref;
+    return true;
+  }
+  return push(stk, st.sp, ref, dist, status);
+}
+
+// Inner phase: tests both children of record `cur` against `thr` and takes
+// them nearer entry first (straight-line selects: no per-lane arrays).
 template <bool COUNT, bool FILTER>
-__device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, float thr, OState& st, int32_t* sn,
-                                            float* sd, int* status, Tally& tally) {
+__device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
+                                            int* status, Tally& tally) {
   const float4* w = s.wide + 4 * (size_t)st.cur;
   float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
-  float dist[2];
-  bool hit[2];
-  hit[0] = child_hit<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, dist[0]);
-  hit[1] = child_hit<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, dist[1]);
+  float d0, d1;
+  const bool h0 = child_hit<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
+  const bool h1 = child_hit<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
   if (COUNT) tally.box += 2;
-  int32_t ref[2] = {__float_as_int(w3.x), __float_as_int(w3.y)};
-  int first = dist[1] < dist[0] ? 1 : 0;
+  const bool swap = d1 < d0;
+  const bool hn = swap ? h1 : h0, hf = swap ? h0 : h1;
+  const float dn = swap ? d1 : d0, df = swap ? d0 : d1;
+  const int32_t rn = __float_as_int(swap ? w3.y : w3.x), rf = __float_as_int(swap ? w3.x : w3.y);
   int32_t next = -1;
-#pragma unroll
-  for (int q = 0; q < 2; ++q) {
-    int c = q == 0 ? first : 1 - first;
-    if (!hit[c]) continue;
-    if (ref[c] < 0) {
-      if (st.pend < 0) {
-        st.pend = -ref[c] - 1;
-        st.pend_dist = dist[c];
-      } else if (!push<FILTER>(sn, sd, st.sp, ref[c], dist[c], status)) {
-        return false;
-      }
-    } else if (next < 0) {
-      next = ref[c];
-    } else if (!push<FILTER>(sn, sd, st.sp, ref[c], dist[c], status)) {
-      return false;
-    }
-  }
+  if (hn && !place(st, next, stk, rn, dn, status)) return false;
+  if (hf && !place(st, next, stk, rf, df, status)) return false;
   st.cur = next;
   return true;
 }
@@ -548,15 +553,16 @@ __device__ __forceinline__ void leaf_visit(const SceneDev& s, const RayPre& rp, 
 
 // Takes the nearest still-open deferred entry; false when none is left.
 template <bool FILTER>
-__device__ __forceinline__ bool pop(OState& st, const int32_t* sn, const float* sd, float thr) {
+__device__ __forceinline__ bool pop(OState& st, const int2* stk, float thr) {
   while (st.sp > 0) {
-    --st.sp;
-    if (!still_open<FILTER>(sd[st.sp], thr)) continue;
-    if (sn[st.sp] < 0) {
-      st.pend = -sn[st.sp] - 1;
-      st.pend_dist = sd[st.sp];
+    const int2 e = stk[--st.sp];
+    const float dist = __int_as_float(e.y);
+    if (!still_open<FILTER>(dist, thr)) continue;
+    if (e.x < 0) {
+      st.pend = -e.x - 1;
+      st.pend_dist = dist;
     } else {
-      st.cur = sn[st.sp];
+      st.cur = e.x;
     }
     return true;
   }
@@ -591,8 +597,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
-  int32_t stack_node[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
-  float stack_dist[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
+  int2 stk[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];  // deferred (ref, entry) pairs
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t r = 0;
@@ -664,10 +669,10 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
             fin = settled<STOP>(best, p.hi);
           }
         } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
-          if (!inner_visit<COUNT, FILTER>(p.s, rp, fminf(best, p.hi), st, stack_node, stack_dist, p.status, tally))
+          if (!inner_visit<COUNT, FILTER>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally))
             fin = true;
         }
-        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stack_node, stack_dist, fminf(best, p.hi));
+        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, p.hi));
         if (fin) {
           p.scratch[r] = best;
           active = false;
@@ -844,8 +849,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
   const unsigned lower = (1u << lane) - 1u;
   // a launch traces at most the scratch's 2^27 rays: lane indices fit 32 bits
   const uint32_t total = (uint32_t)((p.r1 - p.r0 + p.stride - 1) / p.stride);
-  int32_t stack_node[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
-  float stack_dist[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];
+  int2 stk[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];  // deferred (ref, entry) pairs
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t q = 0;
@@ -928,10 +932,10 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
             fin = settled<STOP>(best, hi);
           }
         } else if (st.cur >= 0 && st.pend < 0) {
-          if (!inner_visit<false, FILTER>(s, rp, fminf(best, hi), st, stack_node, stack_dist, p.status, tally))
+          if (!inner_visit<false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally))
             fin = true;
         }
-        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stack_node, stack_dist, fminf(best, hi));
+        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, hi));
         if (fin) {
           p.scratch[q] = best;
           active = false;
