@@ -58,7 +58,7 @@ WORKLOADS = {
         gen=lambda seed: W.plane_pair(seed=seed, lo_quads=64, hi_quads=1024, bumps=200),
         tex=250, spp=16, min_d=0.001, max_d=0.3, bakers=("ao", "bn", "thick")),
 }
-TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2}
+TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2, "ordered4": 3}
 SCHEDULE = {"auto": 0, "static": 0x10, "dynamic": 0x20}
 # DRAM bytes per hemisphere-kernel launch from ncu captures (profiles/), by workload.
 # plane250: measured for one AO+BN trace launch (984,064 rays); plane2048: the same 364.5 B per ray scaled to one

@@ -169,6 +169,8 @@ _SIGS = {
     "fk_diag_fp32_peak": (c_int, [c_vp, ctypes.POINTER(ctypes.c_double)]),
     "fk_diag_traversal_counts": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32,
                                          c_u32, c_int, ctypes.POINTER(c_u64)]),
+    "fk_diag_traversal_profile": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32,
+                                          c_u32, c_int, ctypes.POINTER(c_u64)]),
     "fk_denoiser_create": (c_int, [c_vp, ctypes.POINTER(c_vp)]),
     "fk_denoiser_free": (c_int, [c_vp]),
     "fk_denoiser_set_params": (c_int, [c_vp, f32p, c_u32]),

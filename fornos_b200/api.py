@@ -18,7 +18,7 @@ MISS = 0xFFFFFFFF
 
 # kinds (include/fornos_gpu.h)
 AO, BN, THICK, AO_BN = 0, 1, 2, 3
-TRAVERSE_AUTO, TRAVERSE_ORDERED, TRAVERSE_SKIP = 0, 1, 2
+TRAVERSE_AUTO, TRAVERSE_ORDERED, TRAVERSE_SKIP, TRAVERSE_ORDERED4 = 0, 1, 2, 3
 SCHEDULE_STATIC, SCHEDULE_DYNAMIC = 0x10, 0x20  # or-ed into `traverse`
 EXACT_BOX_TESTS = 0x100  # or-ed into `traverse`: divide in every box test
 GATHER_HEIGHT, GATHER_POSITION, GATHER_NORMAL = 0, 1, 2
@@ -557,6 +557,21 @@ def traversal_counts(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples,
     _check(ctx.lib.fk_diag_traversal_counts(ctx.handle, scene.handle, coords.handle, tidx.handle, kind, ctypes.byref(p),
                                             samples.handle, offset, count, traverse, out), ctx, "traversal counts")
     return int(out[0]), int(out[1])
+
+
+PROFILE_KEYS = ("box_tests", "tri_tests", "iterations", "leaf_iterations", "inner_lanes", "leaf_lanes",
+                "ray_lanes", "refills")
+
+
+def traversal_profile(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, offset=0, count=0, perms=PERMS,
+                      traverse=TRAVERSE_AUTO):
+    """Lane-utilisation profile of the dynamic schedule (fk_diag_traversal_profile)."""
+    p = L.SampleParams(spp, perms, min_d, max_d)
+    out = (L.c_u64 * 8)()
+    _check(ctx.lib.fk_diag_traversal_profile(ctx.handle, scene.handle, coords.handle, tidx.handle, kind,
+                                             ctypes.byref(p), samples.handle, offset, count, traverse, out), ctx,
+           "traversal profile")
+    return dict(zip(PROFILE_KEYS, (int(v) for v in out)))
 
 
 def _sampler(cfg):

@@ -38,7 +38,7 @@ int fk_hemisphere(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk
   if (kind < FK_AO || kind > FK_AO_BN) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown kind");
   if (prm->sample_count == 0 || prm->perm_count == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: zero samples");
   if ((traverse & ~(FK_TRAVERSE_MASK | FK_SCHEDULE_MASK | FK_EXACT_BOX_TESTS)) ||
-      (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_SKIP ||
+      (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_ORDERED4 ||
       (traverse & FK_SCHEDULE_MASK) > FK_SCHEDULE_DYNAMIC)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere: unknown traversal or schedule");
   uint64_t end = (uint64_t)offset + count;
@@ -80,7 +80,7 @@ int fk_hemisphere_texels(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, c
   if (prm->sample_count == 0 || prm->perm_count == 0)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: zero samples");
   if ((traverse & ~(FK_TRAVERSE_MASK | FK_SCHEDULE_MASK | FK_EXACT_BOX_TESTS)) ||
-      (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_SKIP || (traverse & FK_SCHEDULE_MASK) > FK_SCHEDULE_DYNAMIC)
+      (traverse & FK_TRAVERSE_MASK) > FK_TRAVERSE_ORDERED4 || (traverse & FK_SCHEDULE_MASK) > FK_SCHEDULE_DYNAMIC)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_hemisphere_texels: unknown traversal or schedule");
   if ((traverse & FK_SCHEDULE_MASK) == FK_SCHEDULE_STATIC)
     return fk_fail(ctx, FK_ERR_UNSUPPORTED, "fk_hemisphere_texels: texel lists run on the dynamic schedule only");
@@ -116,9 +116,12 @@ int fk_hemisphere_texels(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, c
   return fk::launch_hemisphere(ctx, s, h);
 }
 
-int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk_buf* tidx, int kind,
-                             const fk_sample_params* prm, const fk_buf* samples, uint32_t offset, uint32_t count,
-                             int traverse, uint64_t* tests) {
+// Runs the counting variant and returns its first `n` counters (at most 8):
+// box tests, triangle tests, then for the dynamic schedule the per-warp
+// iteration profile (see fk_diag_traversal_profile).
+static int diag_counts(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk_buf* tidx, int kind,
+                       const fk_sample_params* prm, const fk_buf* samples, uint32_t offset, uint32_t count,
+                       int traverse, uint64_t* tests, int n) {
   if (!ctx || !s || !coords || !tidx || !prm || !samples || !tests)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_diag_traversal_counts: null argument");
   if (kind < FK_AO || kind > FK_AO_BN || prm->sample_count == 0 || prm->perm_count == 0)
@@ -130,8 +133,8 @@ int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* s, const fk_buf* coord
   unsigned long long* tally = nullptr;
   int rc = fk_buf_alloc(ctx, 12 * (end ? end : 1), &o0);
   if (rc == FK_OK) rc = fk_buf_alloc(ctx, 12 * (end ? end : 1), &o1);
-  if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&tally, 2 * sizeof(unsigned long long));
-  if (rc == FK_OK && cudaMemsetAsync(tally, 0, 2 * sizeof(unsigned long long), ctx->stream) != cudaSuccess)
+  if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&tally, 8 * sizeof(unsigned long long));
+  if (rc == FK_OK && cudaMemsetAsync(tally, 0, 8 * sizeof(unsigned long long), ctx->stream) != cudaSuccess)
     rc = fk_fail(ctx, FK_ERR_CUDA, "fk_diag_traversal_counts: memset");
   if (rc == FK_OK && count) {
     fk::HemiLaunch h;
@@ -152,17 +155,30 @@ int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* s, const fk_buf* coord
     h.tally = tally;
     rc = fk::launch_hemisphere(ctx, s, h);
   }
-  unsigned long long host[2] = {0, 0};
+  unsigned long long host[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   if (rc == FK_OK && cudaMemcpyAsync(host, tally, sizeof(host), cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
     rc = fk_fail(ctx, FK_ERR_CUDA, "fk_diag_traversal_counts: copy");
   if (rc == FK_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
     rc = fk_fail(ctx, FK_ERR_CUDA, "fk_diag_traversal_counts: sync");
-  tests[0] = host[0];
-  tests[1] = host[1];
+  for (int k = 0; k < n; ++k) tests[k] = host[k];
   if (o0) fk_buf_free(ctx, o0);
   if (o1) fk_buf_free(ctx, o1);
   fk_dev_free(tally);
   return rc;
+}
+
+int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk_buf* tidx, int kind,
+                             const fk_sample_params* prm, const fk_buf* samples, uint32_t offset, uint32_t count,
+                             int traverse, uint64_t* tests) {
+  return diag_counts(ctx, s, coords, tidx, kind, prm, samples, offset, count, traverse, tests, 2);
+}
+
+int fk_diag_traversal_profile(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk_buf* tidx, int kind,
+                              const fk_sample_params* prm, const fk_buf* samples, uint32_t offset, uint32_t count,
+                              int traverse, uint64_t* counters) {
+  if ((traverse & FK_SCHEDULE_MASK) == FK_SCHEDULE_STATIC)
+    return fk_fail(ctx, FK_ERR_UNSUPPORTED, "fk_diag_traversal_profile: dynamic schedule only");
+  return diag_counts(ctx, s, coords, tidx, kind, prm, samples, offset, count, traverse, counters, 8);
 }
 
 int fk_gather(fk_ctx* ctx, const fk_scene* s, int kind, const fk_buf* coords, const fk_buf* tidx, uint32_t offset,

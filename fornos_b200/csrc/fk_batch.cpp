@@ -38,6 +38,8 @@ struct fk_batch {
   unsigned long long scratch_rays = 0;
   std::vector<Chunk> chunks;
   int traverse = FK_TRAVERSE_ORDERED;     // tuned choice
+  bool ordered_ok = true;                 // every tree fits the 2-wide ordered traversal's stack
+  bool ordered4_ok = true;                // every collapsed tree fits the 4-wide traversal's stack
   bool filter = true;
   fk_tuning tuning = {8, 8, 0, 0};
   cudaGraph_t graph = nullptr;
@@ -204,8 +206,11 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
     return rc;
   }
   // default schedule: ordered when every scene's tree is shallow enough
-  for (uint32_t i = 0; i < njobs; ++i)
-    if (jobs[i].scene->depth > 48) b->traverse = FK_TRAVERSE_SKIP;
+  for (uint32_t i = 0; i < njobs; ++i) {
+    if (jobs[i].scene->depth > 48) b->ordered_ok = false;
+    if (jobs[i].scene->depth4 > fk::kMaxOrdered4Depth) b->ordered4_ok = false;
+  }
+  b->traverse = b->ordered_ok ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
   b->tuning = ctx->tuning;
   *out = b;
   return FK_OK;
@@ -231,10 +236,12 @@ int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int
     fk_tuning t;
   };
   std::vector<Cand> cands;
-  bool ordered_ok = b->traverse == FK_TRAVERSE_ORDERED;
+  const bool ordered_ok = b->ordered_ok;
   for (uint32_t refill : {4u, 8u, 16u}) {
     if (ordered_ok)
       for (uint32_t lb : {1u, 4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED, true, {refill, lb, 0, 0}});
+    if (b->ordered4_ok)
+      for (uint32_t lb : {4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED4, true, {refill, lb, 0, 0}});
     cands.push_back({FK_TRAVERSE_SKIP, true, {refill, 8, 0, 0}});
   }
   if (ordered_ok) cands.push_back({FK_TRAVERSE_ORDERED, false, {8, 8, 0, 0}});
@@ -269,6 +276,10 @@ int fk_batch_run(fk_batch* b, int traverse) {
   if (trav == FK_TRAVERSE_AUTO) trav = b->traverse;
   if (trav == FK_TRAVERSE_ORDERED && b->traverse == FK_TRAVERSE_SKIP && !(traverse & FK_TRAVERSE_MASK))
     trav = FK_TRAVERSE_SKIP;
+  if (trav > FK_TRAVERSE_ORDERED4)
+    return fk_fail(b->ctx, FK_ERR_INVALID, "fk_batch_run: unknown traversal");
+  if (trav == FK_TRAVERSE_ORDERED4 && !b->ordered4_ok)
+    return fk_fail(b->ctx, FK_ERR_INVALID, "fk_batch_run: a job's tree is too deep for the 4-wide traversal");
   return batch_run_chunks(b, trav, filter, b->tuning);
 }
 

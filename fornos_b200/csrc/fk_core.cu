@@ -2,6 +2,8 @@
 // (include/fornos_gpu.h).  Replaces the GL buffer layer: ComputeBuffer<T>
 // (Src/compute.h:37-87) and the uploads of MeshMapping::init
 // (Src/meshmapping.cpp:128-184).
+#include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -255,6 +257,78 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     std::memcpy(f, ints, 16);
     w[3] = make_float4(f[0], f[1], f[2], f[3]);
   }
+  // Collapsed 4-wide layout: the record at the root and every record two
+  // levels below a 4-wide node become 4-wide nodes whose children are the
+  // record's children, each inner child replaced by its own two children.
+  // Leaves and their boxes are those of the 2-wide records, bit for bit.
+  // 128 bytes per node: lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of children 0..3,
+  // their refs (4-wide node index, or -(flattened leaf index + 1)), and the
+  // child count; unused slots repeat child 0 and are masked by the count.
+  std::vector<float4> wide4;
+  uint32_t n4 = 0, depth4 = 0;
+  if (nw > 0) {
+    struct Ent {
+      float lo[3], hi[3];
+      int32_t ref;
+    };
+    auto child = [&](uint32_t r, int k) {
+      const float4* w = &wide[4 * (size_t)r];
+      Ent e;
+      if (k == 0) {
+        e = {{w[0].x, w[0].z, w[2].x}, {w[0].y, w[0].w, w[2].y}, 0};
+        std::memcpy(&e.ref, &w[3].x, 4);
+      } else {
+        e = {{w[1].x, w[1].z, w[2].z}, {w[1].y, w[1].w, w[2].w}, 0};
+        std::memcpy(&e.ref, &w[3].y, 4);
+      }
+      return e;
+    };
+    std::vector<uint32_t> list{0};  // 2-wide records that become 4-wide nodes
+    std::vector<uint32_t> lvl{1};
+    std::vector<std::array<Ent, 4>> kids;
+    std::vector<int> counts;
+    for (size_t q = 0; q < list.size(); ++q) {
+      std::array<Ent, 4> e{};
+      int m = 0;
+      for (int k = 0; k < 2; ++k) {
+        Ent c = child(list[q], k);
+        if (c.ref >= 0) {
+          e[m++] = child((uint32_t)c.ref, 0);
+          e[m++] = child((uint32_t)c.ref, 1);
+        } else {
+          e[m++] = c;
+        }
+      }
+      for (int k = 0; k < m; ++k)
+        if (e[k].ref >= 0) {
+          const uint32_t r = (uint32_t)e[k].ref;
+          e[k].ref = (int32_t)list.size();
+          list.push_back(r);
+          lvl.push_back(lvl[q] + 1);
+        }
+      for (int k = m; k < 4; ++k) e[k] = e[0];
+      kids.push_back(e);
+      counts.push_back(m);
+      depth4 = std::max(depth4, lvl[q]);
+    }
+    n4 = (uint32_t)list.size();
+    wide4.resize(8 * (size_t)n4);
+    for (uint32_t k = 0; k < n4; ++k) {
+      float4* w = &wide4[8 * (size_t)k];
+      const auto& e = kids[k];
+      for (int a = 0; a < 3; ++a) {
+        w[2 * a] = make_float4(e[0].lo[a], e[1].lo[a], e[2].lo[a], e[3].lo[a]);
+        w[2 * a + 1] = make_float4(e[0].hi[a], e[1].hi[a], e[2].hi[a], e[3].hi[a]);
+      }
+      float f[4];
+      int32_t ints[4] = {e[0].ref, e[1].ref, e[2].ref, e[3].ref};
+      std::memcpy(f, ints, 16);
+      w[6] = make_float4(f[0], f[1], f[2], f[3]);
+      int32_t cnt[4] = {counts[k], 0, 0, 0};
+      std::memcpy(f, cnt, 16);
+      w[7] = make_float4(f[0], f[1], f[2], f[3]);
+    }
+  }
   fk_scene* s = new (std::nothrow) fk_scene();
   if (!s) return FK_ERR_NOMEM;
   s->ctx = ctx;
@@ -263,6 +337,8 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   s->depth = maxd;
   s->leaf_count = leaves;
   s->wide_count = nw;
+  s->wide4_count = n4;
+  s->depth4 = depth4;
   s->root_is_leaf = nodes[0].jump == 1;
   // The filtered box test assumes |box - origin| < 2^26; ray origins lie on
   // the scene's triangles, so box and corner coordinates below 2^24 suffice.
@@ -293,6 +369,7 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   up((void**)&s->pos4, pos4, cb);
   up((void**)&s->nrm4, nrm4, cb);
   up((void**)&s->wide, wide.data(), sizeof(float4) * wide.size());
+  up((void**)&s->wide4, wide4.data(), sizeof(float4) * wide4.size());
   if (rc == FK_OK) {
     rc = fk_dev_alloc(ctx, (void**)&s->tri_rec, 4 * sizeof(float4) * (size_t)(nc / 3));
     s->bytes += 4 * sizeof(float4) * (size_t)(nc / 3);
@@ -315,7 +392,7 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
 int fk_scene_free(fk_ctx* ctx, fk_scene* s) {
   if (!ctx || !s || !ctx->scenes.count(s)) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_free: unknown scene");
   cudaStreamSynchronize(ctx->stream);
-  void* ps[] = {s->node_lo, s->node_hi, s->node_jump, s->pos4, s->nrm4, s->wide, s->tri_rec};
+  void* ps[] = {s->node_lo, s->node_hi, s->node_jump, s->pos4, s->nrm4, s->wide, s->wide4, s->tri_rec};
   for (void* p : ps) fk_dev_free(p);
   ctx->scenes.erase(s);
   delete s;

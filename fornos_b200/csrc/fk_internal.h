@@ -52,6 +52,9 @@ struct fk_scene {
   // boxes (4 x float4), and one 64-byte precomputed record per triangle.
   float4* wide = nullptr;
   uint32_t wide_count = 0;
+  // Collapsed layout: 128-byte 4-wide nodes over the same leaves.
+  float4* wide4 = nullptr;
+  uint32_t wide4_count = 0, depth4 = 0;
   float4* tri_rec = nullptr;
   uint32_t root_is_leaf = 0;
   uint32_t filter_ok = 0;        // every coordinate below 2^24 in magnitude
@@ -101,6 +104,7 @@ struct SceneDev {
   const float4* __restrict__ pos4;
   const float4* __restrict__ nrm4;
   const float4* __restrict__ wide;
+  const float4* __restrict__ wide4;
   const float4* __restrict__ rec;
   uint32_t node_count;
   uint32_t root_is_leaf;
@@ -108,6 +112,10 @@ struct SceneDev {
   uint32_t filter_ok;  // scene coordinates small enough for the filtered box test
 };
 SceneDev scene_dev(const fk_scene* s);
+
+// Deepest collapsed (4-wide) tree the 4-wide traversal accepts: it defers at
+// most 3 entries per level within its 64-entry stack.
+constexpr uint32_t kMaxOrdered4Depth = 21;
 
 // One job of a batched hemisphere launch (device-side job table entry).
 static constexpr uint32_t kMaxBatchJobs = 64;

@@ -38,6 +38,7 @@ static SceneDev dev_of(const fk_scene* s) {
   d.pos4 = s->pos4;
   d.nrm4 = s->nrm4;
   d.wide = s->wide;
+  d.wide4 = s->wide4;
   d.rec = s->tri_rec;
   d.node_count = s->node_count;
   d.root_is_leaf = s->root_is_leaf;
@@ -138,6 +139,11 @@ __device__ float trace_skip(const SceneDev& s, f3 o, f3 d, float lo, float hi, T
 
 static constexpr int kStack = 64;
 static constexpr uint32_t kMaxOrderedDepth = 48;  // deeper trees use the skip walk
+// The 4-wide traversal defers at most 3 entries per level.
+static_assert(kMaxOrdered4Depth == (kStack - 1) / 3, "4-wide depth limit follows the stack size");
+__host__ __device__ constexpr bool is_ordered(int trav) {
+  return trav == FK_TRAVERSE_ORDERED || trav == FK_TRAVERSE_ORDERED4;
+}
 
 // Near-first traversal of the children-in-parent layout with the same
 // pruning rule.  The host selects it only when the tree depth fits kStack;
@@ -390,20 +396,27 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
   if (trav == FK_TRAVERSE_ORDERED && s->depth > kMaxOrderedDepth)
     return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 48; use FK_TRAVERSE_SKIP");
+  if (trav == FK_TRAVERSE_ORDERED4 && s->depth4 > kMaxOrdered4Depth)
+    return fk_fail(ctx, FK_ERR_INVALID, "4-wide traversal needs a 4-wide depth <= 21; use FK_TRAVERSE_ORDERED");
   if (sched == 0) sched = FK_SCHEDULE_DYNAMIC;
   if (h.ids && sched != FK_SCHEDULE_DYNAMIC)
     return fk_fail(ctx, FK_ERR_UNSUPPORTED, "texel lists run on the dynamic schedule only");
+  if (trav == FK_TRAVERSE_ORDERED4 && sched != FK_SCHEDULE_DYNAMIC)
+    return fk_fail(ctx, FK_ERR_UNSUPPORTED, "the 4-wide traversal runs on the dynamic schedule only");
   const uint32_t refill = h.refill ? h.refill : ctx->tuning.refill;
   const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
   const uint32_t leaf_batch = h.leaf_batch ? h.leaf_batch : ctx->tuning.leaf_batch;
   const uint32_t speculate = h.speculate ? h.speculate : ctx->tuning.speculate;
-#define FK_HEMI_CASE(K)                                                                              \
-  case K:                                                                                            \
-    if (sched == FK_SCHEDULE_DYNAMIC)                                                                \
-      return trav == FK_TRAVERSE_ORDERED                                                            \
-                 ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill, filter, leaf_batch, speculate)   \
-                 : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill, filter, leaf_batch, speculate);     \
-    return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a)                    \
+#define FK_HEMI_CASE(K)                                                                                     \
+  case K:                                                                                                   \
+    if (sched == FK_SCHEDULE_DYNAMIC) {                                                                     \
+      if (trav == FK_TRAVERSE_ORDERED4)                                                                     \
+        return run_hemi_dynamic<K, FK_TRAVERSE_ORDERED4>(ctx, a, refill, filter, leaf_batch, speculate);  \
+      return trav == FK_TRAVERSE_ORDERED                                                                   \
+                 ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill, filter, leaf_batch, speculate)  \
+                 : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill, filter, leaf_batch, speculate);    \
+    }                                                                                                       \
+    return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a)                           \
                                        : run_hemi<K, FK_TRAVERSE_SKIP>(ctx, a);
   switch (h.kind) {
     FK_HEMI_CASE(FK_AO)
@@ -461,6 +474,18 @@ __device__ __forceinline__ uint32_t list_texel(const uint32_t* ids, uint32_t lim
 template <bool FILTER>
 __device__ __forceinline__ bool child_hit(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
   if (FILTER) return box_hit(r, lo, hi, thr, entry);
+  entry = ray_box(r.o, r.d, lo, hi);
+  return entry < thr;
+}
+
+// Inner-phase child test of the ordered traversals.  The filtered form is
+// conservative: a box there only prunes (the exact slab test is monotone, so a
+// box inside one the ray misses is missed too), and every leaf's box is
+// tested exactly when the leaf is visited, so accepting an uncertain box only
+// adds work.  That keeps the divisions out of the inner phase.
+template <bool FILTER>
+__device__ __forceinline__ bool child_maybe(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
+  if (FILTER) return box_maybe(r, lo, hi, thr, entry);
   entry = ray_box(r.o, r.d, lo, hi);
   return entry < thr;
 }
@@ -525,8 +550,8 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   const float4* w = s.wide + 4 * (size_t)st.cur;
   float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
   float d0, d1;
-  const bool h0 = child_hit<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
-  const bool h1 = child_hit<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
+  const bool h0 = child_maybe<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
+  const bool h1 = child_maybe<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
   if (COUNT) tally.box += 2;
   const bool swap = d1 < d0;
   const bool hn = swap ? h1 : h0, hf = swap ? h0 : h1;
@@ -539,12 +564,84 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   return true;
 }
 
+// Compare-exchange of (key, ref) pairs: ascending keys.
+__device__ __forceinline__ void cex(float& ka, int32_t& ra, float& kb, int32_t& rb) {
+  const bool sw = kb < ka;
+  const float k = sw ? kb : ka;
+  kb = sw ? ka : kb;
+  ka = k;
+  const int32_t r = sw ? rb : ra;
+  rb = sw ? ra : rb;
+  ra = r;
+}
+
+// Inner phase over the collapsed layout: tests the 2 to 4 children of 4-wide
+// node `cur` (four independent box tests), orders the hits by entry distance
+// (a 5-comparator sorting network), keeps the nearest inner child as the next
+// node and the nearest leaf as the postponed leaf when none is held, and
+// defers the rest farthest first, so that the nearest is popped next.
+template <bool COUNT, bool FILTER>
+__device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
+                                             int* status, Tally& tally) {
+  const float4* w = s.wide4 + 8 * (size_t)st.cur;
+  const float4 lx = __ldg(w), hx = __ldg(w + 1), ly = __ldg(w + 2), hy = __ldg(w + 3);
+  const float4 lz = __ldg(w + 4), hz = __ldg(w + 5), rf = __ldg(w + 6);
+  const int cnt = __float_as_int(__ldg(w + 7).x);
+  const float inf = __int_as_float(0x7f800000);
+  float k0, k1, k2, k3;
+  const bool h0 = child_maybe<FILTER>(rp, mk3(lx.x, ly.x, lz.x), mk3(hx.x, hy.x, hz.x), thr, k0);
+  const bool h1 = child_maybe<FILTER>(rp, mk3(lx.y, ly.y, lz.y), mk3(hx.y, hy.y, hz.y), thr, k1);
+  const bool h2 = child_maybe<FILTER>(rp, mk3(lx.z, ly.z, lz.z), mk3(hx.z, hy.z, hz.z), thr, k2) && cnt > 2;
+  const bool h3 = child_maybe<FILTER>(rp, mk3(lx.w, ly.w, lz.w), mk3(hx.w, hy.w, hz.w), thr, k3) && cnt > 3;
+  if (COUNT) tally.box += cnt;
+  // a hit's entry distance is finite (it is below thr); misses sort last as +inf
+  k0 = h0 ? k0 : inf;
+  k1 = h1 ? k1 : inf;
+  k2 = h2 ? k2 : inf;
+  k3 = h3 ? k3 : inf;
+  int32_t r0 = __float_as_int(rf.x), r1 = __float_as_int(rf.y), r2 = __float_as_int(rf.z), r3 = __float_as_int(rf.w);
+  cex(k0, r0, k1, r1);
+  cex(k2, r2, k3, r3);
+  cex(k0, r0, k2, r2);
+  cex(k1, r1, k3, r3);
+  cex(k1, r1, k2, r2);
+  const bool v0 = k0 < inf, v1 = k1 < inf, v2 = k2 < inf, v3 = k3 < inf;
+  const bool n0 = v0 && r0 >= 0, n1 = v1 && r1 >= 0, n2 = v2 && r2 >= 0, n3 = v3 && r3 >= 0;
+  const bool l0 = v0 && r0 < 0, l1 = v1 && r1 < 0, l2 = v2 && r2 < 0, l3 = v3 && r3 < 0;
+  const int ni = n0 ? 0 : (n1 ? 1 : (n2 ? 2 : (n3 ? 3 : 4)));
+  const int nl = (l0 ? 0 : (l1 ? 1 : (l2 ? 2 : (l3 ? 3 : 4))));
+  const int keep = st.pend < 0 ? nl : 4;  // the leaf that becomes the postponed leaf, if any
+  if (v3 && ni != 3 && keep != 3 && !push(stk, st.sp, r3, k3, status)) return false;
+  if (v2 && ni != 2 && keep != 2 && !push(stk, st.sp, r2, k2, status)) return false;
+  if (v1 && ni != 1 && keep != 1 && !push(stk, st.sp, r1, k1, status)) return false;
+  if (v0 && ni != 0 && keep != 0 && !push(stk, st.sp, r0, k0, status)) return false;
+  if (keep < 4) {
+    const int32_t r = keep == 0 ? r0 : (keep == 1 ? r1 : (keep == 2 ? r2 : r3));
+    st.pend = -r - 1;
+    st.pend_dist = keep == 0 ? k0 : (keep == 1 ? k1 : (keep == 2 ? k2 : k3));
+  }
+  st.cur = ni == 0 ? r0 : (ni == 1 ? r1 : (ni == 2 ? r2 : (ni == 3 ? r3 : -1)));
+  return true;
+}
+
+template <int TRAV, bool COUNT, bool FILTER>
+__device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
+                                            int* status, Tally& tally) {
+  if (TRAV == FK_TRAVERSE_ORDERED4) return inner_visit4<COUNT, FILTER>(s, rp, thr, st, stk, status, tally);
+  return inner_visit<COUNT, FILTER>(s, rp, thr, st, stk, status, tally);
+}
+
 // Leaf phase: the postponed leaf's triangles, if its box still passes.
 template <bool COUNT, bool FILTER>
 __device__ __forceinline__ void leaf_visit(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
                                            OState& st, Tally& tally) {
-  if (still_open<FILTER>(st.pend_dist, fminf(best, hi))) {
-    const uint32_t b = as_u32(__ldg(s.node_lo + st.pend).w), e = as_u32(__ldg(s.node_hi + st.pend).w);
+  // The leaf's own box decides here, exactly, against the current threshold
+  // (inner-phase tests of it may have been conservative).
+  const float4 L = __ldg(s.node_lo + st.pend), H = __ldg(s.node_hi + st.pend);
+  float entry;
+  if (COUNT) tally.box++;
+  if (child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry)) {
+    const uint32_t b = as_u32(L.w), e = as_u32(H.w);
     if (COUNT) tally.tri += (e - b) / 3;
     for (uint32_t k = b; k < e; k += 3) tri_sample(s.rec, k / 3, rp.o, rp.d, lo, best);
   }
@@ -597,7 +694,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
-  int2 stk[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];  // deferred (ref, entry) pairs
+  int2 stk[is_ordered(TRAV) ? kStack : 1];  // deferred (ref, entry) pairs
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t r = 0;
@@ -605,9 +702,13 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
   float best = FLT_MAX;
   int32_t cur = 0;  // skip walk: node index
   OState st = {-1, -1, 0.0f, 0};
+  // counting variant, per warp: iterations, leaf-phase iterations, lanes at
+  // work in inner / leaf phases, lanes holding a ray, refills
+  unsigned long long wc[6] = {0, 0, 0, 0, 0, 0};
   for (;;) {
     unsigned idle = __ballot_sync(full, !active);
     if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
+      if (COUNT) wc[5]++;
       const uint32_t n_idle = __popc(idle);
       const int leader = __ffs(idle) - 1;
       uint32_t base = 0;
@@ -630,7 +731,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
             f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
             rp = ray_pre(o, dir);
             if (!p.s.filter_ok) rp.exact_only = true;
-            if (TRAV == FK_TRAVERSE_ORDERED) {
+            if (is_ordered(TRAV)) {
               float4 L = __ldg(p.s.node_lo), H = __ldg(p.s.node_hi);
               float a = ray_box(o, dir, xyz(L), xyz(H));
               if (COUNT) tally.box++;
@@ -655,12 +756,20 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
       idle = __ballot_sync(full, !active);
     }
     if (exhausted && idle == full) break;
-    if (TRAV == FK_TRAVERSE_ORDERED) {
+    if (COUNT) {
+      wc[0]++;
+      wc[4] += 32 - __popc(idle);
+    }
+    if (is_ordered(TRAV)) {
       // phase choice, uniform across the warp
       const bool spec_ok = st.sp < kStack - 4;
       const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
       const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
+      if (COUNT) {
+        wc[1] += leaf_phase;
+        wc[leaf_phase ? 3 : 2] += __popc(leaf_phase ? leaves : need);
+      }
       if (active) {
         bool fin = false;
         if (leaf_phase) {
@@ -669,7 +778,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
             fin = settled<STOP>(best, p.hi);
           }
         } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
-          if (!inner_visit<COUNT, FILTER>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally))
+          if (!visit_inner<TRAV, COUNT, FILTER>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally))
             fin = true;
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, p.hi));
@@ -694,6 +803,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
     if (lane == 0) {
       atomicAdd(p.tally, b);
       atomicAdd(p.tally + 1, t);
+      for (int k = 0; k < 6; ++k) atomicAdd(p.tally + 2 + k, wc[k]);
     }
   }
 }
@@ -849,7 +959,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
   const unsigned lower = (1u << lane) - 1u;
   // a launch traces at most the scratch's 2^27 rays: lane indices fit 32 bits
   const uint32_t total = (uint32_t)((p.r1 - p.r0 + p.stride - 1) / p.stride);
-  int2 stk[TRAV == FK_TRAVERSE_ORDERED ? kStack : 1];  // deferred (ref, entry) pairs
+  int2 stk[is_ordered(TRAV) ? kStack : 1];  // deferred (ref, entry) pairs
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t q = 0;
@@ -894,7 +1004,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
             f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
             rp = ray_pre(o, dir);
             if (!J.s.filter_ok) rp.exact_only = true;
-            if (TRAV == FK_TRAVERSE_ORDERED) {
+            if (is_ordered(TRAV)) {
               float4 L = __ldg(J.s.node_lo), H = __ldg(J.s.node_hi);
               float aa = ray_box(o, dir, xyz(L), xyz(H));
               if (aa < hi) {
@@ -920,7 +1030,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
     }
     if (exhausted && idle == full) break;
     const SceneDev& s = jobs[j].s;
-    if (TRAV == FK_TRAVERSE_ORDERED) {
+    if (is_ordered(TRAV)) {
       const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
       const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
@@ -932,7 +1042,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
             fin = settled<STOP>(best, hi);
           }
         } else if (st.cur >= 0 && st.pend < 0) {
-          if (!inner_visit<false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally))
+          if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally))
             fin = true;
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, hi));
@@ -1058,6 +1168,9 @@ cudaError_t launch_batch(const BatchArgs& a, int kind, int trav, bool filter, cu
                          bool reduce) {
 #define FK_BATCH_CASE(K)                                                                                   \
   case K:                                                                                                  \
+    if (trav == FK_TRAVERSE_ORDERED4)                                                                      \
+      return filter ? batch_launch<K, FK_TRAVERSE_ORDERED4, true>(a, stream, sm_count, reduce)            \
+                    : batch_launch<K, FK_TRAVERSE_ORDERED4, false>(a, stream, sm_count, reduce);          \
     if (trav == FK_TRAVERSE_ORDERED)                                                                       \
       return filter ? batch_launch<K, FK_TRAVERSE_ORDERED, true>(a, stream, sm_count, reduce)             \
                     : batch_launch<K, FK_TRAVERSE_ORDERED, false>(a, stream, sm_count, reduce);           \
@@ -1145,11 +1258,17 @@ int launch_hemisphere_external(const fk_scene* s, const HemiLaunch& h, cudaStrea
     err = "ordered traversal needs tree depth <= 48; use FK_TRAVERSE_SKIP";
     return FK_ERR_INVALID;
   }
+  if (trav == FK_TRAVERSE_ORDERED4 && s->depth4 > kMaxOrdered4Depth) {
+    err = "4-wide traversal needs a 4-wide depth <= 21; use FK_TRAVERSE_ORDERED";
+    return FK_ERR_INVALID;
+  }
   const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
   cudaError_t e = cudaSuccess;
 #define FK_EXT_CASE(K)                                                                                     \
   case K:                                                                                                  \
-    e = trav == FK_TRAVERSE_ORDERED                                                                        \
+    e = trav == FK_TRAVERSE_ORDERED4                                                                       \
+            ? run_hemi_external<K, FK_TRAVERSE_ORDERED4>(a, stream, sm_count, tun, filter, dist, queue)   \
+        : trav == FK_TRAVERSE_ORDERED                                                                      \
             ? run_hemi_external<K, FK_TRAVERSE_ORDERED>(a, stream, sm_count, tun, filter, dist, queue)    \
             : run_hemi_external<K, FK_TRAVERSE_SKIP>(a, stream, sm_count, tun, filter, dist, queue);      \
     break;

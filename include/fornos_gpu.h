@@ -202,6 +202,7 @@ typedef struct fk_sample_params {
 #define FK_TRAVERSE_AUTO 0    /* tuned choice for the scene */
 #define FK_TRAVERSE_ORDERED 1 /* near-first stack traversal over the BVH2 layout */
 #define FK_TRAVERSE_SKIP 2    /* the reference's skip-pointer walk, node order */
+#define FK_TRAVERSE_ORDERED4 3 /* near-first stack traversal over the collapsed 4-wide layout */
 #define FK_TRAVERSE_MASK 0x0F
 /* Ray scheduling, or-ed into the traversal argument (0 = tuned choice). */
 #define FK_SCHEDULE_STATIC 0x10  /* one warp per texel, lanes = samples */
@@ -356,8 +357,9 @@ typedef struct fk_batch_job {
 int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t job_count, int kind, fk_batch** out);
 int fk_batch_info(const fk_batch* batch, uint64_t* rays, uint32_t* texels, uint32_t* launches_per_run);
 /* Autotuner: times a strided sample of about sample_rays rays of every job
- * (0 = 4M) under each candidate schedule (ordered vs skip-pointer traversal,
- * filtered vs divided box tests, refill threshold, postponed-leaf batch) and
+ * (0 = 4M) under each candidate schedule (ordered over the 2-wide or the
+ * collapsed 4-wide layout vs the skip-pointer walk, filtered vs divided box
+ * tests, refill threshold, postponed-leaf batch) and
  * keeps the fastest for later runs; reports it. */
 int fk_batch_tune(fk_batch* batch, uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse);
 /* One run on the context's stream; traverse 0 = the tuned schedule. */
@@ -435,6 +437,14 @@ int fk_diag_fp32_peak(fk_ctx* ctx, double* ops_per_second);
 int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
                              const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
                              int traverse, uint64_t* tests);
+/* The same run's lane-utilisation profile of the dynamic schedule (8
+ * counters): box tests, triangle tests, warp iterations, iterations in a leaf
+ * phase, lanes doing inner work summed over inner-phase iterations, lanes
+ * holding a leaf summed over leaf-phase iterations, lanes holding a ray summed
+ * over all iterations, refills. */
+int fk_diag_traversal_profile(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
+                              const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
+                              int traverse, uint64_t* counters);
 
 /* ------------------------------------------------------------ learned denoiser
  * No counterpart in the reference.  A per-texel MLP that turns a low-sample

@@ -68,7 +68,7 @@ def check(jobs, outs, kind, want):
 
 
 @pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK, api.AO_BN])
-@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_SKIP])
+@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_ORDERED4, api.TRAVERSE_SKIP])
 def test_batch_equals_jobs_alone(ctx, setup, kind, trav):
     want = [alone(ctx, j, kind, trav) for j in setup]
     b, outs = make_batch(ctx, setup, kind)
@@ -97,7 +97,7 @@ def test_autotuner_choice_gives_same_results(ctx, setup):
     kind = api.THICK
     b, outs = make_batch(ctx, setup, kind)
     best = b.tune(sample_rays=1 << 16)
-    assert best["traverse"] & 0x0F in (api.TRAVERSE_ORDERED, api.TRAVERSE_SKIP)
+    assert best["traverse"] & 0x0F in (api.TRAVERSE_ORDERED, api.TRAVERSE_ORDERED4, api.TRAVERSE_SKIP)
     assert 1 <= best["refill"] <= 32 and 1 <= best["leaf_batch"] <= 32
     want = [alone(ctx, j, kind, best["traverse"] & 0x0F) for j in setup]
     b.run()

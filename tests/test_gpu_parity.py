@@ -148,6 +148,39 @@ def test_hemisphere_ordered_matches(ctx, oracle, name, kind, sched):
     assert (~ok).mean() <= 1e-3
 
 
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK, api.AO_BN])
+@pytest.mark.parametrize("exact", [False, True])
+def test_hemisphere_ordered4_matches(ctx, oracle, name, kind, exact):
+    """The collapsed 4-wide layout holds the same leaves and leaf boxes, so it
+    meets the ordered traversal's bar against the reference order."""
+    c = case(name)
+    _, _, mm = mapped(ctx, oracle, c)
+    spp, lo, hi = 32, 0.001, 0.3
+    flags = api.TRAVERSE_ORDERED4 | api.SCHEDULE_DYNAMIC | (api.EXACT_BOX_TESTS if exact else 0)
+    samples, got = run_hemi(ctx, mm, kind, spp, lo, hi, flags)
+    k = api.AO if kind == api.AO_BN else kind
+    ref, rhits, tidx = oracle_hemi(oracle, c, mm, k, samples, spp, lo, hi)
+    hit = tidx != api.MISS
+    out, hits = got[0], got[1]
+    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
+    assert (hits[hit] != rhits[hit]).mean() <= 1e-3
+    ok = bits(out[hit]) == bits(ref[hit])
+    if kind == api.BN:
+        ok = np.all(ok, axis=1)
+    assert (~ok).mean() <= 1e-3
+    if kind == api.AO_BN:
+        bref, bhits, _ = oracle_hemi(oracle, c, mm, api.BN, samples, spp, lo, hi)
+        assert (got[3][hit] != bhits[hit]).mean() <= 1e-3
+        assert (~np.all(bits(got[2][hit]) == bits(bref[hit]), axis=1)).mean() <= 1e-3
+
+
+def test_ordered4_needs_the_dynamic_schedule(ctx, oracle):
+    _, _, mm = mapped(ctx, oracle, case("sphere"))
+    with pytest.raises(api.FornosError):
+        run_hemi(ctx, mm, api.AO, 8, 0.0, 0.3, api.TRAVERSE_ORDERED4 | api.SCHEDULE_STATIC)
+
+
 def test_ao_bn_fused_equals_separate(ctx, oracle):
     c = case("plane")
     _, _, mm = mapped(ctx, oracle, c)
@@ -254,7 +287,7 @@ def test_errors_are_reported_not_fatal(ctx):
 
 @pytest.mark.parametrize("name", list(CASES))
 @pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK, api.AO_BN])
-@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_SKIP])
+@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_ORDERED4, api.TRAVERSE_SKIP])
 def test_filtered_box_tests_equal_exact(ctx, oracle, name, kind, trav):
     """The reciprocal-filtered box test must take every decision the divided
     one takes: outputs and counts are identical bit for bit."""

@@ -42,7 +42,7 @@ def read(bufs, n, kind):
 
 
 @pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK, api.AO_BN])
-@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_SKIP])
+@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_ORDERED4, api.TRAVERSE_SKIP])
 def test_texel_list_equals_whole_map(ctx, mapped_sphere, kind, trav):
     mm = mapped_sphere
     n = mm.tmap.count
