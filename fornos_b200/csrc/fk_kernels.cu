@@ -963,12 +963,14 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t q = 0;
-  int j = 0;
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX, lo = 0.0f, hi = 0.0f;
   int32_t cur = 0;
   uint32_t end = 0;  // skip walk: one past the job's last node
   OState st = {-1, -1, 0.0f, 0};
+  // the lane's job scene, copied from the table when the lane starts a ray so
+  // that node visits read its arrays' addresses from registers
+  SceneDev sc = {};
   for (;;) {
     unsigned idle = __ballot_sync(full, !active);
     if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
@@ -987,8 +989,8 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
             int m = (a + b + 1) >> 1;
             if (jobs[m].ray_base <= r) a = m; else b = m - 1;
           }
-          j = a;
-          const BatchJobDev& J = jobs[j];
+          const BatchJobDev& J = jobs[a];
+          sc = J.s;
           const unsigned long long local = r - J.ray_base;
           const uint32_t g = (uint32_t)(local / J.spp), k = (uint32_t)(local % J.spp);
           const uint32_t id = __ldg(J.tidx + g);
@@ -1029,7 +1031,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
       idle = __ballot_sync(full, !active);
     }
     if (exhausted && idle == full) break;
-    const SceneDev& s = jobs[j].s;
+    const SceneDev& s = sc;
     if (is_ordered(TRAV)) {
       const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
