@@ -417,6 +417,34 @@ def denoise_compare(ctx, stream, prep, scene, weights, seed):
     runs = [timed(bake) for _ in range(3)]
     t_dn, stats, clk_dn = sorted(runs, key=lambda r: r[0])[1]
     ctx.check()
+    # the network alone on each engine, over the 16-sample bake's feature image
+    ao16, bn16 = ctx.buffer(4 * n), ctx.buffer(12 * n)
+    api.hemisphere(ctx, scene, coords, tidx, api.AO_BN, d["low"], *args, low, ao16, bn16, None, None, 0, n)
+    pos, nrm = ctx.buffer(12 * n), ctx.buffer(12 * n)
+    api.gather(ctx, scene, api.GATHER_POSITION, coords, tidx, pos, 0, n)
+    api.gather(ctx, scene, api.GATHER_NORMAL, coords, tidx, nrm, 0, n)
+    image = api.denoise_features(ctx, tm, coords, tidx, ao16, bn16, pos, nrm, d["max_d"])
+    oa, ob = ctx.buffer(4 * n), ctx.buffer(12 * n)
+    net = {}
+    flop = 2 * (250 * 64 + 64 * 64 + 64 * 4)  # per texel, without the padding
+    peak = None
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"]
+    except (OSError, KeyError, ValueError):
+        pass
+    for name, eng in (("tcgen05", api.DN_ENGINE_TCGEN05), ("mma_sync", api.DN_ENGINE_MMA_SYNC)):
+        dn.set_engine(eng)
+        dn.apply(tm, image, tidx, ao16, bn16, oa, ob)  # warm-up
+        ms = sorted(timed(lambda: dn.apply(tm, image, tidx, ao16, bn16, oa, ob))[0] for _ in range(5))[2]
+        tf = flop * n / (ms * 1e-3) / 1e12
+        net[name] = dict(ms=round(ms, 3), tflops=round(tf, 2),
+                         frac_of_bf16_peak=round(tf / peak, 4) if peak else None)
+    dn.set_engine(api.DN_ENGINE_TCGEN05)
+    ctx.check()
+    net["flop_per_texel"] = flop
+    net["peak"] = "%s TFLOP/s bf16 (MEASURED_PEAKS.json, burst)" % peak if peak else "MEASURED_PEAKS.json absent"
+    for b in (ao16, bn16, pos, nrm, image, oa, ob):
+        b.free()
     # accuracy against 4096-sample values on random texels with a mapping hit
     ids = np.sort(np.random.default_rng(seed).choice(hit, min(d["mae_texels"], len(hit)), replace=False))
     ids = ids.astype(np.uint32)
@@ -443,6 +471,7 @@ def denoise_compare(ctx, stream, prep, scene, weights, seed):
             d["label"], len(ids)),
         "fallback_rule": "tile %d x %d, %d spot checks at %d samples, re-bake if error > %.2f" % (
             d["tile"], d["tile"], d["cells"] ** 2, d["full"], d["max_err"]),
+        "network_kernel": net,
     }
     res["speedup"] = round(t_plain / t_dn, 2)
     for b in (tm, coords, tidx, low, full, label, pao, pbn, dao, dbn, lao, lbn):

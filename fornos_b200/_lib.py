@@ -173,6 +173,7 @@ _SIGS = {
                                           c_u32, c_int, ctypes.POINTER(c_u64)]),
     "fk_denoiser_create": (c_int, [c_vp, ctypes.POINTER(c_vp)]),
     "fk_denoiser_free": (c_int, [c_vp]),
+    "fk_denoiser_set_engine": (c_int, [c_vp, c_int]),
     "fk_denoiser_set_params": (c_int, [c_vp, f32p, c_u32]),
     "fk_denoiser_get_params": (c_int, [c_vp, f32p, c_u32]),
     "fk_denoise_features": (c_int, [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_float, c_vp]),

@@ -672,6 +672,7 @@ DN_INPUTS = 250
 DN_PARAMS = 20868
 DN_ROW_BYTES = 512
 DN_TILE_ROWS = 128
+DN_ENGINE_MMA_SYNC, DN_ENGINE_TCGEN05 = 0, 1
 DN_HIDDEN = 64
 DN_OUT = 4
 # parameter blocks: name -> (offset, shape)
@@ -708,6 +709,10 @@ class Denoiser:
         self.handle = h.value
         if params is not None:
             self.set_params(params)
+
+    def set_engine(self, engine):
+        """Inference kernel: DN_ENGINE_TCGEN05 (default) or DN_ENGINE_MMA_SYNC."""
+        _check(self.ctx.lib.fk_denoiser_set_engine(self.handle, engine), self.ctx, "fk_denoiser_set_engine")
 
     def set_params(self, params):
         p = np.ascontiguousarray(params, np.float32).reshape(-1)

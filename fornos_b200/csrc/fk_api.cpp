@@ -455,6 +455,7 @@ int fk_ctx_check(fk_ctx* ctx) {
   if (st & 2) msg += "a texel names a triangle outside the scene; ";
   if (st & 4) msg += "a texel list holds an id beyond texel_count; ";
   if (st & 8) msg += "a training batch names a row beyond n_rows; ";
+  if (st & 16) msg += "a tensor-core wait of the denoiser ran out; ";
   msg += "results are incomplete";
   return fk_fail(ctx, FK_ERR_DEVICE, msg.c_str());
 }

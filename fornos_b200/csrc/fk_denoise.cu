@@ -80,6 +80,37 @@ __device__ __forceinline__ float2 oct_encode(float x, float y, float z) {
 
 __device__ __forceinline__ float clamp4(float v) { return fminf(fmaxf(v, -4.0f), 4.0f); }
 
+// The 10 features of neighbour j (< 25, row-major over the 5 x 5 window) of
+// the texel at pixel p; zeros outside the texture, without a mapping hit, or
+// for p = kNoTexel.
+__device__ __forceinline__ void neighbour_features(const float4* __restrict__ f0, const float4* __restrict__ f1,
+                                                   const float4* __restrict__ f2, uint32_t w, uint32_t h, uint32_t p,
+                                                   int j, float (&v)[10]) {
+#pragma unroll
+  for (int k = 0; k < 10; ++k) v[k] = 0.0f;
+  if (p == kNoTexel) return;
+  const int cx = (int)(p % w), cy = (int)(p / w);
+  const int x = cx + j % 5 - 2, y = cy + j / 5 - 2;
+  if (x < 0 || y < 0 || x >= (int)w || y >= (int)h) return;
+  const uint32_t q = (uint32_t)y * w + (uint32_t)x;
+  const float4 a = __ldg(f0 + q);
+  if (!(a.w > 0.0f)) return;
+  const float4 c = __ldg(f1 + p), b = __ldg(f1 + q), n = __ldg(f2 + q);
+  const float sp = __ldg(f2 + p).z;  // centre texel spacing
+  v[0] = a.x;
+  v[1] = a.y;
+  v[2] = a.z;
+  if (sp > 0.0f) {
+    v[3] = clamp4((b.x - c.x) / sp);
+    v[4] = clamp4((b.y - c.y) / sp);
+    v[5] = clamp4((b.z - c.z) / sp);
+  }
+  v[6] = n.x;
+  v[7] = n.y;
+  v[8] = b.w;
+  v[9] = 1.0f;
+}
+
 // One input row (256 bf16 = 128 words) for the texel at pixel p, written by a
 // whole warp: lane j < 25 writes neighbour j's 10 features, lane 25 the pad.
 __device__ __forceinline__ void assemble_row(const float4* __restrict__ f0, const float4* __restrict__ f1,
@@ -87,32 +118,7 @@ __device__ __forceinline__ void assemble_row(const float4* __restrict__ f0, cons
                                              int lane, uint32_t* dst) {
   if (lane < 25) {
     float v[10];
-#pragma unroll
-    for (int k = 0; k < 10; ++k) v[k] = 0.0f;
-    if (p != kNoTexel) {
-      const int cx = (int)(p % w), cy = (int)(p / w);
-      const int x = cx + lane % 5 - 2, y = cy + lane / 5 - 2;
-      if (x >= 0 && y >= 0 && x < (int)w && y < (int)h) {
-        const uint32_t q = (uint32_t)y * w + (uint32_t)x;
-        const float4 a = __ldg(f0 + q);
-        if (a.w > 0.0f) {
-          const float4 c = __ldg(f1 + p), b = __ldg(f1 + q), n = __ldg(f2 + q);
-          const float sp = __ldg(f2 + p).z;  // centre texel spacing
-          v[0] = a.x;
-          v[1] = a.y;
-          v[2] = a.z;
-          if (sp > 0.0f) {
-            v[3] = clamp4((b.x - c.x) / sp);
-            v[4] = clamp4((b.y - c.y) / sp);
-            v[5] = clamp4((b.z - c.z) / sp);
-          }
-          v[6] = n.x;
-          v[7] = n.y;
-          v[8] = b.w;
-          v[9] = 1.0f;
-        }
-      }
-    }
+    neighbour_features(f0, f1, f2, w, h, p, lane, v);
 #pragma unroll
     for (int k = 0; k < 5; ++k) dst[5 * lane + k] = pack2(v[2 * k], v[2 * k + 1]);
   } else if (lane == 25) {
@@ -685,6 +691,275 @@ __global__ void __launch_bounds__(256, 2) dn_apply_kernel(ApplyArgs a) {
   }
 }
 
+// ------------------------------------------------------------------ inference on tcgen05
+// The same network on sm_100's fifth-generation tensor cores: a CTA of one
+// warpgroup (128 threads) owns a 128-texel tile; the tile's input rows and the
+// weights sit in shared memory in the no-swizzle K-major core-matrix layout
+// (8 rows x 16 bytes per core matrix, core matrices 128 bytes apart along K
+// and SBO bytes apart along the rows), one elected thread issues
+// tcgen05.mma (kind::f16, BF16 operands, FP32 accumulation) for each layer
+// into tensor memory, and every thread reads its own row back with
+// tcgen05.ld (TMEM lane = tile row) for the bias / GELU epilogue, which writes
+// the next layer's operand.  Completion is tracked by an mbarrier that
+// tcgen05.commit arrives on; every wait on it is bounded and a timeout stops
+// the kernel with status bit 16 after freeing its tensor memory.
+namespace tc {
+// 16 warps: all gather input rows; for the epilogues, warps w, w + 4, w + 8 and
+// w + 12 share TMEM lane quarter w % 4 (the only lanes a warp may read) and
+// split its 64 accumulator columns 16 each.
+constexpr uint32_t kThreads = 512;
+constexpr uint32_t kTmemCols = 128;  // layer 1 / 3 accumulators at column 0, layer 2 at column 64
+constexpr uint32_t kA1 = 0;                  // 128 x 256 bf16
+constexpr uint32_t kW1 = kA1 + 128 * 256 * 2;  // 64 x 256
+constexpr uint32_t kA2 = kW1 + 64 * 256 * 2;   // 128 x 64
+constexpr uint32_t kA3 = kA2 + 128 * 64 * 2;   // 128 x 64
+constexpr uint32_t kW2 = kA3 + 128 * 64 * 2;   // 64 x 64
+constexpr uint32_t kW3 = kW2 + 64 * 64 * 2;    // 16 x 64, rows 4..15 zero
+constexpr uint32_t kBar = kW3 + 16 * 64 * 2;   // mbarrier (8 bytes)
+constexpr uint32_t kSlot = kBar + 8;           // allocated TMEM address
+constexpr uint32_t kBytes = kSlot + 8;
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+// Byte offset of element (r, k) in a K-major core-matrix tile whose rows hold
+// `kdim` elements: core matrices of 8 rows x 8 elements, 128 bytes each,
+// consecutive along K; row groups of 8 are kdim / 8 x 128 bytes apart.
+__device__ __forceinline__ uint32_t core_off(uint32_t r, uint32_t k, uint32_t kdim) {
+  return (r >> 3) * (kdim * 16) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2;
+}
+
+// Shared-memory matrix descriptor: start address, leading (K) and stride
+// (row-group) byte offsets in 16-byte units, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t instr_desc(uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+__device__ __forceinline__ bool wait(uint32_t bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it)
+    if (try_wait(bar, parity)) return true;
+  return false;
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// generic-proxy shared-memory writes become visible to the tensor cores' reads
+__device__ __forceinline__ void fence_proxy() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// all threads: tensor-core work before this point is ordered before the barrier,
+// and work after it after the barrier
+__device__ __forceinline__ void sync_all() {
+  fence_before();
+  __syncthreads();
+  fence_after();
+}
+
+__device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+// Bias + GELU of 16 accumulator columns (c0 .. c0 + 15) of this thread's row,
+// written into the row of the next layer's operand tile (K = 64).
+__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, uint32_t c0, const float* __restrict__ bias,
+                                                uint8_t* dst, uint32_t row) {
+  float v[16];
+  ld16(taddr + c0, v);
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    uint32_t w4[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      float dz;
+      const uint32_t c = c0 + 8 * h + 2 * e;
+      const float a0 = gelu(v[8 * h + 2 * e] + __ldg(bias + c), dz);
+      const float a1 = gelu(v[8 * h + 2 * e + 1] + __ldg(bias + c + 1), dz);
+      w4[e] = pack2(a0, a1);
+    }
+    *(uint4*)(dst + core_off(row, c0 + 8 * h, 64)) = make_uint4(w4[0], w4[1], w4[2], w4[3]);
+  }
+}
+}  // namespace tc
+
+__global__ void __launch_bounds__(tc::kThreads, 1) dn_apply_tc_kernel(ApplyArgs a, int* status) {
+  extern __shared__ __align__(128) unsigned char sm[];
+  const uint32_t sb = (uint32_t)__cvta_generic_to_shared(sm);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t quarter = warp & 3;          // TMEM lanes 32 quarter .. + 31
+  const uint32_t cols = 16 * (warp >> 2);     // this warp's accumulator columns in an epilogue
+  const uint32_t row = 32 * quarter + lane;   // tile row = TMEM lane of this thread
+  // weights into the core-matrix layout (16-byte chunks of 8 elements)
+  for (uint32_t i = threadIdx.x; i < 64 * 32; i += tc::kThreads) {
+    const uint32_t n = i / 32, kg = i % 32;
+    *(uint4*)(sm + tc::kW1 + tc::core_off(n, 8 * kg, 256)) = __ldg((const uint4*)a.wt.w1 + n * 32 + kg);
+  }
+  for (uint32_t i = threadIdx.x; i < 64 * 8; i += tc::kThreads) {
+    const uint32_t n = i / 8, kg = i % 8;
+    *(uint4*)(sm + tc::kW2 + tc::core_off(n, 8 * kg, 64)) = __ldg((const uint4*)a.wt.w2 + n * 8 + kg);
+  }
+  for (uint32_t i = threadIdx.x; i < 16 * 8; i += tc::kThreads) {
+    const uint32_t n = i / 8, kg = i % 8;
+    *(uint4*)(sm + tc::kW3 + tc::core_off(n, 8 * kg, 64)) =
+        n < 8 ? __ldg((const uint4*)a.wt.w3 + n * 8 + kg) : make_uint4(0, 0, 0, 0);
+  }
+  const uint32_t bar = sb + tc::kBar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(sb + tc::kSlot),
+                 "r"(tc::kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc::fence_proxy();
+  tc::sync_all();
+  const uint32_t tmem = *(volatile uint32_t*)(sm + tc::kSlot);
+  const uint32_t my_lanes = tmem + ((32 * quarter) << 16);  // this warp's 32 TMEM lanes
+  const uint64_t dA1 = tc::smem_desc(sb + tc::kA1, 128, 4096), dW1 = tc::smem_desc(sb + tc::kW1, 128, 4096);
+  const uint64_t dA2 = tc::smem_desc(sb + tc::kA2, 128, 1024), dA3 = tc::smem_desc(sb + tc::kA3, 128, 1024);
+  const uint64_t dW2 = tc::smem_desc(sb + tc::kW2, 128, 1024), dW3 = tc::smem_desc(sb + tc::kW3, 128, 1024);
+  // a descriptor's start address advances 256 bytes (16 elements of K) per MMA: 16 in 16-byte units
+  const uint32_t end = a.offset + a.count;
+  const uint32_t tiles = (a.count + dn::kRows - 1) / dn::kRows;
+  uint32_t parity = 0;
+  bool failed = false;  // a bounded wait ran out (agreed by all threads)
+  for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    const uint32_t first = a.offset + tile * dn::kRows;
+    // input rows: warp w assembles rows 8w .. 8w + 7
+    for (int rr = 0; rr < 8; ++rr) {
+      const uint32_t r = (uint32_t)(warp * 8 + rr), i = first + r;
+      if (a.rows) {
+        const uint4 v = i < end ? __ldg((const uint4*)(a.rows + (size_t)i * (dn::kK1 / 2)) + lane)
+                                : make_uint4(0, 0, 0, 0);
+        *(uint4*)(sm + tc::kA1 + tc::core_off(r, 8 * lane, 256)) = v;
+      } else {
+        uint32_t px = i < end ? __ldg(a.indices + i) : kNoTexel;
+        if (px >= a.w * a.h) px = kNoTexel;
+        if (lane < 25) {
+          float v[10];
+          neighbour_features(a.f0, a.f1, a.f2, a.w, a.h, px, lane, v);
+#pragma unroll
+          for (int k = 0; k < 5; ++k)
+            *(uint32_t*)(sm + tc::kA1 + tc::core_off(r, 10 * lane + 2 * k, 256)) = pack2(v[2 * k], v[2 * k + 1]);
+        } else if (lane == 25) {
+          for (int k = 250; k < 256; k += 2) *(uint32_t*)(sm + tc::kA1 + tc::core_off(r, k, 256)) = 0u;
+        }
+      }
+    }
+    tc::fence_proxy();
+    tc::sync_all();
+    // layer 1: D[:, 0..63] = X W1^T over K = 256
+    if (threadIdx.x == 0) {
+      for (uint32_t s = 0; s < 16; ++s) tc::mma(tmem, dA1 + 16 * s, dW1 + 16 * s, tc::instr_desc(64), s > 0);
+      tc::commit(bar);
+    }
+    parity ^= 1;
+    if (!__syncthreads_and(tc::wait(bar, parity ^ 1))) {
+      failed = true;
+      break;
+    }
+    tc::fence_after();
+    tc::hidden_epilogue(my_lanes, cols, a.wt.params + dn::kB1, sm + tc::kA2, row);
+    tc::fence_proxy();
+    tc::sync_all();
+    // layer 2: D[:, 64..127] = A1 W2^T over K = 64
+    if (threadIdx.x == 0) {
+      for (uint32_t s = 0; s < 4; ++s) tc::mma(tmem + 64, dA2 + 16 * s, dW2 + 16 * s, tc::instr_desc(64), s > 0);
+      tc::commit(bar);
+    }
+    parity ^= 1;
+    if (!__syncthreads_and(tc::wait(bar, parity ^ 1))) {
+      failed = true;
+      break;
+    }
+    tc::fence_after();
+    tc::hidden_epilogue(my_lanes + 64, cols, a.wt.params + dn::kB2, sm + tc::kA3, row);
+    tc::fence_proxy();
+    tc::sync_all();
+    // layer 3: D[:, 0..15] = A2 W3^T over K = 64 (outputs 4..15 are zero rows of W3)
+    if (threadIdx.x == 0) {
+      for (uint32_t s = 0; s < 4; ++s) tc::mma(tmem, dA3 + 16 * s, dW3 + 16 * s, tc::instr_desc(16), s > 0);
+      tc::commit(bar);
+    }
+    parity ^= 1;
+    if (!__syncthreads_and(tc::wait(bar, parity ^ 1))) {
+      failed = true;
+      break;
+    }
+    tc::fence_after();
+    float y[16];
+    if (cols == 0) tc::ld16(my_lanes, y);  // the output columns: one warp per lane quarter
+    const uint32_t i = first + row;
+    if (cols == 0 && i < end) {
+      const float o0 = y[0] + __ldg(a.wt.params + dn::kB3), o1 = y[1] + __ldg(a.wt.params + dn::kB3 + 1);
+      const float o2 = y[2] + __ldg(a.wt.params + dn::kB3 + 2), o3 = y[3] + __ldg(a.wt.params + dn::kB3 + 3);
+      if (!a.ao_out) {
+        a.y_out[i] = make_float4(o0, o1, o2, o3);
+      } else {
+        float ao = 1.0f, bx = 0.0f, by = 0.0f, bz = 0.0f;
+        if (__ldg(a.tidx + i) != kMiss) {
+          float cx = __ldg(a.bn_in + 3 * (size_t)i), cy = __ldg(a.bn_in + 3 * (size_t)i + 1),
+                cz = __ldg(a.bn_in + 3 * (size_t)i + 2);
+          if (!isfinite(cx) || !isfinite(cy) || !isfinite(cz)) cx = cy = cz = 0.0f;
+          ao = fminf(fmaxf(__ldg(a.ao_in + i) + o0, 0.0f), 1.0f);
+          const float vx = cx + o1, vy = cy + o2, vz = cz + o3;
+          const float d = (vx * vx + vy * vy) + vz * vz;
+          if (d > 0.0f) {
+            const float inv = 1.0f / sqrtf(d);
+            bx = vx * inv;
+            by = vy * inv;
+            bz = vz * inv;
+          }
+        }
+        a.ao_out[i] = ao;
+        a.bn_out[3 * (size_t)i] = bx;
+        a.bn_out[3 * (size_t)i + 1] = by;
+        a.bn_out[3 * (size_t)i + 2] = bz;
+      }
+    }
+    tc::sync_all();  // the next tile overwrites the operand tiles and the accumulators
+  }
+  if (failed) {
+    if (threadIdx.x == 0) atomicOr(status, 16);
+    // let the committed group that timed out drain before the memory is freed
+    tc::wait(bar, parity ^ 1);
+  }
+  tc::sync_all();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(tc::kTmemCols) : "memory");
+}
+
 // ------------------------------------------------------------------ per-tile verification
 __global__ void dn_inverse_kernel(uint32_t n, const uint32_t* __restrict__ indices, uint32_t pixels, uint32_t* inv) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -868,6 +1143,37 @@ cudaError_t launch_apply(cudaStream_t st, int sm_count, const float4* image, uin
   const uint32_t tiles = (count + kRows - 1) / kRows;
   const uint32_t blocks = std::min<uint32_t>(tiles, (uint32_t)sm_count * 2);
   dn_apply_kernel<<<blocks, 256, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_apply_tc(cudaStream_t st, int sm_count, const float4* image, uint32_t w, uint32_t h,
+                            const uint32_t* indices, const uint32_t* tidx, const float* ao_in, const float* bn_in,
+                            uint32_t offset, uint32_t count, const DnWeights& wt, float* ao_out, float* bn_out,
+                            const uint32_t* rows, float4* y_out, int* status) {
+  cudaError_t e = cudaFuncSetAttribute(dn_apply_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::kBytes);
+  if (e != cudaSuccess) return e;
+  if (count == 0) return cudaSuccess;
+  ApplyArgs a;
+  const size_t px = (size_t)w * h;
+  a.f0 = image;
+  a.f1 = image ? image + px : nullptr;
+  a.f2 = image ? image + 2 * px : nullptr;
+  a.w = w;
+  a.h = h;
+  a.indices = indices;
+  a.tidx = tidx;
+  a.ao_in = ao_in;
+  a.bn_in = bn_in;
+  a.offset = offset;
+  a.count = count;
+  a.wt = wt;
+  a.ao_out = ao_out;
+  a.bn_out = bn_out;
+  a.y_out = y_out;
+  a.rows = rows;
+  const uint32_t tiles = (count + kRows - 1) / kRows;
+  const uint32_t blocks = std::min<uint32_t>(tiles, (uint32_t)sm_count);  // one CTA per SM (141 KB of shared memory)
+  dn_apply_tc_kernel<<<blocks, tc::kThreads, tc::kBytes, st>>>(a, status);
   return cudaGetLastError();
 }
 

@@ -24,6 +24,7 @@ struct fk_denoiser {
   float* loss = nullptr;    // per-tile squared-error sums of the last step
   uint32_t tile_capacity = 0, last_tiles = 0, last_batch = 0;
   uint32_t step = 0;
+  int engine = FK_DN_ENGINE_TCGEN05;  // inference kernel
   // denoised-bake scratch
   void* scratch[6] = {};
   size_t scratch_bytes[6] = {};
@@ -39,6 +40,19 @@ int launched(fk_ctx* ctx, cudaError_t e, const char* what, int kernels = 1) {
   if (e != cudaSuccess) return fk_cuda_fail(ctx, e, what);
   ctx->launches += kernels;
   return FK_OK;
+}
+
+// Inference through the denoiser's engine (the two kernels compute the same
+// network; see fk_denoiser_set_engine).
+cudaError_t apply(const fk_denoiser* d, const float4* image, uint32_t w, uint32_t h, const uint32_t* indices,
+                  const uint32_t* tidx, const float* ao_in, const float* bn_in, uint32_t offset, uint32_t count,
+                  float* ao_out, float* bn_out, const uint32_t* rows, float4* y_out) {
+  fk_ctx* ctx = d->ctx;
+  if (d->engine == FK_DN_ENGINE_TCGEN05)
+    return dn::launch_apply_tc(ctx->stream, ctx->sm_count, image, w, h, indices, tidx, ao_in, bn_in, offset, count,
+                               weights(d), ao_out, bn_out, rows, y_out, ctx->status);
+  return dn::launch_apply(ctx->stream, ctx->sm_count, image, w, h, indices, tidx, ao_in, bn_in, offset, count,
+                          weights(d), ao_out, bn_out, rows, y_out);
 }
 
 int ensure_tiles(fk_denoiser* d, uint32_t tiles) {
@@ -183,6 +197,14 @@ int fk_denoiser_set_params(fk_denoiser* d, const float* params, uint32_t count) 
   return FK_OK;
 }
 
+int fk_denoiser_set_engine(fk_denoiser* d, int engine) {
+  if (!d) return FK_ERR_INVALID;
+  if (engine != FK_DN_ENGINE_MMA_SYNC && engine != FK_DN_ENGINE_TCGEN05)
+    return fk_fail(d->ctx, FK_ERR_INVALID, "fk_denoiser_set_engine: unknown engine");
+  d->engine = engine;
+  return FK_OK;
+}
+
 int fk_denoiser_get_params(fk_denoiser* d, float* params, uint32_t count) {
   if (!d || !params) return FK_ERR_INVALID;
   fk_ctx* ctx = d->ctx;
@@ -257,8 +279,8 @@ int fk_denoiser_forward(fk_denoiser* d, const fk_buf* rows, uint32_t count, fk_b
   if (!fits(rows, (uint64_t)count * FK_DN_ROW_BYTES) || !fits(y4, 16ull * count))
     return fk_fail(ctx, FK_ERR_INVALID, "fk_denoiser_forward: buffers too small");
   return launched(ctx,
-                  dn::launch_apply(ctx->stream, ctx->sm_count, nullptr, 0, 0, nullptr, nullptr, nullptr, nullptr, 0,
-                                   count, weights(d), nullptr, nullptr, (const uint32_t*)rows->ptr,
+                  apply(d, nullptr, 0, 0, nullptr, nullptr, nullptr, nullptr, 0,
+                                   count, nullptr, nullptr, (const uint32_t*)rows->ptr,
                                    (float4*)y4->ptr),
                   "dn_apply_kernel", count ? 1 : 0);
 }
@@ -274,9 +296,9 @@ int fk_denoise_apply(fk_denoiser* d, const fk_texel_map* map, const fk_buf* imag
       !fits(bn_in, 12 * n) || !fits(ao_out, 4 * n) || !fits(bn_out, 12 * n))
     return fk_fail(ctx, FK_ERR_INVALID, "fk_denoise_apply: buffers smaller than the map");
   return launched(ctx,
-                  dn::launch_apply(ctx->stream, ctx->sm_count, (const float4*)image->ptr, map->width, map->height,
+                  apply(d, (const float4*)image->ptr, map->width, map->height,
                                    map->indices, (const uint32_t*)tidx->ptr, (const float*)ao_in->ptr,
-                                   (const float*)bn_in->ptr, offset, count, weights(d), (float*)ao_out->ptr,
+                                   (const float*)bn_in->ptr, offset, count, (float*)ao_out->ptr,
                                    (float*)bn_out->ptr, nullptr, nullptr),
                   "dn_apply_kernel", count ? 1 : 0);
 }
@@ -348,8 +370,8 @@ int fk_denoise_bake(fk_denoiser* d, const fk_scene* scene, const fk_texel_map* m
                 "dn_features_kernel", 2);
   if (rc == FK_OK)
     rc = launched(ctx,
-                  dn::launch_apply(ctx->stream, ctx->sm_count, image, w, h, map->indices, ti, ao, bn, 0, n,
-                                   weights(d), ao, bn, nullptr, nullptr),
+                  apply(d, image, w, h, map->indices, ti, ao, bn, 0, n,
+                                   ao, bn, nullptr, nullptr),
                   "dn_apply_kernel");
   if (rc != FK_OK) return rc;
   // 3. spot checks at full sample count (into the position / normal scratch)

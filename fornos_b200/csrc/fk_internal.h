@@ -220,6 +220,11 @@ cudaError_t launch_apply(cudaStream_t st, int sm_count, const float4* image, uin
                          const uint32_t* indices, const uint32_t* tidx, const float* ao_in, const float* bn_in,
                          uint32_t offset, uint32_t count, const DnWeights& wt, float* ao_out, float* bn_out,
                          const uint32_t* rows, float4* y_out);
+// The same inference on tcgen05 / tensor memory (status bit 16: a bounded wait ran out).
+cudaError_t launch_apply_tc(cudaStream_t st, int sm_count, const float4* image, uint32_t w, uint32_t h,
+                            const uint32_t* indices, const uint32_t* tidx, const float* ao_in, const float* bn_in,
+                            uint32_t offset, uint32_t count, const DnWeights& wt, float* ao_out, float* bn_out,
+                            const uint32_t* rows, float4* y_out, int* status);
 cudaError_t launch_inverse(cudaStream_t st, uint32_t n, const uint32_t* indices, uint32_t pixels, uint32_t* inv);
 cudaError_t launch_verify_slots(cudaStream_t st, uint32_t w, uint32_t h, uint32_t tile, uint32_t cells,
                                 const uint32_t* inv, const uint32_t* tidx, uint32_t* slots);

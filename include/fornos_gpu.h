@@ -473,6 +473,14 @@ typedef struct fk_denoiser fk_denoiser;
 
 int fk_denoiser_create(fk_ctx* ctx, fk_denoiser** out);
 int fk_denoiser_free(fk_denoiser* d);
+/* Inference kernel: FK_DN_ENGINE_TCGEN05 (the default; tcgen05.mma with
+ * accumulators in tensor memory, sm_100a) or FK_DN_ENGINE_MMA_SYNC
+ * (mma.sync.m16n8k16); both compute the same network in BF16 with FP32
+ * accumulation, differing only in accumulation order.  Training always runs
+ * the mma.sync kernels. */
+#define FK_DN_ENGINE_MMA_SYNC 0
+#define FK_DN_ENGINE_TCGEN05 1
+int fk_denoiser_set_engine(fk_denoiser* d, int engine);
 /* Host fp32 parameters in the layout above (count = FK_DN_PARAMS); setting
  * them zeroes W1's padding columns and resets the optimiser state. */
 int fk_denoiser_set_params(fk_denoiser* d, const float* params, uint32_t count);
