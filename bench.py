@@ -192,6 +192,8 @@ def run_fornos(args, wl, rank, world):
     raster_ms = e0.elapsed_time(e1)
     n = tmap.count
     scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
+    if args.tree == "reference":
+        scene.set_tree(api.TREE_REFERENCE)
     info = scene.info()
     samples = api.samples_cosine(spp, api.PERMS, args.seed)
     sbuf = ctx.upload(samples)
@@ -320,7 +322,7 @@ def run_fornos(args, wl, rank, world):
         "dtype": "f32", "data": "synthetic (seeded generated meshes; no public dataset)",
         "config": {"workload": args.workload, "desc": wl["desc"], "texels": n, "texture": tex, "spp": spp,
                    "high_poly_triangles": prep.triangles, "bvh_nodes": info["node_count"],
-                   "bvh_depth": info["depth"], "traverse": args.traverse, "schedule": args.schedule,
+                   "bvh_depth": info["depth"], "traverse": args.traverse, "schedule": args.schedule, "tree": args.tree,
                    "rays_per_texel": rays_per_texel(wl),
                    "rays_counted": "2 mapping + spp each for AO, bent normals, thickness (AO and bent normals "
                                    "share one traversal)",
@@ -689,6 +691,9 @@ def main():
     ap.add_argument("--batch-jobs", type=int, default=64)
     ap.add_argument("--traverse", default="auto", choices=list(TRAVERSE))
     ap.add_argument("--schedule", default="auto", choices=list(SCHEDULE))
+    ap.add_argument("--tree", default="sah", choices=["reference", "sah"],
+                    help="inner tree of the ordered traversals: rebuilt over the reference's leaves (sah) or the "
+                         "reference's own")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")

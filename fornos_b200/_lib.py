@@ -119,6 +119,7 @@ _SIGS = {
     "fk_scene_upload": (c_int, [c_vp, c_vp, c_u32, f32p, f32p, c_u32, ctypes.POINTER(c_vp)]),
     "fk_scene_free": (c_int, [c_vp, c_vp]),
     "fk_scene_get_info": (c_int, [c_vp, ctypes.POINTER(SceneInfo)]),
+    "fk_scene_set_tree": (c_int, [c_vp, c_int]),
     "fk_raster_uv": (c_int, [c_vp, c_vp, c_vp, c_u32, c_u32, c_int, c_float, ctypes.POINTER(c_vp)]),
     "fk_texel_map_from_host": (c_int, [c_vp, c_u32, c_u32, c_u32, f32p, f32p, u32p, ctypes.POINTER(c_vp)]),
     "fk_texel_map_info": (c_int, [c_vp, u32p, u32p, u32p]),

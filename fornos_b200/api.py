@@ -19,6 +19,7 @@ MISS = 0xFFFFFFFF
 # kinds (include/fornos_gpu.h)
 AO, BN, THICK, AO_BN = 0, 1, 2, 3
 TRAVERSE_AUTO, TRAVERSE_ORDERED, TRAVERSE_SKIP, TRAVERSE_ORDERED4 = 0, 1, 2, 3
+TREE_REFERENCE, TREE_SAH = 0, 1
 SCHEDULE_STATIC, SCHEDULE_DYNAMIC = 0x10, 0x20  # or-ed into `traverse`
 EXACT_BOX_TESTS = 0x100  # or-ed into `traverse`: divide in every box test
 GATHER_HEIGHT, GATHER_POSITION, GATHER_NORMAL = 0, 1, 2
@@ -269,6 +270,10 @@ class Scene:
         i = L.SceneInfo()
         _check(self.ctx.lib.fk_scene_get_info(self.handle, ctypes.byref(i)))
         return {k: getattr(i, k) for k, _ in L.SceneInfo._fields_}
+
+    def set_tree(self, tree):
+        """Inner tree of the ordered traversals: TREE_REFERENCE or TREE_SAH."""
+        _check(self.ctx.lib.fk_scene_set_tree(self.handle, tree), self.ctx, "fk_scene_set_tree")
 
     def free(self):
         if self.owned and self.handle and self.ctx.handle:

@@ -144,6 +144,9 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
       return fk_fail(ctx, FK_ERR_INVALID, who + " has a buffer too small for its texels");
     if ((unsigned long long)J.params.sample_count > kMaxChunkRays)
       return fk_fail(ctx, FK_ERR_INVALID, who + " has too many samples per texel");
+    // the tuner may pick the 4-wide traversal: its layout must exist before the table is copied
+    const int rc = fk::ensure_wide4(ctx, const_cast<fk_scene*>(J.scene));
+    if (rc != FK_OK) return rc;
     fk::BatchJobDev& d = table[i];
     std::memset(&d, 0, sizeof(d));
     d.s = fk::scene_dev(J.scene);
@@ -207,7 +210,7 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   }
   // default schedule: ordered when every scene's tree is shallow enough
   for (uint32_t i = 0; i < njobs; ++i) {
-    if (jobs[i].scene->depth > 48) b->ordered_ok = false;
+    if (jobs[i].scene->odepth > fk::kMaxOrderedDepth) b->ordered_ok = false;
     if (jobs[i].scene->depth4 > fk::kMaxOrdered4Depth) b->ordered4_ok = false;
   }
   b->traverse = b->ordered_ok ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;

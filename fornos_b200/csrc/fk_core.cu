@@ -59,6 +59,39 @@ void* fk_scratch(fk_ctx* ctx, size_t bytes) {
   return ctx->scratch;
 }
 
+namespace fk {
+// Builds the collapsed 4-wide layout of the scene's active inner tree on first
+// use (from the 2-wide records on the device) and points the scene at it.
+int ensure_wide4(fk_ctx* ctx, fk_scene* s) {
+  const int t = s->tree;
+  if (!s->tree_wide4[t] && s->tree_wide[t] && s->tree_count[t] > 0) {
+    std::vector<float4> wide(4 * (size_t)s->tree_count[t]), wide4;
+    FK_CUDA(ctx, cudaMemcpyAsync(wide.data(), s->tree_wide[t], sizeof(float4) * wide.size(), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    uint32_t n4 = 0, d4 = 0;
+    collapse_wide4(wide, wide4, n4, d4);
+    float4* dw4 = nullptr;
+    int rc = fk_dev_alloc(ctx, (void**)&dw4, sizeof(float4) * wide4.size());
+    if (rc != FK_OK) return rc;
+    if (cudaMemcpyAsync(dw4, wide4.data(), sizeof(float4) * wide4.size(), cudaMemcpyHostToDevice, ctx->stream) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+      fk_dev_free(dw4);
+      return fk_fail(ctx, FK_ERR_CUDA, "4-wide layout upload");
+    }
+    s->tree_wide4[t] = dw4;
+    s->tree_count4[t] = n4;
+    s->tree_depth4[t] = d4;
+    s->bytes += sizeof(float4) * wide4.size();
+  }
+  s->wide4 = s->tree_wide4[t];
+  s->wide4_count = s->tree_count4[t];
+  s->depth4 = s->tree_depth4[t];
+  return FK_OK;
+}
+}  // namespace fk
+
 extern "C" {
 
 int fk_ctx_create(int device, fk_ctx** out) {
@@ -257,77 +290,15 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     std::memcpy(f, ints, 16);
     w[3] = make_float4(f[0], f[1], f[2], f[3]);
   }
-  // Collapsed 4-wide layout: the record at the root and every record two
-  // levels below a 4-wide node become 4-wide nodes whose children are the
-  // record's children, each inner child replaced by its own two children.
-  // Leaves and their boxes are those of the 2-wide records, bit for bit.
-  // 128 bytes per node: lo.x, hi.x, lo.y, hi.y, lo.z, hi.z of children 0..3,
-  // their refs (4-wide node index, or -(flattened leaf index + 1)), and the
-  // child count; unused slots repeat child 0 and are masked by the count.
-  std::vector<float4> wide4;
-  uint32_t n4 = 0, depth4 = 0;
+  // Collapsed 4-wide layout over the same records (fk_tree.cpp).
+  // The inner tree the ordered traversals walk by default: rebuilt over the
+  // same leaves with a surface-area split on all three face pairs (fk_tree.cpp);
+  // the reference's records above stay available (fk_scene_set_tree).
+  std::vector<float4> swide;
+  uint32_t sdepth = 0;
   if (nw > 0) {
-    struct Ent {
-      float lo[3], hi[3];
-      int32_t ref;
-    };
-    auto child = [&](uint32_t r, int k) {
-      const float4* w = &wide[4 * (size_t)r];
-      Ent e;
-      if (k == 0) {
-        e = {{w[0].x, w[0].z, w[2].x}, {w[0].y, w[0].w, w[2].y}, 0};
-        std::memcpy(&e.ref, &w[3].x, 4);
-      } else {
-        e = {{w[1].x, w[1].z, w[2].z}, {w[1].y, w[1].w, w[2].w}, 0};
-        std::memcpy(&e.ref, &w[3].y, 4);
-      }
-      return e;
-    };
-    std::vector<uint32_t> list{0};  // 2-wide records that become 4-wide nodes
-    std::vector<uint32_t> lvl{1};
-    std::vector<std::array<Ent, 4>> kids;
-    std::vector<int> counts;
-    for (size_t q = 0; q < list.size(); ++q) {
-      std::array<Ent, 4> e{};
-      int m = 0;
-      for (int k = 0; k < 2; ++k) {
-        Ent c = child(list[q], k);
-        if (c.ref >= 0) {
-          e[m++] = child((uint32_t)c.ref, 0);
-          e[m++] = child((uint32_t)c.ref, 1);
-        } else {
-          e[m++] = c;
-        }
-      }
-      for (int k = 0; k < m; ++k)
-        if (e[k].ref >= 0) {
-          const uint32_t r = (uint32_t)e[k].ref;
-          e[k].ref = (int32_t)list.size();
-          list.push_back(r);
-          lvl.push_back(lvl[q] + 1);
-        }
-      for (int k = m; k < 4; ++k) e[k] = e[0];
-      kids.push_back(e);
-      counts.push_back(m);
-      depth4 = std::max(depth4, lvl[q]);
-    }
-    n4 = (uint32_t)list.size();
-    wide4.resize(8 * (size_t)n4);
-    for (uint32_t k = 0; k < n4; ++k) {
-      float4* w = &wide4[8 * (size_t)k];
-      const auto& e = kids[k];
-      for (int a = 0; a < 3; ++a) {
-        w[2 * a] = make_float4(e[0].lo[a], e[1].lo[a], e[2].lo[a], e[3].lo[a]);
-        w[2 * a + 1] = make_float4(e[0].hi[a], e[1].hi[a], e[2].hi[a], e[3].hi[a]);
-      }
-      float f[4];
-      int32_t ints[4] = {e[0].ref, e[1].ref, e[2].ref, e[3].ref};
-      std::memcpy(f, ints, 16);
-      w[6] = make_float4(f[0], f[1], f[2], f[3]);
-      int32_t cnt[4] = {counts[k], 0, 0, 0};
-      std::memcpy(f, cnt, 16);
-      w[7] = make_float4(f[0], f[1], f[2], f[3]);
-    }
+    sdepth = fk::build_sah_wide(lo.data(), hi.data(), jump.data(), nn, swide);
+    if (sdepth > fk::kMaxOrderedDepth) swide.clear();
   }
   fk_scene* s = new (std::nothrow) fk_scene();
   if (!s) return FK_ERR_NOMEM;
@@ -335,10 +306,11 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   s->node_count = nn;
   s->corner_count = nc;
   s->depth = maxd;
+  s->odepth = maxd;
   s->leaf_count = leaves;
   s->wide_count = nw;
-  s->wide4_count = n4;
-  s->depth4 = depth4;
+  s->wide4_count = 0;  // the 4-wide layout is built on first use (fk::ensure_wide4)
+  s->depth4 = 0;
   s->root_is_leaf = nodes[0].jump == 1;
   // The filtered box test assumes |box - origin| < 2^26; ray origins lie on
   // the scene's triangles, so box and corner coordinates below 2^24 suffice.
@@ -369,7 +341,14 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   up((void**)&s->pos4, pos4, cb);
   up((void**)&s->nrm4, nrm4, cb);
   up((void**)&s->wide, wide.data(), sizeof(float4) * wide.size());
-  up((void**)&s->wide4, wide4.data(), sizeof(float4) * wide4.size());
+  s->tree_wide[FK_TREE_REFERENCE] = s->wide;
+  s->tree_count[FK_TREE_REFERENCE] = nw;
+  s->tree_depth[FK_TREE_REFERENCE] = maxd;
+  if (!swide.empty()) {
+    up((void**)&s->tree_wide[FK_TREE_SAH], swide.data(), sizeof(float4) * swide.size());
+    s->tree_count[FK_TREE_SAH] = (uint32_t)(swide.size() / 4);
+    s->tree_depth[FK_TREE_SAH] = sdepth;
+  }
   if (rc == FK_OK) {
     rc = fk_dev_alloc(ctx, (void**)&s->tri_rec, 4 * sizeof(float4) * (size_t)(nc / 3));
     s->bytes += 4 * sizeof(float4) * (size_t)(nc / 3);
@@ -385,6 +364,13 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     return rc;
   }
   ctx->scenes.insert(s);
+  if (s->tree_wide[FK_TREE_SAH]) {
+    rc = fk_scene_set_tree(s, FK_TREE_SAH);
+    if (rc != FK_OK) {
+      fk_scene_free(ctx, s);
+      return rc;
+    }
+  }
   *out = s;
   return FK_OK;
 }
@@ -392,10 +378,30 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
 int fk_scene_free(fk_ctx* ctx, fk_scene* s) {
   if (!ctx || !s || !ctx->scenes.count(s)) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_free: unknown scene");
   cudaStreamSynchronize(ctx->stream);
-  void* ps[] = {s->node_lo, s->node_hi, s->node_jump, s->pos4, s->nrm4, s->wide, s->wide4, s->tri_rec};
+  void* ps[] = {s->node_lo,      s->node_hi,      s->node_jump,     s->pos4,          s->nrm4,
+                s->tree_wide[0], s->tree_wide[1], s->tree_wide4[0], s->tree_wide4[1], s->tri_rec};
   for (void* p : ps) fk_dev_free(p);
   ctx->scenes.erase(s);
   delete s;
+  return FK_OK;
+}
+
+int fk_scene_set_tree(fk_scene* s, int tree) {
+  if (!s) return FK_ERR_INVALID;
+  fk_ctx* ctx = s->ctx;
+  if (tree != FK_TREE_REFERENCE && tree != FK_TREE_SAH)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_set_tree: unknown tree");
+  if (tree == FK_TREE_SAH && !s->tree_wide[FK_TREE_SAH] && !s->root_is_leaf)
+    return fk_fail(ctx, FK_ERR_UNSUPPORTED, "fk_scene_set_tree: the rebuilt tree is deeper than the ordered traversal's 48");
+  if (s->root_is_leaf) tree = FK_TREE_REFERENCE;  // a single leaf has no inner tree to rebuild
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // work queued on the previous tree is done
+  s->tree = tree;
+  s->wide = s->tree_wide[tree];
+  s->wide4 = s->tree_wide4[tree];
+  s->wide_count = s->tree_count[tree];
+  s->wide4_count = s->tree_count4[tree];
+  s->odepth = s->tree_depth[tree];
+  s->depth4 = s->tree_depth4[tree];
   return FK_OK;
 }
 

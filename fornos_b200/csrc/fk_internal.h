@@ -52,6 +52,13 @@ struct fk_scene {
   // boxes (4 x float4), and one 64-byte precomputed record per triangle.
   float4* wide = nullptr;
   uint32_t wide_count = 0;
+  uint32_t odepth = 0;           // levels of the ordered layouts' tree (the reference's, or a rebuilt one)
+  int tree = 0;                  // FK_TREE_*: which inner tree wide / wide4 point into
+  // Both inner trees' arrays once built, kept until the scene is freed (a
+  // batch's job table may hold either): [FK_TREE_REFERENCE], [FK_TREE_SAH].
+  float4* tree_wide[2] = {nullptr, nullptr};
+  float4* tree_wide4[2] = {nullptr, nullptr};
+  uint32_t tree_count[2] = {0, 0}, tree_count4[2] = {0, 0}, tree_depth[2] = {0, 0}, tree_depth4[2] = {0, 0};
   // Collapsed layout: 128-byte 4-wide nodes over the same leaves.
   float4* wide4 = nullptr;
   uint32_t wide4_count = 0, depth4 = 0;
@@ -116,6 +123,19 @@ SceneDev scene_dev(const fk_scene* s);
 // Deepest collapsed (4-wide) tree the 4-wide traversal accepts: it defers at
 // most 3 entries per level within its 64-entry stack.
 constexpr uint32_t kMaxOrdered4Depth = 21;
+// Deepest 2-wide tree the ordered traversal accepts.
+constexpr uint32_t kMaxOrderedDepth = 48;
+
+// Inner-tree layouts (fk_tree.cpp).  2-wide records: 4 float4 per inner node,
+// child boxes, refs (record index, or -(flattened leaf index + 1)) and leaf
+// triangle counts; root record 0.  build_sah_wide rebuilds them over the
+// leaves of a flattened node array with a binned surface-area split and
+// returns the tree's depth (root = 1, counting the leaf level).
+uint32_t build_sah_wide(const float4* lo, const float4* hi, const uint32_t* jump, uint32_t nn,
+                        std::vector<float4>& wide);
+void collapse_wide4(const std::vector<float4>& wide, std::vector<float4>& wide4, uint32_t& n4, uint32_t& depth4);
+// The scene's 4-wide layout for its active tree, built on first use.
+int ensure_wide4(fk_ctx* ctx, fk_scene* s);
 
 // One job of a batched hemisphere launch (device-side job table entry).
 static constexpr uint32_t kMaxBatchJobs = 64;

@@ -138,7 +138,7 @@ __device__ float trace_skip(const SceneDev& s, f3 o, f3 d, float lo, float hi, T
 }
 
 static constexpr int kStack = 64;
-static constexpr uint32_t kMaxOrderedDepth = 48;  // deeper trees use the skip walk
+static_assert(kMaxOrderedDepth < kStack, "the ordered traversal defers at most one entry per level");
 // The 4-wide traversal defers at most 3 entries per level.
 static_assert(kMaxOrdered4Depth == (kStack - 1) / 3, "4-wide depth limit follows the stack size");
 __host__ __device__ constexpr bool is_ordered(int trav) {
@@ -371,6 +371,11 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
                             uint32_t speculate);
 
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
+  if ((h.traverse & FK_TRAVERSE_MASK) == FK_TRAVERSE_ORDERED4) {
+    // the scene's 4-wide layout is built on first use; the scene is otherwise unchanged
+    const int rc = ensure_wide4(ctx, const_cast<fk_scene*>(s));
+    if (rc != FK_OK) return rc;
+  }
   HemiArgs a;
   a.s = dev_of(s);
   a.samples = h.samples;
@@ -393,8 +398,8 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   a.texel_limit = h.texel_limit;
   int trav = h.traverse & FK_TRAVERSE_MASK;
   int sched = h.traverse & FK_SCHEDULE_MASK;
-  if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
-  if (trav == FK_TRAVERSE_ORDERED && s->depth > kMaxOrderedDepth)
+  if (trav == FK_TRAVERSE_AUTO) trav = s->odepth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
+  if (trav == FK_TRAVERSE_ORDERED && s->odepth > kMaxOrderedDepth)
     return fk_fail(ctx, FK_ERR_INVALID, "ordered traversal needs tree depth <= 48; use FK_TRAVERSE_SKIP");
   if (trav == FK_TRAVERSE_ORDERED4 && s->depth4 > kMaxOrdered4Depth)
     return fk_fail(ctx, FK_ERR_INVALID, "4-wide traversal needs a 4-wide depth <= 21; use FK_TRAVERSE_ORDERED");
@@ -1255,8 +1260,8 @@ int launch_hemisphere_external(const fk_scene* s, const HemiLaunch& h, cudaStrea
   a.ids = nullptr;
   a.texel_limit = 0;
   int trav = h.traverse & FK_TRAVERSE_MASK;
-  if (trav == FK_TRAVERSE_AUTO) trav = s->depth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
-  if (trav == FK_TRAVERSE_ORDERED && s->depth > kMaxOrderedDepth) {
+  if (trav == FK_TRAVERSE_AUTO) trav = s->odepth <= kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
+  if (trav == FK_TRAVERSE_ORDERED && s->odepth > kMaxOrderedDepth) {
     err = "ordered traversal needs tree depth <= 48; use FK_TRAVERSE_SKIP";
     return FK_ERR_INVALID;
   }

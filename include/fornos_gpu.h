@@ -153,6 +153,18 @@ typedef struct fk_scene_info {
   uint64_t device_bytes;
 } fk_scene_info;
 int fk_scene_get_info(const fk_scene* scene, fk_scene_info* out);
+/* No counterpart in the reference.  The inner tree the ordered traversals
+ * (FK_TRAVERSE_ORDERED / ORDERED4) walk: FK_TREE_REFERENCE, the inner nodes of
+ * BVH::createBinary as uploaded (the default), or FK_TREE_SAH, an inner tree
+ * rebuilt over the same leaves with a binned surface-area split on all three
+ * box faces (the reference's split cost, Src/bvh.cpp:63-68, counts x*y twice and
+ * y*z never).  Leaves, leaf boxes and the skip-pointer walk are untouched, and
+ * the outcome is that of any inner tree over these leaves (an inner box only
+ * prunes what its leaves' own tests reject), so results stay within the
+ * ordered traversal's bar.  Both trees stay resident once built. */
+#define FK_TREE_REFERENCE 0
+#define FK_TREE_SAH 1
+int fk_scene_set_tree(fk_scene* scene, int tree);
 
 /* ------------------------------------------------------------ texel map
  * MapUV::fromMesh / fromMeshes / fromMeshes_Hybrid (Src/compute.cpp:352-370)

@@ -175,6 +175,36 @@ def test_hemisphere_ordered4_matches(ctx, oracle, name, kind, exact):
         assert (~np.all(bits(got[2][hit]) == bits(bref[hit]), axis=1)).mean() <= 1e-3
 
 
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("kind", [api.AO, api.BN, api.THICK])
+@pytest.mark.parametrize("trav", [api.TRAVERSE_ORDERED, api.TRAVERSE_ORDERED4, api.TRAVERSE_SKIP])
+@pytest.mark.parametrize("tree", [api.TREE_REFERENCE, api.TREE_SAH])
+def test_either_inner_tree_matches(ctx, oracle, name, kind, trav, tree):
+    """The reference's inner tree or one rebuilt over the same leaves (the
+    default): the ordered traversals meet their bar against the reference
+    order, the skip walk stays bit-exact."""
+    c = case(name)
+    _, _, mm = mapped(ctx, oracle, c)
+    mm.scene.set_tree(tree)
+    try:
+        spp, lo, hi = 32, 0.001, 0.3
+        samples, (out, hits) = run_hemi(ctx, mm, kind, spp, lo, hi, trav | api.SCHEDULE_DYNAMIC)
+        ctx.check()
+    finally:
+        mm.scene.set_tree(api.TREE_SAH)
+    ref, rhits, tidx = oracle_hemi(oracle, c, mm, kind, samples, spp, lo, hi)
+    hit = tidx != api.MISS
+    if trav == api.TRAVERSE_SKIP:
+        assert np.array_equal(hits[hit], rhits[hit]) and same_bits(out[hit], ref[hit])
+        return
+    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
+    assert (hits[hit] != rhits[hit]).mean() <= 1e-3
+    ok = bits(out[hit]) == bits(ref[hit])
+    if kind == api.BN:
+        ok = np.all(ok, axis=1)
+    assert (~ok).mean() <= 1e-3
+
+
 def test_ordered4_needs_the_dynamic_schedule(ctx, oracle):
     _, _, mm = mapped(ctx, oracle, case("sphere"))
     with pytest.raises(api.FornosError):
