@@ -95,6 +95,7 @@ _SIGS = {
     "fk_ctx_set_stream": (c_int, [c_vp, c_vp]),
     "fk_ctx_stream": (c_vp, [c_vp]),
     "fk_sync": (c_int, [c_vp]),
+    "fk_ctx_trim": (c_int, [c_vp]),
     "fk_launch_count": (c_u64, [c_vp]),
     "fk_ctx_set_tuning": (c_int, [c_vp, ctypes.POINTER(Tuning)]),
     "fk_ctx_get_tuning": (c_int, [c_vp, ctypes.POINTER(Tuning)]),
@@ -172,6 +173,8 @@ _SIGS = {
                                          c_u32, c_int, ctypes.POINTER(c_u64)]),
     "fk_diag_traversal_profile": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32,
                                           c_u32, c_int, ctypes.POINTER(c_u64)]),
+    "fk_diag_scene_tree": (c_int, [c_vp, c_vp, c_int, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
+    "fk_diag_sah_host": (c_int, [c_vp, c_u32, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
     "fk_denoiser_create": (c_int, [c_vp, ctypes.POINTER(c_vp)]),
     "fk_denoiser_free": (c_int, [c_vp]),
     "fk_denoiser_set_engine": (c_int, [c_vp, c_int]),

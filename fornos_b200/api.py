@@ -82,6 +82,10 @@ class Context:
     def sync(self):
         _check(self.lib.fk_sync(self.handle), self)
 
+    def trim(self):
+        """Release the context pool's unused device memory (fk_ctx_trim)."""
+        _check(self.lib.fk_ctx_trim(self.handle), self)
+
     def check(self):
         """Waits for the stream; raises FornosError when a kernel flagged an
         error since the last check (fk_ctx_check)."""
@@ -275,6 +279,19 @@ class Scene:
         """Inner tree of the ordered traversals: TREE_REFERENCE or TREE_SAH."""
         _check(self.ctx.lib.fk_scene_set_tree(self.handle, tree), self.ctx, "fk_scene_set_tree")
 
+    def tree(self, tree):
+        """(records, depth) of an inner tree as resident on the device
+        (fk_diag_scene_tree): records is (count, 16) float32, count 0 when that
+        tree was not built."""
+        n, d = L.c_u32(), L.c_u32()
+        _check(self.ctx.lib.fk_diag_scene_tree(self.ctx.handle, self.handle, tree, None, 0, ctypes.byref(n),
+                                               ctypes.byref(d)), self.ctx, "fk_diag_scene_tree")
+        out = np.zeros((n.value, 16), np.float32)
+        if n.value:
+            _check(self.ctx.lib.fk_diag_scene_tree(self.ctx.handle, self.handle, tree, _f32(out), n.value,
+                                                   ctypes.byref(n), ctypes.byref(d)), self.ctx, "fk_diag_scene_tree")
+        return out, d.value
+
     def free(self):
         if self.owned and self.handle and self.ctx.handle:
             self.ctx.lib.fk_scene_free(self.ctx.handle, self.handle)
@@ -345,6 +362,20 @@ class TexelMap:
             self.free()
         except Exception:
             pass
+
+
+def sah_tree_host(nodes):
+    """(records, depth) of the surface-area inner tree computed on the host
+    (fk_diag_sah_host), the records fk_scene_upload builds on the device."""
+    nodes = np.ascontiguousarray(nodes, NODE_DTYPE)
+    lib = L.load()
+    n, d = L.c_u32(), L.c_u32()
+    _check(lib.fk_diag_sah_host(nodes.ctypes.data, len(nodes), None, 0, ctypes.byref(n), ctypes.byref(d)))
+    out = np.zeros((n.value, 16), np.float32)
+    if n.value:
+        _check(lib.fk_diag_sah_host(nodes.ctypes.data, len(nodes), _f32(out), n.value, ctypes.byref(n),
+                                    ctypes.byref(d)))
+    return out, d.value
 
 
 def samples_cosine(spp, perms=PERMS, seed=0):

@@ -163,7 +163,7 @@ static int diag_counts(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, con
   for (int k = 0; k < n; ++k) tests[k] = host[k];
   if (o0) fk_buf_free(ctx, o0);
   if (o1) fk_buf_free(ctx, o1);
-  fk_dev_free(tally);
+  fk_dev_free(ctx, tally);
   return rc;
 }
 

@@ -15,7 +15,7 @@ struct Scoped {
   fk_scene* scene = nullptr;
   fk_texel_map* map = nullptr;
   ~Scoped() {
-    for (fk_buf* b : bufs) fk_buf_free(ctx, b);
+    for (fk_buf* b : bufs) fk_buf_release(ctx, b);  // used on the context's stream only
     if (scene) fk_scene_free(ctx, scene);
     if (map) fk_texel_map_free(ctx, map);
   }

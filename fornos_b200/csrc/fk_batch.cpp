@@ -320,9 +320,9 @@ int fk_batch_free(fk_batch* b) {
   if (!b) return FK_ERR_INVALID;
   if (b->ctx) cudaStreamSynchronize(b->ctx->stream);
   batch_drop_graph(b);
-  fk_dev_free(b->jobs);
-  fk_dev_free(b->queues);
-  fk_dev_free(b->scratch);
+  fk_dev_free(b->ctx, b->jobs);
+  fk_dev_free(b->ctx, b->queues);
+  fk_dev_free(b->ctx, b->scratch);
   delete b;
   return FK_OK;
 }

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "fk_internal.h"
+#include "fk_sah_rules.h"
 
 int fk_fail(fk_ctx* ctx, int code, const std::string& msg) {
   if (ctx) ctx->err = msg;
@@ -31,12 +32,15 @@ int fk_after_launch(fk_ctx* ctx, const char* what) {
 int fk_dev_alloc(fk_ctx* ctx, void** p, size_t bytes) {
   *p = nullptr;
   if (bytes == 0) return FK_OK;
-  FK_CUDA(ctx, cudaMalloc(p, bytes));
+  if (ctx->pool) FK_CUDA(ctx, cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream));
+  else FK_CUDA(ctx, cudaMalloc(p, bytes));
   return FK_OK;
 }
 
-void fk_dev_free(void* p) {
-  if (p) cudaFree(p);
+void fk_dev_free(fk_ctx* ctx, void* p) {
+  if (!p) return;
+  if (ctx->pool) cudaFreeAsync(p, ctx->stream);
+  else cudaFree(p);
 }
 
 uint32_t* fk_take_counter(fk_ctx* ctx) {
@@ -77,7 +81,7 @@ int ensure_wide4(fk_ctx* ctx, fk_scene* s) {
     if (cudaMemcpyAsync(dw4, wide4.data(), sizeof(float4) * wide4.size(), cudaMemcpyHostToDevice, ctx->stream) !=
             cudaSuccess ||
         cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
-      fk_dev_free(dw4);
+      fk_dev_free(ctx, dw4);
       return fk_fail(ctx, FK_ERR_CUDA, "4-wide layout upload");
     }
     s->tree_wide4[t] = dw4;
@@ -122,6 +126,17 @@ int fk_ctx_create(int device, fk_ctx** out) {
   }
   cudaMemset(c->counters, 0, c->counter_slots * sizeof(uint32_t));
   cudaMemset(c->status, 0, sizeof(int));
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  if (cudaMemPoolCreate(&c->pool, &props) == cudaSuccess) {
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  } else {
+    c->pool = nullptr;  // plain cudaMalloc / cudaFree
+    cudaGetLastError();
+  }
   *out = c;
   return FK_OK;
 }
@@ -130,14 +145,23 @@ int fk_ctx_destroy(fk_ctx* ctx) {
   if (!ctx) return FK_ERR_INVALID;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
-  for (fk_buf* b : ctx->bufs) { cudaFree(b->ptr); delete b; }
+  for (fk_buf* b : ctx->bufs) { fk_dev_free(ctx, b->ptr); delete b; }
   for (fk_scene* s : std::set<fk_scene*>(ctx->scenes)) fk_scene_free(ctx, s);
   for (fk_texel_map* m : std::set<fk_texel_map*>(ctx->maps)) fk_texel_map_free(ctx, m);
+  cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->counters);
   cudaFree(ctx->status);
   cudaFree(ctx->scratch);
+  if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
+  return FK_OK;
+}
+
+int fk_ctx_trim(fk_ctx* ctx) {
+  if (!ctx) return FK_ERR_INVALID;
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (ctx->pool) FK_CUDA(ctx, cudaMemPoolTrimTo(ctx->pool, 0));
   return FK_OK;
 }
 
@@ -145,6 +169,9 @@ const char* fk_last_error(const fk_ctx* ctx) { return ctx ? ctx->err.c_str() : "
 
 int fk_ctx_set_stream(fk_ctx* ctx, void* s) {
   if (!ctx) return FK_ERR_INVALID;
+  // work queued on the old stream (and memory it gives back) is done before
+  // the new stream orders anything
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   ctx->stream = s ? (cudaStream_t)s : ctx->own_stream;
   return FK_OK;
 }
@@ -178,14 +205,14 @@ int fk_buf_alloc(fk_ctx* ctx, size_t bytes, fk_buf** out) {
   if (!ctx || !out || bytes == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_alloc: zero size or null");
   fk_buf* b = new (std::nothrow) fk_buf();
   if (!b) return FK_ERR_NOMEM;
-  cudaError_t e = cudaMalloc(&b->ptr, bytes);
-  if (e != cudaSuccess) {
+  int rc = fk_dev_alloc(ctx, &b->ptr, bytes);
+  if (rc != FK_OK) {
     delete b;
-    return fk_cuda_fail(ctx, e, "cudaMalloc");
+    return rc;
   }
-  e = cudaMemsetAsync(b->ptr, 0, bytes, ctx->stream);
+  cudaError_t e = cudaMemsetAsync(b->ptr, 0, bytes, ctx->stream);
   if (e != cudaSuccess) {
-    cudaFree(b->ptr);
+    fk_dev_free(ctx, b->ptr);
     delete b;
     return fk_cuda_fail(ctx, e, "cudaMemsetAsync");
   }
@@ -216,8 +243,15 @@ int fk_buf_download(fk_ctx* ctx, const fk_buf* b, size_t off, void* dst, size_t 
 
 int fk_buf_free(fk_ctx* ctx, fk_buf* b) {
   if (!ctx || !b || !ctx->bufs.count(b)) return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_free: unknown buffer");
-  cudaStreamSynchronize(ctx->stream);
-  cudaFree(b->ptr);
+  // the caller may have used the buffer on any stream: wait for the device
+  // before the pool can hand the memory out again
+  cudaDeviceSynchronize();
+  return fk_buf_release(ctx, b);
+}
+
+int fk_buf_release(fk_ctx* ctx, fk_buf* b) {
+  if (!ctx || !b || !ctx->bufs.count(b)) return fk_fail(ctx, FK_ERR_INVALID, "fk_buf_free: unknown buffer");
+  fk_dev_free(ctx, b->ptr);
   ctx->bufs.erase(b);
   delete b;
   return FK_OK;
@@ -235,6 +269,8 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   std::vector<float4> lo(nn), hi(nn);
   std::vector<uint32_t> jump(nn);
   uint32_t leaves = 0;
+  std::vector<uint32_t> leaf_ids;  // flattened indices of the leaves, ascending
+  bool sah_ok = true;              // leaf boxes within the rebuilt tree's coordinate range
   for (uint32_t i = 0; i < nn; ++i) {
     const fk_bvh_node& n = nodes[i];
     if (n.start > n.end || n.end > nc || n.start % 3 || n.end % 3 || n.jump <= i || n.jump > nn)
@@ -243,6 +279,11 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     if (leaf != (n.end > n.start))
       return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node " + std::to_string(i) + " mixes children and triangles");
     leaves += leaf;
+    if (leaf) {
+      leaf_ids.push_back(i);
+      for (int a = 0; a < 3; ++a)
+        sah_ok = sah_ok && fk::sah::coord_ok(n.aabb_min[a]) && fk::sah::coord_ok(n.aabb_max[a]);
+    }
     uint32_t s = n.start, e = n.end;
     float fs, fe;
     std::memcpy(&fs, &s, 4);
@@ -290,16 +331,6 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     std::memcpy(f, ints, 16);
     w[3] = make_float4(f[0], f[1], f[2], f[3]);
   }
-  // Collapsed 4-wide layout over the same records (fk_tree.cpp).
-  // The inner tree the ordered traversals walk by default: rebuilt over the
-  // same leaves with a surface-area split on all three face pairs (fk_tree.cpp);
-  // the reference's records above stay available (fk_scene_set_tree).
-  std::vector<float4> swide;
-  uint32_t sdepth = 0;
-  if (nw > 0) {
-    sdepth = fk::build_sah_wide(lo.data(), hi.data(), jump.data(), nn, swide);
-    if (sdepth > fk::kMaxOrderedDepth) swide.clear();
-  }
   fk_scene* s = new (std::nothrow) fk_scene();
   if (!s) return FK_ERR_NOMEM;
   s->ctx = ctx;
@@ -344,10 +375,20 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   s->tree_wide[FK_TREE_REFERENCE] = s->wide;
   s->tree_count[FK_TREE_REFERENCE] = nw;
   s->tree_depth[FK_TREE_REFERENCE] = maxd;
-  if (!swide.empty()) {
-    up((void**)&s->tree_wide[FK_TREE_SAH], swide.data(), sizeof(float4) * swide.size());
-    s->tree_count[FK_TREE_SAH] = (uint32_t)(swide.size() / 4);
-    s->tree_depth[FK_TREE_SAH] = sdepth;
+  // The inner tree the ordered traversals walk by default: rebuilt on the
+  // device over the same leaves with a surface-area split on all three face
+  // pairs (fk_sah.cu); the reference's records above stay available
+  // (fk_scene_set_tree).  Too deep for the ordered traversals: not kept.
+  if (rc == FK_OK && nw > 0 && sah_ok) {
+    float4* sw = nullptr;
+    uint32_t sdepth = 0;
+    rc = fk::build_sah_device(ctx, s->node_lo, s->node_hi, leaf_ids, &sw, &sdepth);
+    if (rc == FK_OK && sw) {
+      s->tree_wide[FK_TREE_SAH] = sw;
+      s->tree_count[FK_TREE_SAH] = leaves - 1;
+      s->tree_depth[FK_TREE_SAH] = sdepth;
+      s->bytes += sizeof(float4) * 4 * (size_t)(leaves - 1);
+    }
   }
   if (rc == FK_OK) {
     rc = fk_dev_alloc(ctx, (void**)&s->tri_rec, 4 * sizeof(float4) * (size_t)(nc / 3));
@@ -380,7 +421,7 @@ int fk_scene_free(fk_ctx* ctx, fk_scene* s) {
   cudaStreamSynchronize(ctx->stream);
   void* ps[] = {s->node_lo,      s->node_hi,      s->node_jump,     s->pos4,          s->nrm4,
                 s->tree_wide[0], s->tree_wide[1], s->tree_wide4[0], s->tree_wide4[1], s->tri_rec};
-  for (void* p : ps) fk_dev_free(p);
+  for (void* p : ps) fk_dev_free(ctx, p);
   ctx->scenes.erase(s);
   delete s;
   return FK_OK;
@@ -402,6 +443,22 @@ int fk_scene_set_tree(fk_scene* s, int tree) {
   s->wide4_count = s->tree_count4[tree];
   s->odepth = s->tree_depth[tree];
   s->depth4 = s->tree_depth4[tree];
+  return FK_OK;
+}
+
+int fk_diag_scene_tree(fk_ctx* ctx, const fk_scene* s, int tree, float* records, uint32_t capacity, uint32_t* count,
+                       uint32_t* depth) {
+  if (!ctx || !s || !ctx->scenes.count(const_cast<fk_scene*>(s)) || (tree != FK_TREE_REFERENCE && tree != FK_TREE_SAH))
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_diag_scene_tree: bad arguments");
+  const uint32_t n = s->tree_wide[tree] ? s->tree_count[tree] : 0;
+  if (count) *count = n;
+  if (depth) *depth = s->tree_depth[tree];
+  if (records && n) {
+    if (capacity < n) return fk_fail(ctx, FK_ERR_INVALID, "fk_diag_scene_tree: capacity below the record count");
+    FK_CUDA(ctx, cudaMemcpyAsync(records, s->tree_wide[tree], sizeof(float4) * 4 * (size_t)n, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  }
   return FK_OK;
 }
 
@@ -465,9 +522,9 @@ int fk_texel_map_download(fk_ctx* ctx, const fk_texel_map* m, float* pix8, float
 int fk_texel_map_free(fk_ctx* ctx, fk_texel_map* m) {
   if (!ctx || !m || !ctx->maps.count(m)) return fk_fail(ctx, FK_ERR_INVALID, "fk_texel_map_free: unknown map");
   cudaStreamSynchronize(ctx->stream);
-  fk_dev_free(m->pix);
-  fk_dev_free(m->pixt);
-  fk_dev_free(m->indices);
+  fk_dev_free(ctx, m->pix);
+  fk_dev_free(ctx, m->pixt);
+  fk_dev_free(ctx, m->indices);
   ctx->maps.erase(m);
   delete m;
   return FK_OK;

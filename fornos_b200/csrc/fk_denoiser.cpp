@@ -57,8 +57,8 @@ cudaError_t apply(const fk_denoiser* d, const float4* image, uint32_t w, uint32_
 
 int ensure_tiles(fk_denoiser* d, uint32_t tiles) {
   if (tiles <= d->tile_capacity) return FK_OK;
-  fk_dev_free(d->partials);
-  fk_dev_free(d->loss);
+  fk_dev_free(d->ctx, d->partials);
+  fk_dev_free(d->ctx, d->loss);
   d->partials = nullptr;
   d->loss = nullptr;
   d->tile_capacity = 0;
@@ -72,7 +72,7 @@ int ensure_tiles(fk_denoiser* d, uint32_t tiles) {
 void* scratch(fk_denoiser* d, int k, size_t bytes) {
   if (d->scratch_bytes[k] >= bytes) return d->scratch[k];
   if (cudaStreamSynchronize(d->ctx->stream) != cudaSuccess) return nullptr;
-  fk_dev_free(d->scratch[k]);
+  fk_dev_free(d->ctx, d->scratch[k]);
   d->scratch[k] = nullptr;
   d->scratch_bytes[k] = 0;
   if (fk_dev_alloc(d->ctx, &d->scratch[k], std::max<size_t>(bytes, 16)) != FK_OK) return nullptr;
@@ -173,8 +173,8 @@ int fk_denoiser_free(fk_denoiser* d) {
   if (d->ctx) cudaStreamSynchronize(d->ctx->stream);
   for (void* p : {(void*)d->params, (void*)d->m, (void*)d->v, (void*)d->grad, d->w1, d->w2, d->w2t, d->w3, d->w3t,
                   (void*)d->partials, (void*)d->loss})
-    fk_dev_free(p);
-  for (void* p : d->scratch) fk_dev_free(p);
+    fk_dev_free(d->ctx, p);
+  for (void* p : d->scratch) fk_dev_free(d->ctx, p);
   delete d;
   return FK_OK;
 }

@@ -58,7 +58,7 @@ extern "C" int fk_diag_fp32_peak(fk_ctx* ctx, double* ops) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  fk_dev_free(sink);
+  fk_dev_free(ctx, sink);
   if (rc != FK_OK) return rc;
   double total = (double)blocks * 256.0 * fk::kIters * fk::kChains * 3.0;
   *ops = total / (best_ms * 1e-3);

@@ -25,6 +25,10 @@ struct fk_ctx {
   uint32_t next_counter = 0;
   int* status = nullptr;          // device status word (limits a kernel could not honour)
   void* scratch = nullptr;        // see fk_scratch
+  // Stream-ordered pool behind every device allocation of the library; it
+  // keeps freed memory (release threshold: all), so repeated uploads and
+  // bakes reuse it instead of mapping and unmapping pages (fk_ctx_trim).
+  cudaMemPool_t pool = nullptr;
   size_t scratch_bytes = 0;
   fk_tuning tuning = {8, 8, 0, 0};   // dynamic-schedule knobs (fk_ctx_set_tuning)
   std::set<fk_buf*> bufs;
@@ -89,9 +93,12 @@ int fk_cuda_fail(fk_ctx* ctx, cudaError_t e, const char* what);
 // Checks a launch just issued on ctx->stream and counts it.
 int fk_after_launch(fk_ctx* ctx, const char* what);
 
-// Device memory owned by the library (not visible as fk_buf).
+// Device memory owned by the library (not visible as fk_buf): taken from the
+// context's pool in the order of ctx->stream and given back in that order.
 int fk_dev_alloc(fk_ctx* ctx, void** p, size_t bytes);
-void fk_dev_free(void* p);
+void fk_dev_free(fk_ctx* ctx, void* p);
+// fk_buf_free for buffers used on ctx->stream only: no device-wide wait.
+extern "C" int fk_buf_release(fk_ctx* ctx, fk_buf* b);
 
 // Reserves a zeroed device counter for one persistent-kernel launch.
 uint32_t* fk_take_counter(fk_ctx* ctx);
@@ -134,6 +141,12 @@ constexpr uint32_t kMaxOrderedDepth = 48;
 uint32_t build_sah_wide(const float4* lo, const float4* hi, const uint32_t* jump, uint32_t nn,
                         std::vector<float4>& wide);
 void collapse_wide4(const std::vector<float4>& wide, std::vector<float4>& wide4, uint32_t& n4, uint32_t& depth4);
+// The same tree built on the device (fk_sah.cu) from the scene's node boxes
+// and its leaves' flattened indices (ascending): *wide gets 4 (L - 1) float4
+// records, or stays null when the tree would be deeper than
+// kMaxOrderedDepth (*depth then exceeds it); depth 1 for a single leaf.
+int build_sah_device(fk_ctx* ctx, const float4* node_lo, const float4* node_hi, const std::vector<uint32_t>& leaves,
+                     float4** wide, uint32_t* depth);
 // The scene's 4-wide layout for its active tree, built on first use.
 int ensure_wide4(fk_ctx* ctx, fk_scene* s);
 

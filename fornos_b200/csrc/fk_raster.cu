@@ -304,9 +304,9 @@ extern "C" int fk_raster_uv(fk_ctx* ctx, const fk_mesh* m, const fk_mesh* dirs, 
   uint32_t count = 0;
   auto cleanup = [&]() {
     cudaStreamSynchronize(ctx->stream);
-    fk_dev_free(dtris);
-    fk_dev_free(owner);
-    fk_dev_free(counts);
+    fk_dev_free(ctx, dtris);
+    fk_dev_free(ctx, owner);
+    fk_dev_free(ctx, counts);
   };
   auto cuda_ok = [&](cudaError_t e, const char* what) {
     if (rc == FK_OK && e != cudaSuccess) rc = fk_cuda_fail(ctx, e, what);

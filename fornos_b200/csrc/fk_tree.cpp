@@ -13,45 +13,50 @@
 #include <vector>
 
 #include "fk_internal.h"
+#include "fk_sah_rules.h"
 
 namespace fk {
 namespace {
 
-struct Box {
-  float lo[3], hi[3];
+using sah::key;
+using sah::kmax;
+using sah::kmin;
+using sah::unkey;
+
+// Box as float keys (fk_sah_rules.h): merging is a key min / max.
+struct KBox {
+  uint32_t lo[3], hi[3];
 };
 
-Box merge(const Box& a, const Box& b) {
-  Box r;
+KBox merge(const KBox& a, const KBox& b) {
+  KBox r;
   for (int k = 0; k < 3; ++k) {
-    r.lo[k] = std::min(a.lo[k], b.lo[k]);
-    r.hi[k] = std::max(a.hi[k], b.hi[k]);
+    r.lo[k] = kmin(a.lo[k], b.lo[k]);
+    r.hi[k] = kmax(a.hi[k], b.hi[k]);
   }
   return r;
 }
 
-Box empty_box() {
-  Box b;
+KBox empty_box() {
+  KBox b;
   for (int k = 0; k < 3; ++k) {
-    b.lo[k] = 3.4e38f;
-    b.hi[k] = -3.4e38f;
+    b.lo[k] = 0xffffffffu;
+    b.hi[k] = 0u;
   }
   return b;
 }
 
-// Half the surface area (all three face pairs, in double).
-double half_area(const Box& b) {
-  const double x = std::max(0.0, (double)b.hi[0] - b.lo[0]), y = std::max(0.0, (double)b.hi[1] - b.lo[1]),
-               z = std::max(0.0, (double)b.hi[2] - b.lo[2]);
-  return x * y + y * z + z * x;
+double half_area(const KBox& b) {
+  return sah::half_area(unkey(b.lo[0]), unkey(b.hi[0]), unkey(b.lo[1]), unkey(b.hi[1]), unkey(b.lo[2]),
+                        unkey(b.hi[2]));
 }
 
-void put_record(std::vector<float4>& wide, uint32_t rec, const Box& L, int32_t refL, int32_t cntL, const Box& R,
+void put_record(std::vector<float4>& wide, uint32_t rec, const KBox& L, int32_t refL, int32_t cntL, const KBox& R,
                 int32_t refR, int32_t cntR) {
   float4* w = &wide[4 * (size_t)rec];
-  w[0] = make_float4(L.lo[0], L.hi[0], L.lo[1], L.hi[1]);
-  w[1] = make_float4(R.lo[0], R.hi[0], R.lo[1], R.hi[1]);
-  w[2] = make_float4(L.lo[2], L.hi[2], R.lo[2], R.hi[2]);
+  w[0] = make_float4(unkey(L.lo[0]), unkey(L.hi[0]), unkey(L.lo[1]), unkey(L.hi[1]));
+  w[1] = make_float4(unkey(R.lo[0]), unkey(R.hi[0]), unkey(R.lo[1]), unkey(R.hi[1]));
+  w[2] = make_float4(unkey(L.lo[2]), unkey(L.hi[2]), unkey(R.lo[2]), unkey(R.hi[2]));
   int32_t ints[4] = {refL, refR, cntL, cntR};
   float f[4];
   std::memcpy(f, ints, 16);
@@ -59,17 +64,17 @@ void put_record(std::vector<float4>& wide, uint32_t rec, const Box& L, int32_t r
 }
 
 struct Leaf {
-  Box box;
+  KBox box;
   float c[3];      // box centre
   uint32_t flat;   // flattened node index
   uint32_t tris;
 };
 
 struct SahBuilder {
-  std::vector<Leaf>& leaves;
+  std::vector<Leaf>& leaves;  // flattened-index order; every node's range stays in that order
   std::vector<float4>& wide;  // L - 1 records for L leaves, preallocated
   std::atomic<uint32_t> depth{1};
-  static constexpr int kBins = 32;
+  static constexpr int kBins = sah::kBins;
   static constexpr uint32_t kParallelLeaves = 16384;  // smaller subtrees build on the calling thread
 
   // Builds the subtree over leaves [b, e) (e - b >= 2) into records
@@ -77,9 +82,9 @@ struct SahBuilder {
   // from rec + 1, the right one from rec + (m - b).  Disjoint subtrees write
   // disjoint records, so the two halves of a large node build on two threads.
   // Returns the subtree's box; `level` counts the root as 1.
-  Box build(uint32_t rec, uint32_t b, uint32_t e, uint32_t level) {
+  KBox build(uint32_t rec, uint32_t b, uint32_t e, uint32_t level) {
     const uint32_t m = split(b, e);
-    Box boxes[2];
+    KBox boxes[2];
     int32_t refs[2], cnts[2];
     const uint32_t lo[2] = {b, m}, hi[2] = {m, e};
     const uint32_t kids[2] = {rec + 1, rec + (m - b)};
@@ -112,67 +117,66 @@ struct SahBuilder {
     }
   }
 
-  // Binned SAH over box centres on all three axes (cost = half area x
-  // triangles); partitions [b, e) and returns the split point.
+  // Binned surface-area split of [b, e) over box centres on all three axes
+  // (cost = half area x triangles, fk_sah_rules.h); stably partitions the
+  // range and returns the split point.
   uint32_t split(uint32_t b, uint32_t e) {
-    float cmin[3] = {3.4e38f, 3.4e38f, 3.4e38f}, cmax[3] = {-3.4e38f, -3.4e38f, -3.4e38f};
+    uint32_t cmin_k[3] = {0xffffffffu, 0xffffffffu, 0xffffffffu}, cmax_k[3] = {0u, 0u, 0u};
     for (uint32_t i = b; i < e; ++i)
       for (int k = 0; k < 3; ++k) {
-        cmin[k] = std::min(cmin[k], leaves[i].c[k]);
-        cmax[k] = std::max(cmax[k], leaves[i].c[k]);
+        cmin_k[k] = kmin(cmin_k[k], key(leaves[i].c[k]));
+        cmax_k[k] = kmax(cmax_k[k], key(leaves[i].c[k]));
       }
+    float cmin[3], scale[3];
+    for (int k = 0; k < 3; ++k) {
+      cmin[k] = unkey(cmin_k[k]);
+      scale[k] = sah::bin_scale(unkey(cmax_k[k]) - cmin[k]);
+    }
     double best = 1e300;
     int best_axis = -1, best_bin = 0;
-    float scale[3];
-    for (int k = 0; k < 3; ++k) {
-      const float ext = cmax[k] - cmin[k];
-      scale[k] = ext > 0.0f ? (float)kBins / ext : 0.0f;
-    }
+    uint32_t best_left = 0;
     for (int k = 0; k < 3; ++k) {
       if (!(scale[k] > 0.0f)) continue;
-      std::array<Box, kBins> bb;
-      std::array<double, kBins> bn{};
+      std::array<KBox, kBins> bb;
+      std::array<uint32_t, kBins> bt{}, bc{};
       bb.fill(empty_box());
       for (uint32_t i = b; i < e; ++i) {
-        int q = (int)((leaves[i].c[k] - cmin[k]) * scale[k]);
-        q = std::min(std::max(q, 0), kBins - 1);
+        const int q = sah::bin_of(leaves[i].c[k], cmin[k], scale[k]);
         bb[q] = merge(bb[q], leaves[i].box);
-        bn[q] += leaves[i].tris;
+        bt[q] += leaves[i].tris;
+        bc[q] += 1;
       }
       std::array<double, kBins> right_cost{};
-      Box acc = empty_box();
-      double n = 0;
+      KBox acc = empty_box();
+      uint32_t n = 0;
       for (int q = kBins - 1; q > 0; --q) {
         acc = merge(acc, bb[q]);
-        n += bn[q];
-        right_cost[q] = n > 0 ? half_area(acc) * n : 0.0;
+        n += bt[q];
+        right_cost[q] = n > 0 ? half_area(acc) * (double)n : 0.0;
       }
       acc = empty_box();
       n = 0;
+      uint32_t count = 0;
       for (int q = 0; q < kBins - 1; ++q) {
         acc = merge(acc, bb[q]);
-        n += bn[q];
-        if (n == 0 || right_cost[q + 1] == 0) continue;
-        const double cost = half_area(acc) * n + right_cost[q + 1];
+        n += bt[q];
+        count += bc[q];
+        if (n == 0 || right_cost[q + 1] == 0.0) continue;
+        const double cost = half_area(acc) * (double)n + right_cost[q + 1];
         if (cost < best) {
           best = cost;
           best_axis = k;
           best_bin = q;
+          best_left = count;
         }
       }
     }
-    uint32_t m = (b + e) / 2;
-    if (best_axis >= 0) {
-      const int k = best_axis;
-      auto it = std::partition(leaves.begin() + b, leaves.begin() + e, [&](const Leaf& l) {
-        int q = (int)((l.c[k] - cmin[k]) * scale[k]);
-        q = std::min(std::max(q, 0), kBins - 1);
-        return q <= best_bin;
-      });
-      m = (uint32_t)(it - leaves.begin());
-      if (m == b || m == e) m = (b + e) / 2;
-    }
-    return m;
+    if (best_axis < 0) return b + (e - b) / 2;  // no candidate plane: first half in flattened order
+    const int k = best_axis;
+    const float cm = cmin[k], sc = scale[k];
+    std::stable_partition(leaves.begin() + b, leaves.begin() + e,
+                          [&](const Leaf& l) { return sah::bin_of(l.c[k], cm, sc) <= best_bin; });
+    return b + best_left;
   }
 };
 
@@ -181,11 +185,17 @@ struct SahBuilder {
 uint32_t build_sah_wide(const float4* lo, const float4* hi, const uint32_t* jump, uint32_t nn,
                         std::vector<float4>& wide) {
   std::vector<Leaf> leaves;
+  wide.clear();
   for (uint32_t i = 0; i < nn; ++i) {
     if (jump[i] != i + 1) continue;
+    const float l3[3] = {lo[i].x, lo[i].y, lo[i].z}, h3[3] = {hi[i].x, hi[i].y, hi[i].z};
     Leaf l;
-    l.box = {{lo[i].x, lo[i].y, lo[i].z}, {hi[i].x, hi[i].y, hi[i].z}};
-    for (int k = 0; k < 3; ++k) l.c[k] = 0.5f * (l.box.lo[k] + l.box.hi[k]);
+    for (int k = 0; k < 3; ++k) {
+      if (!sah::coord_ok(l3[k]) || !sah::coord_ok(h3[k])) return 0;  // no rebuilt tree for this scene
+      l.box.lo[k] = key(l3[k]);
+      l.box.hi[k] = key(h3[k]);
+      l.c[k] = sah::centre(l3[k], h3[k]);
+    }
     l.flat = i;
     uint32_t s, e;
     std::memcpy(&s, &lo[i].w, 4);
@@ -193,7 +203,6 @@ uint32_t build_sah_wide(const float4* lo, const float4* hi, const uint32_t* jump
     l.tris = (e - s) / 3;
     leaves.push_back(l);
   }
-  wide.clear();
   if (leaves.size() < 2) return 1;
   wide.resize(4 * (leaves.size() - 1));
   SahBuilder sb{leaves, wide};
@@ -270,3 +279,30 @@ void collapse_wide4(const std::vector<float4>& wide, std::vector<float4>& wide4,
 }
 
 }  // namespace fk
+
+extern "C" int fk_diag_sah_host(const fk_bvh_node* nodes, uint32_t nn, float* records, uint32_t capacity,
+                                uint32_t* count, uint32_t* depth) {
+  if (!nodes || nn == 0) return FK_ERR_INVALID;
+  std::vector<float4> lo(nn), hi(nn);
+  std::vector<uint32_t> jump(nn);
+  for (uint32_t i = 0; i < nn; ++i) {
+    const fk_bvh_node& n = nodes[i];
+    if (n.jump <= i || n.jump > nn || n.start > n.end || (n.jump == i + 1) != (n.end > n.start)) return FK_ERR_INVALID;
+    float fs, fe;
+    std::memcpy(&fs, &n.start, 4);
+    std::memcpy(&fe, &n.end, 4);
+    lo[i] = make_float4(n.aabb_min[0], n.aabb_min[1], n.aabb_min[2], fs);
+    hi[i] = make_float4(n.aabb_max[0], n.aabb_max[1], n.aabb_max[2], fe);
+    jump[i] = n.jump;
+  }
+  std::vector<float4> wide;
+  const uint32_t d = fk::build_sah_wide(lo.data(), hi.data(), jump.data(), nn, wide);
+  const uint32_t n = (uint32_t)(wide.size() / 4);
+  if (count) *count = n;
+  if (depth) *depth = d;
+  if (records) {
+    if (capacity < n) return FK_ERR_INVALID;
+    std::memcpy(records, wide.data(), sizeof(float4) * wide.size());
+  }
+  return FK_OK;
+}

@@ -57,14 +57,21 @@ typedef struct fk_meshmapping fk_meshmapping;
 typedef struct fk_solver fk_solver;
 
 /* ------------------------------------------------------------ context */
-/* Opens `device` (must be compute capability 10.x).  No graphics context. */
+/* Opens `device` (must be compute capability 10.x).  No graphics context.
+ * Device memory of the context (buffers, scenes, texel maps, scratch) comes
+ * from a stream-ordered pool of its own that keeps what is freed for reuse;
+ * fk_ctx_trim returns the unused part to the device. */
 int fk_ctx_create(int device, fk_ctx** out);
 int fk_ctx_destroy(fk_ctx* ctx);
 const char* fk_last_error(const fk_ctx* ctx);
-/* cudaStream_t to order work on; NULL = the context's own stream. */
+/* cudaStream_t to order work on; NULL = the context's own stream.  Waits for
+ * the work queued on the previous stream. */
 int fk_ctx_set_stream(fk_ctx* ctx, void* cuda_stream);
 void* fk_ctx_stream(const fk_ctx* ctx);
 int fk_sync(fk_ctx* ctx);
+/* No counterpart in the reference.  Waits for the context's stream and
+ * releases the pool memory no live object uses. */
+int fk_ctx_trim(fk_ctx* ctx);
 /* Kernel launches issued by this context so far. */
 uint64_t fk_launch_count(const fk_ctx* ctx);
 
@@ -154,14 +161,17 @@ typedef struct fk_scene_info {
 } fk_scene_info;
 int fk_scene_get_info(const fk_scene* scene, fk_scene_info* out);
 /* No counterpart in the reference.  The inner tree the ordered traversals
- * (FK_TRAVERSE_ORDERED / ORDERED4) walk: FK_TREE_REFERENCE, the inner nodes of
- * BVH::createBinary as uploaded (the default), or FK_TREE_SAH, an inner tree
- * rebuilt over the same leaves with a binned surface-area split on all three
- * box faces (the reference's split cost, Src/bvh.cpp:63-68, counts x*y twice and
- * y*z never).  Leaves, leaf boxes and the skip-pointer walk are untouched, and
- * the outcome is that of any inner tree over these leaves (an inner box only
- * prunes what its leaves' own tests reject), so results stay within the
- * ordered traversal's bar.  Both trees stay resident once built. */
+ * (FK_TRAVERSE_ORDERED / ORDERED4) walk: FK_TREE_SAH (the default whenever it
+ * was built), an inner tree rebuilt on the device at upload over the same
+ * leaves with a binned surface-area split on all three box faces (the
+ * reference's split cost, Src/bvh.cpp:63-68, counts x*y twice and y*z never),
+ * or FK_TREE_REFERENCE, the inner nodes of BVH::createBinary as uploaded.
+ * Leaves, leaf boxes and the skip-pointer walk are untouched, and the outcome
+ * is that of any inner tree over these leaves (an inner box only prunes what
+ * its leaves' own tests reject), so results stay within the ordered
+ * traversal's bar.  Both trees stay resident.  The rebuilt tree is not built
+ * when a leaf box coordinate is not finite or not below 1e30 in magnitude, nor
+ * kept when it is deeper than 48 levels. */
 #define FK_TREE_REFERENCE 0
 #define FK_TREE_SAH 1
 int fk_scene_set_tree(fk_scene* scene, int tree);
@@ -457,6 +467,24 @@ int fk_diag_traversal_counts(fk_ctx* ctx, const fk_scene* scene, const fk_buf* c
 int fk_diag_traversal_profile(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
                               const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
                               int traverse, uint64_t* counters);
+
+/* No counterpart in the reference.  An inner tree of the scene as resident on
+ * the device (FK_TREE_REFERENCE or FK_TREE_SAH): its 2-wide records, 16 words
+ * each (floats 0-3 / 4-7: the left / right child's x and y bounds, 8-9 /
+ * 10-11: their z bounds; ints 12 / 13: the children's refs, a record index or
+ * -(flattened leaf index + 1); ints 14 / 15: leaf triangle counts), root
+ * record 0, and its depth (root = 1, counting the leaf level).  records may be
+ * NULL to query count and depth, else capacity (in records) must hold them
+ * all.  count 0: that tree was not built for this scene. */
+int fk_diag_scene_tree(fk_ctx* ctx, const fk_scene* scene, int tree, float* records, uint32_t capacity,
+                       uint32_t* count, uint32_t* depth);
+/* The surface-area inner tree computed on the host from a flattened node
+ * array, no device needed: when its depth is at most 48 these are, bit for
+ * bit, the FK_TREE_SAH records fk_scene_upload builds on the device.  count 0
+ * and depth 0: a leaf box coordinate is not finite or not below 1e30 in
+ * magnitude (no rebuilt tree); count 0 and depth 1: a single leaf. */
+int fk_diag_sah_host(const fk_bvh_node* nodes, uint32_t node_count, float* records, uint32_t capacity,
+                     uint32_t* count, uint32_t* depth);
 
 /* ------------------------------------------------------------ learned denoiser
  * No counterpart in the reference.  A per-texel MLP that turns a low-sample
