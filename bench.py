@@ -1,7 +1,9 @@
 """Headline benchmark: plain bake throughput (Mrays/s) on one or more B200s.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fornos|reference]
-                    [--workload plane2048|sphere512|icosphere4096] [--traverse auto|ordered|skip]
+                    [--workload plane2048|sphere512|icosphere4096|plane250|batch|denoise]
+                    [--traverse auto|ordered|skip|ordered4] [--schedule auto|static|dynamic]
+                    [--tree sah|reference] [--no-denoise] [--denoise-tex T] [--no-cpu-baseline]
 
 One step = one full plain bake of the workload with every input resident in
 HBM: mesh mapping (2 rays / texel), height, position and tangent-space normal
@@ -11,6 +13,11 @@ texel).  value = rays of all ranks / max-over-ranks device time.  e2e = the
 same bake through fk_bake from pinned host arrays (uploads and result copies
 inside the timed region).  Multi-GPU: one process per GPU, each baking its
 own seeded replica of the workload (weak scaling, no data-path collective).
+
+The default line also carries the denoised-vs-plain comparison at 4096x4096
+(`denoise`); --workload batch measures 64 batched jobs and --workload denoise
+the comparison alone.  --tree reference walks the reference's inner BVH nodes
+instead of the surface-area tree built at upload.
 
 --impl reference times the reference's own CPU implementation of the path
 (the reference's shaders and host code compiled by oracle/build_ref.py, or
@@ -60,10 +67,10 @@ WORKLOADS = {
 }
 TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2, "ordered4": 3}
 SCHEDULE = {"auto": 0, "static": 0x10, "dynamic": 0x20}
-# DRAM bytes per hemisphere-kernel launch from ncu captures (profiles/), by workload.
-# plane250: measured for one AO+BN trace launch (984,064 rays); plane2048: the same 364.5 B per ray scaled to one
-# chunk launch of 134,217,728 rays (traffic grows with rays).  Source: profiles/hemi_trace_kernel_plane250.md.
-NCU_TRAFFIC = {"plane250": 358.7e6, "plane2048": 48.9e9}
+# DRAM bytes (read + write) per hemisphere-kernel launch from ncu captures, by workload: plane250, one AO+BN
+# trace launch of 968,256 rays (profiles/hemi_trace_kernel_plane250.md); plane2048, the mean of two AO+BN chunk
+# launches of 134,217,728 rays each, 4.88 and 3.27 GB (profiles/hemi_trace_traffic_plane2048.md).
+NCU_TRAFFIC = {"plane250": 301.0e6, "plane2048": 4.08e9}
 
 
 def rays_per_texel(wl):
@@ -357,13 +364,15 @@ def run_denoise_bench(args):
     ctx.set_stream(stream.cuda_stream)
     prep = Prepared(WORKLOADS["plane2048"], args.seed)
     scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
-    r = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed)
+    r = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed, args.denoise_tex)
     if "unavailable" in r:
         return dict(r, metric="AO + bent-normal texels/s, 16 spp + denoiser vs 1024 spp")
-    return {"metric": "AO + bent-normal texels/s at 4096x4096: 16 spp + denoiser (verified) vs plain 1024 spp",
+    return {"metric": "AO + bent-normal texels/s at %dx%d: 16 spp + denoiser (verified) vs plain 1024 spp" % (
+                args.denoise_tex, args.denoise_tex),
             "value": r["denoised"]["texels_per_s"], "unit": "texels/s", "n_gpus": 1, "higher_is_better": True,
             "dtype": "f32 traversal, bf16 network", "data": "synthetic (seeded generated meshes)",
-            "config": {"workload": "denoise4096", "scene": WORKLOADS["plane2048"]["desc"], "seed": args.seed},
+            "config": {"workload": "denoise%d" % args.denoise_tex, "scene": WORKLOADS["plane2048"]["desc"],
+                       "seed": args.seed},
             "denoise": r}
 
 
@@ -372,8 +381,9 @@ DENOISE = dict(tex=4096, low=16, full=1024, label=4096, min_d=0.001, max_d=0.3, 
                mae_texels=65536)
 
 
-def denoise_compare(ctx, stream, prep, scene, weights, seed):
-    """AO + bent normals of the plane workload's scene at 4096 x 4096 texels:
+def denoise_compare(ctx, stream, prep, scene, weights, seed, tex=4096):
+    """AO + bent normals of the plane workload's scene at tex x tex texels
+    (4096 for the reported comparison; smaller sizes serve as profiling cases):
     the plain 1024-sample bake against the verified 16-sample + network bake
     (spot checks and per-tile fallback included), each timed with CUDA events
     over one whole pass, and each scored by mean absolute error against
@@ -383,8 +393,7 @@ def denoise_compare(ctx, stream, prep, scene, weights, seed):
     from fornos_b200 import api
     if not os.path.exists(weights):
         return {"unavailable": "no trained denoiser weights at %s" % os.path.relpath(weights, ROOT)}
-    d = DENOISE
-    tex = d["tex"]
+    d = dict(DENOISE, tex=tex)
     tm = api.TexelMap.from_meshes(ctx, prep.lm, prep.dm, tex, tex)
     n = tm.count
     coords, tidx = ctx.buffer(16 * n), ctx.buffer(4 * n)
@@ -698,6 +707,8 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoised-vs-plain comparison")
+    ap.add_argument("--denoise-tex", type=int, default=4096,
+                    help="texture size of the denoised-vs-plain comparison (4096 reported; smaller for profiling)")
     ap.add_argument("--denoiser", default=os.path.join(ROOT, "fornos_b200", "data", "denoiser_plane2048.npz"))
     args = ap.parse_args()
     if args.workload == "batch":
@@ -732,7 +743,7 @@ def main():
                                   "sample": cpu.describe(rays, m)}
     if rank == 0 and world == 1 and args.workload == "plane2048" and not args.no_denoise:
         prep, _, _, _, ctx, stream, scene = state
-        result["denoise"] = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed)
+        result["denoise"] = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed, args.denoise_tex)
     if rank == 0:
         print(json.dumps(result))
     if world > 1:
