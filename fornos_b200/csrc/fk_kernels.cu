@@ -653,6 +653,80 @@ __device__ __forceinline__ void leaf_visit(const SceneDev& s, const RayPre& rp, 
   st.pend = -1;
 }
 
+// Order-preserving key of a non-negative distance (total order, -0 below +0)
+// for the leaf phase's shared-memory minimum.
+__device__ __forceinline__ uint32_t dist_key(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float dist_unkey(uint32_t k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+// Leaf phase, warp-cooperative.  Every lane holding a postponed leaf tests
+// the leaf's box exactly against its current threshold; the triangles of the
+// leaves that pass are then laid end to end by a warp scan and spread over all
+// 32 lanes: lane j of a round takes item base + j, finds the owning lane by a
+// binary search over the scan and fetches that lane's ray and distance by
+// shuffles.  A hit lowers the owner's distance through a key minimum in
+// shared memory (`skey`, 32 words for this warp).  The closest distance is the
+// minimum over the hits in [lo, best), so neither the order of the tests nor
+// the owner's distance at the start of the phase (which only admits more
+// candidates) changes it.  All lanes of the warp call this; returns whether
+// this lane visited a leaf.
+template <bool COUNT, bool FILTER>
+__device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
+                                                OState& st, bool active, uint32_t* skey, Tally& tally) {
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  uint32_t first = 0, cnt = 0;
+  const bool mine = active && st.pend >= 0;
+  if (mine) {
+    const float4 L = __ldg(s.node_lo + st.pend), H = __ldg(s.node_hi + st.pend);
+    float entry;
+    if (COUNT) tally.box++;
+    if (child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry)) {
+      first = as_u32(L.w) / 3;
+      cnt = (as_u32(H.w) - as_u32(L.w)) / 3;
+      if (COUNT) tally.tri += cnt;
+    }
+    st.pend = -1;
+  }
+  uint32_t incl = cnt;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t v = __shfl_up_sync(full, incl, d);
+    if (lane >= d) incl += v;
+  }
+  const uint32_t total = __shfl_sync(full, incl, 31);
+  if (total == 0) return mine;
+  skey[lane] = dist_key(best);
+  __syncwarp();
+  const uint32_t excl = incl - cnt;
+  for (uint32_t base = 0; base < total; base += 32) {
+    const uint32_t j = base + lane;
+    // owner: the number of lanes whose inclusive count is <= j (steps sum to
+    // 31, so o stays a lane index; for j < total it is the lane holding item j)
+    int o = 0;
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t v = __shfl_sync(full, incl, o + step - 1);
+      if (v <= j) o += step;
+    }
+    const f3 ro = mk3(__shfl_sync(full, rp.o.x, o), __shfl_sync(full, rp.o.y, o), __shfl_sync(full, rp.o.z, o));
+    const f3 rd = mk3(__shfl_sync(full, rp.d.x, o), __shfl_sync(full, rp.d.y, o), __shfl_sync(full, rp.d.z, o));
+    const float ob = __shfl_sync(full, best, o);
+    const uint32_t tri = __shfl_sync(full, first, o) + (j - __shfl_sync(full, excl, o));
+    if (j < total) {
+      float b = ob;
+      tri_sample(s.rec, tri, ro, rd, lo, b);
+      if (b < ob) atomicMin(skey + o, dist_key(b));
+    }
+  }
+  __syncwarp();
+  if (cnt > 0) best = dist_unkey(skey[lane]);
+  __syncwarp();  // the words are rewritten by the next leaf phase
+  return mine;
+}
+
 // Takes the nearest still-open deferred entry; false when none is left.
 template <bool FILTER>
 __device__ __forceinline__ bool pop(OState& st, const int2* stk, float thr) {
@@ -700,6 +774,8 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
   int2 stk[is_ordered(TRAV) ? kStack : 1];  // deferred (ref, entry) pairs
+  __shared__ uint32_t leaf_keys[256 / 32][32];  // leaf-phase distance minimum, per warp
+  uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t r = 0;
@@ -775,13 +851,12 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
         wc[1] += leaf_phase;
         wc[leaf_phase ? 3 : 2] += __popc(leaf_phase ? leaves : need);
       }
+      const bool visited =
+          leaf_phase && leaf_phase_warp<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, active, skey, tally);
       if (active) {
         bool fin = false;
         if (leaf_phase) {
-          if (st.pend >= 0) {
-            leaf_visit<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, tally);
-            fin = settled<STOP>(best, p.hi);
-          }
+          if (visited) fin = settled<STOP>(best, p.hi);
         } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
           if (!visit_inner<TRAV, COUNT, FILTER>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally))
             fin = true;
