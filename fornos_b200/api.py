@@ -95,7 +95,7 @@ class Context:
     def launches(self):
         return int(self.lib.fk_launch_count(self.handle))
 
-    def set_tuning(self, refill=8, leaf_batch=16, speculate=0):
+    def set_tuning(self, refill=16, leaf_batch=8, speculate=1):
         t = L.Tuning(refill, leaf_batch, speculate, 0)
         _check(self.lib.fk_ctx_set_tuning(self.handle, ctypes.byref(t)), self, "fk_ctx_set_tuning")
 

@@ -30,7 +30,7 @@ struct fk_ctx {
   // bakes reuse it instead of mapping and unmapping pages (fk_ctx_trim).
   cudaMemPool_t pool = nullptr;
   size_t scratch_bytes = 0;
-  fk_tuning tuning = {8, 8, 0, 0};   // dynamic-schedule knobs (fk_ctx_set_tuning)
+  fk_tuning tuning = {16, 8, 1, 0};  // dynamic-schedule knobs (fk_ctx_set_tuning)
   std::set<fk_buf*> bufs;
   std::set<fk_scene*> scenes;
   std::set<fk_texel_map*> maps;

@@ -636,23 +636,6 @@ __device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp,
   return inner_visit<COUNT, FILTER>(s, rp, thr, st, stk, status, tally);
 }
 
-// Leaf phase: the postponed leaf's triangles, if its box still passes.
-template <bool COUNT, bool FILTER>
-__device__ __forceinline__ void leaf_visit(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
-                                           OState& st, Tally& tally) {
-  // The leaf's own box decides here, exactly, against the current threshold
-  // (inner-phase tests of it may have been conservative).
-  const float4 L = __ldg(s.node_lo + st.pend), H = __ldg(s.node_hi + st.pend);
-  float entry;
-  if (COUNT) tally.box++;
-  if (child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry)) {
-    const uint32_t b = as_u32(L.w), e = as_u32(H.w);
-    if (COUNT) tally.tri += (e - b) / 3;
-    for (uint32_t k = b; k < e; k += 3) tri_sample(s.rec, k / 3, rp.o, rp.d, lo, best);
-  }
-  st.pend = -1;
-}
-
 // Order-preserving key of a non-negative distance (total order, -0 below +0)
 // for the leaf phase's shared-memory minimum.
 __device__ __forceinline__ uint32_t dist_key(float f) {
@@ -673,8 +656,10 @@ __device__ __forceinline__ float dist_unkey(uint32_t k) {
 // minimum over the hits in [lo, best), so neither the order of the tests nor
 // the owner's distance at the start of the phase (which only admits more
 // candidates) changes it.  All lanes of the warp call this; returns whether
-// this lane visited a leaf.
-template <bool COUNT, bool FILTER>
+// this lane visited a leaf.  MULTI: lanes may trace different scenes and
+// distance ranges (batched jobs), so the owner's triangle records and minimum
+// distance travel with its ray.
+template <bool COUNT, bool FILTER, bool MULTI = false>
 __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
                                                 OState& st, bool active, uint32_t* skey, Tally& tally) {
   const unsigned full = 0xFFFFFFFFu;
@@ -715,9 +700,16 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
     const f3 rd = mk3(__shfl_sync(full, rp.d.x, o), __shfl_sync(full, rp.d.y, o), __shfl_sync(full, rp.d.z, o));
     const float ob = __shfl_sync(full, best, o);
     const uint32_t tri = __shfl_sync(full, first, o) + (j - __shfl_sync(full, excl, o));
+    const float4* rec = s.rec;
+    float olo = lo;
+    if (MULTI) {
+      const unsigned long long a = __shfl_sync(full, (unsigned long long)(uintptr_t)s.rec, o);
+      rec = reinterpret_cast<const float4*>((uintptr_t)a);
+      olo = __shfl_sync(full, lo, o);
+    }
     if (j < total) {
       float b = ob;
-      tri_sample(s.rec, tri, ro, rd, lo, b);
+      tri_sample(rec, tri, ro, rd, olo, b);
       if (b < ob) atomicMin(skey + o, dist_key(b));
     }
   }
@@ -1040,6 +1032,8 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
   // a launch traces at most the scratch's 2^27 rays: lane indices fit 32 bits
   const uint32_t total = (uint32_t)((p.r1 - p.r0 + p.stride - 1) / p.stride);
   int2 stk[is_ordered(TRAV) ? kStack : 1];  // deferred (ref, entry) pairs
+  __shared__ uint32_t leaf_keys[256 / 32][32];  // leaf-phase distance minimum, per warp
+  uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t q = 0;
@@ -1116,13 +1110,12 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
       const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
       const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
+      const bool visited =
+          leaf_phase && leaf_phase_warp<false, FILTER, true>(s, rp, lo, hi, best, st, active, skey, tally);
       if (active) {
         bool fin = false;
         if (leaf_phase) {
-          if (st.pend >= 0) {
-            leaf_visit<false, FILTER>(s, rp, lo, hi, best, st, tally);
-            fin = settled<STOP>(best, hi);
-          }
+          if (visited) fin = settled<STOP>(best, hi);
         } else if (st.cur >= 0 && st.pend < 0) {
           if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally))
             fin = true;

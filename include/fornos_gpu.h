@@ -75,8 +75,9 @@ int fk_ctx_trim(fk_ctx* ctx);
 /* Kernel launches issued by this context so far. */
 uint64_t fk_launch_count(const fk_ctx* ctx);
 
-/* Knobs of the dynamically scheduled hemisphere traversal (defaults 8, 8,
- * 0, 0); fk_tune_hemisphere picks them by measurement. */
+/* Knobs of the dynamically scheduled hemisphere traversal (defaults 16, 8,
+ * 1, 0, from a full-size sweep of the plane workload); fk_tune_hemisphere
+ * picks them by measurement. */
 typedef struct fk_tuning {
   uint32_t refill;      /* idle lanes of a warp that trigger a batch fetch (1..32) */
   uint32_t leaf_batch;  /* lanes holding a postponed leaf that start a leaf phase (1..32) */
