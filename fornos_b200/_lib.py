@@ -173,6 +173,8 @@ _SIGS = {
                                          c_u32, c_int, ctypes.POINTER(c_u64)]),
     "fk_diag_traversal_profile": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32,
                                           c_u32, c_int, ctypes.POINTER(c_u64)]),
+    "fk_bvh_build_flat": (c_int, [c_vp, c_vp, c_u32, c_u32, c_vp, c_u32, ctypes.POINTER(c_u32), f32p, f32p]),
+    "fk_scene_build": (c_int, [c_vp, c_vp, c_u32, c_u32, ctypes.POINTER(c_vp)]),
     "fk_diag_scene_tree": (c_int, [c_vp, c_vp, c_int, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
     "fk_diag_sah_host": (c_int, [c_vp, c_u32, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
     "fk_denoiser_create": (c_int, [c_vp, ctypes.POINTER(c_vp)]),

@@ -249,6 +249,20 @@ class BVH:
         except Exception:
             pass
 
+    @staticmethod
+    def build_flat_device(ctx, mesh, max_triangle_count=8, max_tree_depth=8192):
+        """createBinary + fillMeshData on the device (fk_bvh_build_flat):
+        (nodes, positions4, normals4), equal to create_binary(...).flatten(mesh)."""
+        nf = mesh.arrays().triangle_count
+        nodes = np.zeros(max(2 * nf - 1, 1), NODE_DTYPE)
+        pos4 = np.zeros((3 * nf, 4), np.float32)
+        nrm4 = np.zeros((3 * nf, 4), np.float32)
+        nn = L.c_u32()
+        _check(ctx.lib.fk_bvh_build_flat(ctx.handle, mesh.handle, max_triangle_count, max_tree_depth, nodes.ctypes.data,
+                                         len(nodes), ctypes.byref(nn), _f32(pos4), _f32(nrm4)), ctx,
+               "fk_bvh_build_flat")
+        return nodes[:nn.value].copy(), pos4, nrm4
+
 
 class Scene:
     """High-poly mesh + BVH resident on the device (fk_scene)."""
@@ -268,6 +282,16 @@ class Scene:
     def borrowed(cls, ctx, handle):
         s = cls.__new__(cls)
         s.ctx, s.handle, s.owned = ctx, handle, False
+        return s
+
+    @classmethod
+    def build(cls, ctx, mesh, max_triangle_count=8, max_tree_depth=8192):
+        """BVH built on the device straight into a scene (fk_scene_build)."""
+        h = L.c_vp()
+        _check(ctx.lib.fk_scene_build(ctx.handle, mesh.handle, max_triangle_count, max_tree_depth, ctypes.byref(h)),
+               ctx, "fk_scene_build")
+        s = cls.__new__(cls)
+        s.ctx, s.handle, s.owned = ctx, h.value, True
         return s
 
     def info(self):

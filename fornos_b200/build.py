@@ -22,7 +22,7 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "--fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false",
-              "-Xcompiler", "-fPIC", "-Xptxas", "-warn-spills"]
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xptxas", "-warn-spills"]
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall",
              "-I" + os.path.join(CUDA, "include")]
 

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <thread>
 
+#include "fk_bvh_rules.h"
 #include "fk_internal.h"
 
 namespace {
@@ -26,24 +27,24 @@ inline Box empty_box() {
   for (int a = 0; a < 3; ++a) { b.lo[a] = FLT_MAX; b.hi[a] = -FLT_MAX; }
   return b;
 }
-// addPoint (Src/bvh.cpp:31-35): min(p, acc), argument order kept because a
-// tie between +0 and -0 resolves by position.
+// min / max below are fk::bvh::fmin / fmax (fk_bvh_rules.h): order does not
+// matter, so these folds equal the device build's parallel ones.
+// addPoint (Src/bvh.cpp:31-35).
 inline void add_point(Box& b, const float* p) {
-  for (int a = 0; a < 3; ++a) { b.lo[a] = std::fmin(p[a], b.lo[a]); b.hi[a] = std::fmax(p[a], b.hi[a]); }
+  for (int a = 0; a < 3; ++a) { b.lo[a] = fk::bvh::fmin(p[a], b.lo[a]); b.hi[a] = fk::bvh::fmax(p[a], b.hi[a]); }
 }
 // min(acc, triangle bounds) of the partition loop (Src/bvh.cpp:240-247).
 inline void grow_acc(Box& b, const float* lo, const float* hi) {
-  for (int a = 0; a < 3; ++a) { b.lo[a] = std::fmin(b.lo[a], lo[a]); b.hi[a] = std::fmax(b.hi[a], hi[a]); }
+  for (int a = 0; a < 3; ++a) { b.lo[a] = fk::bvh::fmin(b.lo[a], lo[a]); b.hi[a] = fk::bvh::fmax(b.hi[a], hi[a]); }
 }
 inline Box join(const Box& a, const Box& b) {
   Box r = a;
-  for (int k = 0; k < 3; ++k) { r.lo[k] = std::fmin(b.lo[k], r.lo[k]); r.hi[k] = std::fmax(b.hi[k], r.hi[k]); }
+  for (int k = 0; k < 3; ++k) { r.lo[k] = fk::bvh::fmin(b.lo[k], r.lo[k]); r.hi[k] = fk::bvh::fmax(b.hi[k], r.hi[k]); }
   return r;
 }
 // Src/bvh.cpp:63-68 (x*y appears twice in the reference's area term).
 inline float cost_of(const Box& b, int n) {
-  float ex = b.hi[0] - b.lo[0], ey = b.hi[1] - b.lo[1], ez = b.hi[2] - b.lo[2];
-  return float(n) * (2.0f * (ex * ey + ex * ez + ex * ey));
+  return fk::bvh::cost(b.hi[0] - b.lo[0], b.hi[1] - b.lo[1], b.hi[2] - b.lo[2], n);
 }
 
 // Per-triangle values the build reads repeatedly.
@@ -66,51 +67,28 @@ struct Build {
     Box cb = empty_box();
     for (uint32_t i = b; i < e; ++i) add_point(cb, pre[order[i]].cdiv);
     uint32_t cnt[3][16] = {};
-    Box bb[3][16];
+    float blo[3][16][3], bhi[3][16][3];
     for (int a = 0; a < 3; ++a)
-      for (int k = 0; k < 16; ++k) bb[a][k] = empty_box();
+      for (int k = 0; k < 16; ++k)
+        for (int q = 0; q < 3; ++q) {
+          blo[a][k][q] = FLT_MAX;
+          bhi[a][k][q] = -FLT_MAX;
+        }
     float ext[3];
     for (int a = 0; a < 3; ++a) ext[a] = cb.hi[a] - cb.lo[a];
     for (uint32_t i = b; i < e; ++i) {
       const Pre& p = pre[order[i]];
       for (int a = 0; a < 3; ++a) {
-        float r = ((p.cdiv[a] - cb.lo[a]) / ext[a]) * 15.99f;
-        size_t k = std::isnan(r) ? 0 : (size_t)r;
+        const uint32_t k = fk::bvh::bucket(p.cdiv[a], cb.lo[a], ext[a]);
         cnt[a][k]++;
-        add_point(bb[a][k], p.p[0]);
-        add_point(bb[a][k], p.p[1]);
-        add_point(bb[a][k], p.p[2]);
+        for (int c = 0; c < 3; ++c)
+          for (int q = 0; q < 3; ++q) {
+            blo[a][k][q] = fk::bvh::fmin(p.p[c][q], blo[a][k][q]);
+            bhi[a][k][q] = fk::bvh::fmax(p.p[c][q], bhi[a][k][q]);
+          }
       }
     }
-    float best_cost[3];
-    int best_idx[3];
-    const int n = (int)(e - b);
-    for (int a = 0; a < 3; ++a) {
-      Box right[15];
-      right[14] = bb[a][15];
-      for (int k = 13; k >= 0; --k) right[k] = join(right[k + 1], bb[a][k + 1]);
-      Box left = empty_box();
-      int nl = 0, nr = n;
-      float best = FLT_MAX;
-      int bi = 0;
-      // The all-left step (k = 15) has an empty right side: its cost is NaN
-      // and it never wins (the reference reads past its table there).
-      for (int k = 0; k < 15; ++k) {
-        nl += (int)cnt[a][k];
-        nr -= (int)cnt[a][k];
-        left = join(left, bb[a][k]);
-        float c = cost_of(left, nl) + cost_of(right[k], nr);
-        if (c < best) { best = c; bi = k; }
-      }
-      best_cost[a] = best;
-      best_idx[a] = bi;
-    }
-    int ax;
-    if (best_cost[0] <= best_cost[1] && best_cost[0] <= best_cost[2]) ax = 0;
-    else if (best_cost[1] <= best_cost[0] && best_cost[1] <= best_cost[2]) ax = 1;
-    else ax = 2;
-    *axis = ax;
-    *value = cb.lo[ax] + (cb.hi[ax] - cb.lo[ax]) / 16.0f * float(best_idx[ax] + 1);
+    fk::bvh::pick_split(blo, bhi, cnt, (int)(e - b), cb.lo, cb.hi, axis, value);
   }
 
   static void set_box(Node& n, const Box& b) {
@@ -141,8 +119,8 @@ struct Build {
       const Pre& p = pre[t];
       float lo[3], hi[3];
       for (int a = 0; a < 3; ++a) {
-        lo[a] = std::fmin(p.p[0][a], std::fmin(p.p[1][a], p.p[2][a]));
-        hi[a] = std::fmax(p.p[0][a], std::fmax(p.p[1][a], p.p[2][a]));
+        lo[a] = fk::bvh::fmin(p.p[0][a], fk::bvh::fmin(p.p[1][a], p.p[2][a]));
+        hi[a] = fk::bvh::fmax(p.p[0][a], fk::bvh::fmax(p.p[1][a], p.p[2][a]));
       }
       if (p.cmul[axis] <= split) {
         order[w++] = t;
@@ -187,8 +165,8 @@ struct Build {
     const Node& B = out[ri];
     Box u;
     for (int a = 0; a < 3; ++a) {
-      u.lo[a] = std::fmin(A.c[a] - A.s[a], B.c[a] - B.s[a]);
-      u.hi[a] = std::fmax(A.c[a] + A.s[a], B.c[a] + B.s[a]);
+      u.lo[a] = fk::bvh::fmin(A.c[a] - A.s[a], B.c[a] - B.s[a]);
+      u.hi[a] = fk::bvh::fmax(A.c[a] + A.s[a], B.c[a] + B.s[a]);
       out[ni].c[a] = (u.hi[a] + u.lo[a]) * 0.5f;
       out[ni].s[a] = (u.hi[a] - u.lo[a]) * 0.5f;
     }

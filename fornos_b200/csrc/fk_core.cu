@@ -261,9 +261,13 @@ size_t fk_buf_size(const fk_buf* b) { return b ? b->bytes : 0; }
 void* fk_buf_device_ptr(const fk_buf* b) { return b ? b->ptr : nullptr; }
 
 // ------------------------------------------------------------------ scene
-int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const float* pos4, const float* nrm4,
-                    uint32_t nc, fk_scene** out) {
-  if (!ctx || !out || !nodes || !pos4 || !nrm4 || nn == 0 || nc == 0 || nc % 3 != 0)
+}  // extern "C"
+
+// Scene from a flattened node array: host corner arrays (fk_scene_upload), or
+// the device build's arrays, which the scene adopts (`dev`: nodes, corners).
+static int scene_create(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const float* pos4, const float* nrm4,
+                        uint32_t nc, fk::DevBvh* dev, fk_scene** out) {
+  if (!ctx || !out || !nodes || (!dev && (!pos4 || !nrm4)) || nn == 0 || nc == 0 || nc % 3 != 0)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: empty or malformed scene");
   // Validate the skip-pointer structure so no kernel can walk outside it.
   std::vector<float4> lo(nn), hi(nn);
@@ -351,8 +355,18 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     for (uint32_t i = 0; i < nn && ok; ++i)
       for (int a = 0; a < 3; ++a)
         ok = ok && std::fabs(nodes[i].aabb_min[a]) < lim && std::fabs(nodes[i].aabb_max[a]) < lim;
-    for (size_t i = 0; i < (size_t)nc && ok; ++i)
-      for (int a = 0; a < 3; ++a) ok = ok && std::fabs(pos4[4 * i + a]) < lim;
+    if (!dev) {
+      for (size_t i = 0; i < (size_t)nc && ok; ++i)
+        for (int a = 0; a < 3; ++a) ok = ok && std::fabs(pos4[4 * i + a]) < lim;
+    } else if (ok) {
+      bool below = false;
+      const int rc = fk::corners_below(ctx, dev->pos4, nc, lim, &below);
+      if (rc != FK_OK) {
+        delete s;
+        return rc;
+      }
+      ok = below;
+    }
     s->filter_ok = ok ? 1 : 0;
   }
   size_t nb = sizeof(float4) * nn, cb = sizeof(float4) * (size_t)nc;
@@ -366,11 +380,21 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
     }
     s->bytes += bytes;
   };
-  up((void**)&s->node_lo, lo.data(), nb);
-  up((void**)&s->node_hi, hi.data(), nb);
-  up((void**)&s->node_jump, jump.data(), sizeof(uint32_t) * nn);
-  up((void**)&s->pos4, pos4, cb);
-  up((void**)&s->nrm4, nrm4, cb);
+  if (dev) {  // adopted: the scene frees them
+    s->node_lo = dev->lo;
+    s->node_hi = dev->hi;
+    s->node_jump = dev->jump;
+    s->pos4 = dev->pos4;
+    s->nrm4 = dev->nrm4;
+    *dev = fk::DevBvh{};
+    s->bytes += 2 * nb + sizeof(uint32_t) * nn + 2 * cb;
+  } else {
+    up((void**)&s->node_lo, lo.data(), nb);
+    up((void**)&s->node_hi, hi.data(), nb);
+    up((void**)&s->node_jump, jump.data(), sizeof(uint32_t) * nn);
+    up((void**)&s->pos4, pos4, cb);
+    up((void**)&s->nrm4, nrm4, cb);
+  }
   up((void**)&s->wide, wide.data(), sizeof(float4) * wide.size());
   s->tree_wide[FK_TREE_REFERENCE] = s->wide;
   s->tree_count[FK_TREE_REFERENCE] = nw;
@@ -414,6 +438,88 @@ int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const fl
   }
   *out = s;
   return FK_OK;
+}
+
+// Flattened nodes of a device build, downloaded into the ABI's node layout.
+static int dev_nodes(fk_ctx* ctx, const fk::DevBvh& d, std::vector<fk_bvh_node>& nodes) {
+  const uint32_t nn = d.node_count;
+  std::vector<float4> lo(nn), hi(nn);
+  std::vector<uint32_t> jump(nn);
+  FK_CUDA(ctx, cudaMemcpyAsync(lo.data(), d.lo, sizeof(float4) * nn, cudaMemcpyDeviceToHost, ctx->stream));
+  FK_CUDA(ctx, cudaMemcpyAsync(hi.data(), d.hi, sizeof(float4) * nn, cudaMemcpyDeviceToHost, ctx->stream));
+  FK_CUDA(ctx, cudaMemcpyAsync(jump.data(), d.jump, sizeof(uint32_t) * nn, cudaMemcpyDeviceToHost, ctx->stream));
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  nodes.resize(nn);
+  for (uint32_t i = 0; i < nn; ++i) {
+    fk_bvh_node& n = nodes[i];
+    n.aabb_min[0] = lo[i].x;
+    n.aabb_min[1] = lo[i].y;
+    n.aabb_min[2] = lo[i].z;
+    n.aabb_max[0] = hi[i].x;
+    n.aabb_max[1] = hi[i].y;
+    n.aabb_max[2] = hi[i].z;
+    std::memcpy(&n.start, &lo[i].w, 4);
+    std::memcpy(&n.end, &hi[i].w, 4);
+    n.jump = jump[i];
+  }
+  return FK_OK;
+}
+
+static void dev_free(fk_ctx* ctx, fk::DevBvh& d) {
+  for (void* p : {(void*)d.lo, (void*)d.hi, (void*)d.jump, (void*)d.pos4, (void*)d.nrm4}) fk_dev_free(ctx, p);
+  d = fk::DevBvh{};
+}
+
+extern "C" {
+
+int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, const float* pos4, const float* nrm4,
+                    uint32_t nc, fk_scene** out) {
+  return scene_create(ctx, nodes, nn, pos4, nrm4, nc, nullptr, out);
+}
+
+int fk_bvh_build_flat(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, fk_bvh_node* nodes,
+                      uint32_t node_capacity, uint32_t* node_count, float* positions4, float* normals4) {
+  if (!ctx || !mesh || max_tris == 0 || !node_count)
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_bvh_build_flat: bad arguments");
+  fk::DevBvh d;
+  int rc = fk::build_bvh_device(ctx, mesh, max_tris, max_depth, &d);
+  if (rc != FK_OK) return rc;
+  *node_count = d.node_count;
+  std::vector<fk_bvh_node> v;
+  if (nodes || positions4 || normals4) {
+    if (nodes && node_capacity < d.node_count) {
+      dev_free(ctx, d);
+      return fk_fail(ctx, FK_ERR_INVALID, "fk_bvh_build_flat: node capacity below the node count");
+    }
+    if (nodes && (rc = dev_nodes(ctx, d, v)) == FK_OK) std::memcpy(nodes, v.data(), sizeof(fk_bvh_node) * v.size());
+    const size_t cb = sizeof(float4) * (size_t)d.corner_count;
+    if (rc == FK_OK && positions4 && cb &&
+        cudaMemcpyAsync(positions4, d.pos4, cb, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+      rc = fk_fail(ctx, FK_ERR_CUDA, "fk_bvh_build_flat: corner copy");
+    if (rc == FK_OK && normals4 && cb &&
+        cudaMemcpyAsync(normals4, d.nrm4, cb, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess)
+      rc = fk_fail(ctx, FK_ERR_CUDA, "fk_bvh_build_flat: corner copy");
+    if (rc == FK_OK && cudaStreamSynchronize(ctx->stream) != cudaSuccess)
+      rc = fk_fail(ctx, FK_ERR_CUDA, "fk_bvh_build_flat: sync");
+  }
+  dev_free(ctx, d);
+  return rc;
+}
+
+int fk_scene_build(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, fk_scene** out) {
+  if (!ctx || !mesh || !out || max_tris == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_build: bad arguments");
+  fk::DevBvh d;
+  int rc = fk::build_bvh_device(ctx, mesh, max_tris, max_depth, &d);
+  if (rc != FK_OK) return rc;
+  if (d.node_count == 0) {
+    dev_free(ctx, d);
+    return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_build: the mesh has no triangles");
+  }
+  std::vector<fk_bvh_node> v;
+  rc = dev_nodes(ctx, d, v);
+  if (rc == FK_OK) rc = scene_create(ctx, v.data(), d.node_count, nullptr, nullptr, d.corner_count, &d, out);
+  dev_free(ctx, d);  // nothing left after a successful adoption
+  return rc;
 }
 
 int fk_scene_free(fk_ctx* ctx, fk_scene* s) {

@@ -141,6 +141,22 @@ constexpr uint32_t kMaxOrderedDepth = 48;
 uint32_t build_sah_wide(const float4* lo, const float4* hi, const uint32_t* jump, uint32_t nn,
                         std::vector<float4>& wide);
 void collapse_wide4(const std::vector<float4>& wide, std::vector<float4>& wide4, uint32_t& n4, uint32_t& depth4);
+// BVH::createBinary + fillMeshData on the device (fk_bvh_dev.cu): the
+// flattened nodes (scene layout: lo / hi float4 with start / end bits, jump)
+// and corner arrays of fk_bvh_build + fk_bvh_flatten, bit for bit, in
+// library-owned device memory.
+struct DevBvh {
+  float4* lo = nullptr;
+  float4* hi = nullptr;
+  uint32_t* jump = nullptr;
+  float4* pos4 = nullptr;
+  float4* nrm4 = nullptr;
+  uint32_t node_count = 0, corner_count = 0, triangle_count = 0;
+};
+int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, DevBvh* out);
+// *ok: every coordinate of the n corners is below lim in magnitude.
+int corners_below(fk_ctx* ctx, const float4* p, uint32_t n, float lim, bool* ok);
+
 // The same tree built on the device (fk_sah.cu) from the scene's node boxes
 // and its leaves' flattened indices (ascending): *wide gets 4 (L - 1) float4
 // records, or stays null when the tree would be deeper than

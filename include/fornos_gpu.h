@@ -148,11 +148,21 @@ typedef struct fk_bvh_node {
  * arrays (positions / normals as 4 floats per corner, w = 0). */
 int fk_bvh_flatten_sizes(const fk_bvh* bvh, uint32_t* node_count, uint32_t* corner_count);
 int fk_bvh_flatten(const fk_bvh* bvh, const fk_mesh* mesh, fk_bvh_node* nodes, float* positions4, float* normals4);
+/* BVH::createBinary (Src/bvh.cpp:128-314) + fillMeshData
+ * (Src/meshmapping.cpp:62-125) built on the device: the nodes and corner
+ * arrays of fk_bvh_build + fk_bvh_flatten, bit for bit.  *node_count gets the
+ * node count (at most 2 x triangles - 1); nodes (capacity in entries),
+ * positions4 and normals4 (3 x triangles x 4 floats) may each be NULL. */
+int fk_bvh_build_flat(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, fk_bvh_node* nodes,
+                      uint32_t node_capacity, uint32_t* node_count, float* positions4, float* normals4);
 
 /* ------------------------------------------------------------ device scene */
 int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t node_count, const float* positions4,
                     const float* normals4, uint32_t corner_count, fk_scene** out);
 int fk_scene_free(fk_ctx* ctx, fk_scene* scene);
+/* fk_bvh_build_flat + fk_scene_upload without the round trip: the device-built
+ * nodes and corners become the scene's arrays. */
+int fk_scene_build(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, fk_scene** out);
 typedef struct fk_scene_info {
   uint32_t node_count;
   uint32_t corner_count;
