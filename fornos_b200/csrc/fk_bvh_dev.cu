@@ -675,48 +675,50 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
   // device inputs and work arrays
   const size_t F = nf ? nf : 1;
   const uint32_t max_tasks = nf / (kSmall + 1) + 1, max_chunks = nf / kChunk + max_tasks + 1;
-  const size_t parts[] = {sizeof(float) * mesh->positions.size() + 4,
-                          sizeof(float) * mesh->normals.size() + 4,
-                          sizeof(uint32_t) * mesh->vertices.size() + 4,
-                          sizeof(uint32_t) * mesh->triangles.size() + 4,
-                          4 * sizeof(float4) * F,  // pc, pm, plo, phi
-                          3 * sizeof(uint32_t) * F,  // perm, tmp, scratch
-                          sizeof(Frame) * F,
-                          sizeof(DNode) * 2 * F,
-                          4 * (size_t)kTaskWords * max_tasks + 4 * kBox,
-                          sizeof(Task) * max_tasks,
-                          sizeof(Split) * max_tasks,
-                          4 * (size_t)max_tasks * 2,  // node_left, task_b
-                          sizeof(Chunk) * max_chunks,
-                          4 * 3 * (size_t)max_chunks,  // chunk_left, offs
-                          64};
-  size_t bytes = 0;
-  for (size_t b : parts) bytes += (b + 255) & ~(size_t)255;
+  // work arrays, carved from one allocation; the size comes from the same
+  // carve sequence run over offsets
+  float* d_pos;
+  float* d_nrm;
+  uint32_t *d_verts, *d_tris, *perm, *tmp, *scratch, *acc, *d_node_left, *d_task_b, *d_chunk_left, *d_offs, *d_status;
+  float4 *pc, *pm, *plo, *phi;
+  Frame* frames;
+  DNode* dnodes;
+  Task* d_tasks;
+  Split* d_splits;
+  Chunk* d_chunks;
+  auto layout = [&](char* base) -> size_t {
+    char* p = base;
+    d_pos = carve<float>(p, mesh->positions.size() + 1);
+    d_nrm = carve<float>(p, mesh->normals.size() + 1);
+    d_verts = carve<uint32_t>(p, mesh->vertices.size() + 1);
+    d_tris = carve<uint32_t>(p, mesh->triangles.size() + 1);
+    pc = carve<float4>(p, F);
+    pm = carve<float4>(p, F);
+    plo = carve<float4>(p, F);
+    phi = carve<float4>(p, F);
+    perm = carve<uint32_t>(p, F);
+    tmp = carve<uint32_t>(p, F);
+    scratch = carve<uint32_t>(p, F);
+    frames = carve<Frame>(p, F);
+    dnodes = carve<DNode>(p, 2 * F);
+    acc = carve<uint32_t>(p, (size_t)kTaskWords * max_tasks + kBox);
+    d_tasks = carve<Task>(p, max_tasks);
+    d_splits = carve<Split>(p, max_tasks);
+    d_node_left = carve<uint32_t>(p, max_tasks);
+    d_task_b = carve<uint32_t>(p, max_tasks);
+    d_chunks = carve<Chunk>(p, max_chunks);
+    d_chunk_left = carve<uint32_t>(p, max_chunks);
+    d_offs = carve<uint32_t>(p, 2 * (size_t)max_chunks);
+    d_status = carve<uint32_t>(p, 1);
+    return (size_t)(p - base);
+  };
   char* base = nullptr;
-  if ((rc = fk_dev_alloc(ctx, (void**)&base, bytes)) != FK_OK) return rc;
-  char* p = base;
-  float* d_pos = carve<float>(p, mesh->positions.size() + 1);
-  float* d_nrm = carve<float>(p, mesh->normals.size() + 1);
-  uint32_t* d_verts = carve<uint32_t>(p, mesh->vertices.size() + 1);
-  uint32_t* d_tris = carve<uint32_t>(p, mesh->triangles.size() + 1);
-  float4* pc = carve<float4>(p, F);
-  float4* pm = carve<float4>(p, F);
-  float4* plo = carve<float4>(p, F);
-  float4* phi = carve<float4>(p, F);
-  uint32_t* perm = carve<uint32_t>(p, F);
-  uint32_t* tmp = carve<uint32_t>(p, F);
-  uint32_t* scratch = carve<uint32_t>(p, F);
-  Frame* frames = carve<Frame>(p, F);
-  DNode* dnodes = carve<DNode>(p, 2 * F);
-  uint32_t* acc = carve<uint32_t>(p, (size_t)kTaskWords * max_tasks + kBox);
-  Task* d_tasks = carve<Task>(p, max_tasks);
-  Split* d_splits = carve<Split>(p, max_tasks);
-  uint32_t* d_node_left = carve<uint32_t>(p, max_tasks);
-  uint32_t* d_task_b = carve<uint32_t>(p, max_tasks);
-  Chunk* d_chunks = carve<Chunk>(p, max_chunks);
-  uint32_t* d_chunk_left = carve<uint32_t>(p, max_chunks);
-  uint32_t* d_offs = carve<uint32_t>(p, 2 * (size_t)max_chunks);
-  uint32_t* d_status = carve<uint32_t>(p, 1);
+  {
+    char probe_base[1];
+    const size_t bytes = layout(probe_base);  // offsets only: nothing is written through these pointers
+    if ((rc = fk_dev_alloc(ctx, (void**)&base, bytes)) != FK_OK) return rc;
+    layout(base);
+  }
   auto done = [&](int code) {
     cudaStreamSynchronize(st);
     fk_dev_free(ctx, base);
