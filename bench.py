@@ -70,7 +70,7 @@ SCHEDULE = {"auto": 0, "static": 0x10, "dynamic": 0x20}
 # DRAM bytes (read + write) per hemisphere-kernel launch from ncu captures, by workload: plane250, one AO+BN
 # trace launch of 968,256 rays (profiles/hemi_trace_kernel_plane250.md); plane2048, the mean of two AO+BN chunk
 # launches of 134,217,728 rays each, 4.88 and 3.27 GB (profiles/hemi_trace_traffic_plane2048.md).
-NCU_TRAFFIC = {"plane250": 301.0e6, "plane2048": 4.08e9}
+NCU_TRAFFIC = {"plane250": 257.6e6, "plane2048": 4.08e9}
 
 
 def rays_per_texel(wl):
@@ -198,6 +198,13 @@ def run_fornos(args, wl, rank, world):
     stream.synchronize()
     raster_ms = e0.elapsed_time(e1)
     n = tmap.count
+    # the same scene from the mesh, BVH built on the device (fk_scene_build; informational)
+    api.Scene.build(ctx, prep.hm, 8, 8192).free()
+    ctx.sync()
+    t0 = time.perf_counter()
+    api.Scene.build(ctx, prep.hm, 8, 8192).free()
+    ctx.sync()
+    scene_build_ms = (time.perf_counter() - t0) * 1e3
     scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
     if args.tree == "reference":
         scene.set_tree(api.TREE_REFERENCE)
@@ -334,7 +341,7 @@ def run_fornos(args, wl, rank, world):
                    "rays_counted": "2 mapping + spp each for AO, bent normals, thickness (AO and bent normals "
                                    "share one traversal)",
                    "l2": "inputs larger than L2 (scene %.0f MB resident)" % (info["device_bytes"] / 1e6),
-                   "bvh_build_s": round(prep.bvh_s, 3), "raster_ms": round(raster_ms, 3),
+                   "bvh_build_s": round(prep.bvh_s, 3), "scene_build_device_ms": round(scene_build_ms, 1), "raster_ms": round(raster_ms, 3),
                    "parallelism": "replicas" if world > 1 else "single"},
         "e2e": {"value": round(rays_all / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
                 "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

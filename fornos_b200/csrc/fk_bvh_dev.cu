@@ -27,7 +27,7 @@
 namespace fk {
 namespace {
 
-constexpr uint32_t kSmall = 512;   // subtrees of at most this many triangles: one thread each
+constexpr uint32_t kSmall = 128;   // subtrees of at most this many triangles: one thread each
 constexpr uint32_t kChunk = 4096;  // triangles per block in the level passes
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
@@ -164,7 +164,7 @@ __device__ __forceinline__ float comp(const float4& v, int a) { return a == 0 ? 
 // ------------------------------------------------------------ per triangle
 // Src/bvh.cpp:139 / :227 centroids and the triangle's box (the fold of its
 // corners, as addPoint of the three corners gives it).
-__global__ void pre_kernel(uint32_t nf, const float* __restrict__ pos, const uint32_t* __restrict__ verts,
+__global__ void bvh_pre_kernel(uint32_t nf, const float* __restrict__ pos, const uint32_t* __restrict__ verts,
                            const uint32_t* __restrict__ tris, float4* pc, float4* pm, float4* plo, float4* phi) {
   const uint32_t f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
@@ -189,7 +189,7 @@ __global__ void pre_kernel(uint32_t nf, const float* __restrict__ pos, const uin
 }
 
 // Root box over every position (Src/bvh.cpp:287-297), referenced or not.
-__global__ void __launch_bounds__(kThreads) points_kernel(const float* __restrict__ pos, uint32_t np, uint32_t* w) {
+__global__ void __launch_bounds__(kThreads) bvh_points_kernel(const float* __restrict__ pos, uint32_t np, uint32_t* w) {
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
   for (uint32_t i = blockIdx.x * kThreads + threadIdx.x; i < np; i += gridDim.x * kThreads)
     for (int q = 0; q < 3; ++q) {
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kThreads) points_kernel(const float* __restric
 }
 
 // ------------------------------------------------------------ level passes
-__global__ void init_kernel(uint32_t* acc, uint32_t nt) {
+__global__ void bvh_init_kernel(uint32_t* acc, uint32_t nt) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   uint32_t* w = acc + (size_t)t * kTaskWords;
@@ -214,7 +214,7 @@ __global__ void init_kernel(uint32_t* acc, uint32_t nt) {
   box_init(w + kRightOff);
 }
 
-__global__ void __launch_bounds__(kThreads) centroid_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
+__global__ void __launch_bounds__(kThreads) bvh_centroid_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
                                                             const float4* __restrict__ pc, uint32_t* acc) {
   const Chunk c = chunks[blockIdx.x];
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
@@ -228,7 +228,7 @@ __global__ void __launch_bounds__(kThreads) centroid_kernel(const Chunk* chunks,
   fold_block(lo, hi, acc + (size_t)c.task * kTaskWords);
 }
 
-__global__ void __launch_bounds__(kThreads) bucket_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
+__global__ void __launch_bounds__(kThreads) bvh_bucket_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
                                                           const float4* __restrict__ pc,
                                                           const float4* __restrict__ plo,
                                                           const float4* __restrict__ phi, uint32_t* acc) {
@@ -268,7 +268,7 @@ __global__ void __launch_bounds__(kThreads) bucket_kernel(const Chunk* chunks, c
   }
 }
 
-__global__ void choose_kernel(const Task* tasks, uint32_t nt, const uint32_t* acc, Split* splits) {
+__global__ void bvh_choose_kernel(const Task* tasks, uint32_t nt, const uint32_t* acc, Split* splits) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nt) return;
   const uint32_t* w = acc + (size_t)t * kTaskWords;
@@ -289,7 +289,7 @@ __global__ void choose_kernel(const Task* tasks, uint32_t nt, const uint32_t* ac
 }
 
 // Left / right boxes and the left count per chunk (Src/bvh.cpp:222-247).
-__global__ void __launch_bounds__(kThreads) side_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
+__global__ void __launch_bounds__(kThreads) bvh_side_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
                                                         const float4* __restrict__ pm,
                                                         const float4* __restrict__ plo,
                                                         const float4* __restrict__ phi, const Split* splits,
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(kThreads) side_kernel(const Chunk* chunks, con
 // Stable partition of the chunk into `out` (offs: this chunk's start on the
 // left and on the right side of its node); chunks of nodes that stay leaves
 // are not launched.
-__global__ void __launch_bounds__(kThreads) scatter_kernel(const Chunk* chunks, const uint32_t* node_left,
+__global__ void __launch_bounds__(kThreads) bvh_scatter_kernel(const Chunk* chunks, const uint32_t* node_left,
                                                            const uint32_t* __restrict__ perm, uint32_t* out,
                                                            const float4* __restrict__ pm, const Split* splits,
                                                            const uint32_t* offs, const uint32_t* task_b) {
@@ -372,7 +372,7 @@ __global__ void __launch_bounds__(kThreads) scatter_kernel(const Chunk* chunks, 
   }
 }
 
-__global__ void copy_back_kernel(const Chunk* chunks, const uint32_t* __restrict__ from, uint32_t* to) {
+__global__ void bvh_copy_back_kernel(const Chunk* chunks, const uint32_t* __restrict__ from, uint32_t* to) {
   const Chunk c = chunks[blockIdx.x];
   for (uint32_t i = c.b + threadIdx.x; i < c.e; i += blockDim.x) to[i] = from[i];
 }
@@ -387,7 +387,7 @@ __device__ __forceinline__ void set_box(DNode& n, const float lo[3], const float
 
 // status: 1 = a subtree ran out of its node slots or stack (cannot happen:
 // a subtree over n triangles has at most 2 n - 1 nodes and depth n).
-__global__ void __launch_bounds__(64) small_kernel(const SmallTask* tasks, uint32_t ns, uint32_t* perm,
+__global__ void __launch_bounds__(64) bvh_small_kernel(const SmallTask* tasks, uint32_t ns, uint32_t* perm,
                                                    uint32_t* scratch, Frame* frames, const float4* __restrict__ pc,
                                                    const float4* __restrict__ pm, const float4* __restrict__ plo,
                                                    const float4* __restrict__ phi, DNode* nodes, uint32_t max_tris,
@@ -522,7 +522,7 @@ __global__ void __launch_bounds__(64) small_kernel(const SmallTask* tasks, uint3
   }
 }
 
-__global__ void small_roots_kernel(const SmallTask* tasks, uint32_t ns, const DNode* nodes, DNode* roots) {
+__global__ void bvh_small_roots_kernel(const SmallTask* tasks, uint32_t ns, const DNode* nodes, DNode* roots) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k < ns) roots[k] = nodes[2 * tasks[k].b];
 }
@@ -530,7 +530,7 @@ __global__ void small_roots_kernel(const SmallTask* tasks, uint32_t ns, const DN
 // Flattened records of one subtree, its root at preorder index tasks[k].pre:
 // aabbMin = c - s, aabbMax = c + s, start / end corners, jump (Src/meshmapping.cpp:62-125).
 // status bit 2: a preorder index fell outside the node arrays (not written).
-__global__ void __launch_bounds__(64) small_flatten_kernel(const SmallTask* tasks, uint32_t ns, const DNode* nodes,
+__global__ void __launch_bounds__(64) bvh_small_flatten_kernel(const SmallTask* tasks, uint32_t ns, const DNode* nodes,
                                                            uint32_t* stack, float4* lo, float4* hi,
                                                            uint32_t* jump, uint32_t nn, uint32_t* status) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -574,7 +574,7 @@ struct FlatRec {
   float4 lo, hi;
   uint32_t pre, jump, pad[2];
 };
-__global__ void host_records_kernel(const FlatRec* recs, uint32_t n, float4* lo, float4* hi, uint32_t* jump) {
+__global__ void bvh_host_records_kernel(const FlatRec* recs, uint32_t n, float4* lo, float4* hi, uint32_t* jump) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
   const FlatRec r = recs[k];
@@ -585,7 +585,7 @@ __global__ void host_records_kernel(const FlatRec* recs, uint32_t n, float4* lo,
 
 // Corners in leaf order (Src/meshmapping.cpp:94-109): position and normal of
 // each corner of the i-th triangle of the final order, w = 0.
-__global__ void corners_kernel(uint32_t nf, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ tris,
+__global__ void bvh_corners_kernel(uint32_t nf, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ tris,
                                const uint32_t* __restrict__ verts, const float* __restrict__ pos,
                                const float* __restrict__ nrm, float4* pos4, float4* nrm4) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -602,7 +602,7 @@ __global__ void corners_kernel(uint32_t nf, const uint32_t* __restrict__ perm, c
 }
 
 // Whether every corner coordinate is below `lim` in magnitude (a NaN is not).
-__global__ void corners_below_kernel(const float4* __restrict__ p, uint32_t n, float lim, uint32_t* bad) {
+__global__ void bvh_corners_below_kernel(const float4* __restrict__ p, uint32_t n, float lim, uint32_t* bad) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const float4 v = p[i];
     if (!(fabsf(v.x) < lim && fabsf(v.y) < lim && fabsf(v.z) < lim)) {
@@ -646,7 +646,7 @@ int corners_below(fk_ctx* ctx, const float4* p, uint32_t n, float lim, bool* ok)
   uint32_t h = 0;
   cudaError_t e = cudaMemsetAsync(bad, 0, 4, ctx->stream);
   if (e == cudaSuccess) {
-    corners_below_kernel<<<std::min<uint32_t>((n + 255) / 256, (uint32_t)ctx->sm_count * 8), 256, 0, ctx->stream>>>(
+    bvh_corners_below_kernel<<<std::min<uint32_t>((n + 255) / 256, (uint32_t)ctx->sm_count * 8), 256, 0, ctx->stream>>>(
         p, n, lim, bad);
     rc = fk_after_launch(ctx, "corner bound");
     if (rc == FK_OK) e = cudaMemcpyAsync(&h, bad, 4, cudaMemcpyDeviceToHost, ctx->stream);
@@ -742,7 +742,7 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
   FK_BVH_TRY(up(d_tris, mesh->triangles.data(), sizeof(uint32_t) * mesh->triangles.size()));
   FK_BVH_TRY(cudaMemsetAsync(d_status, 0, 4, st));
   if (nf) {
-    pre_kernel<<<(nf + 255) / 256, 256, 0, st>>>(nf, d_pos, d_verts, d_tris, pc, pm, plo, phi);
+    bvh_pre_kernel<<<(nf + 255) / 256, 256, 0, st>>>(nf, d_pos, d_verts, d_tris, pc, pm, plo, phi);
     FK_BVH_LAUNCHED("bvh pre");
   }
   {  // identity order
@@ -757,7 +757,7 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
     box_init(w);
     FK_BVH_TRY(up(root_w, w, sizeof(w)));
     if (np) {
-      points_kernel<<<std::min<uint32_t>((np + kThreads - 1) / kThreads, (uint32_t)ctx->sm_count * 4), kThreads, 0,
+      bvh_points_kernel<<<std::min<uint32_t>((np + kThreads - 1) / kThreads, (uint32_t)ctx->sm_count * 4), kThreads, 0,
                       st>>>(d_pos, np, root_w);
       FK_BVH_LAUNCHED("bvh root box");
     }
@@ -812,15 +812,15 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
       return done(fk_fail(ctx, FK_ERR_DEVICE, "device BVH build: task overflow"));
     FK_BVH_TRY(up(d_tasks, htasks.data(), sizeof(Task) * nt));
     FK_BVH_TRY(up(d_chunks, hch.data(), sizeof(Chunk) * nc));
-    init_kernel<<<(nt + 127) / 128, 128, 0, st>>>(acc, nt);
+    bvh_init_kernel<<<(nt + 127) / 128, 128, 0, st>>>(acc, nt);
     FK_BVH_LAUNCHED("bvh init");
-    centroid_kernel<<<nc, kThreads, 0, st>>>(d_chunks, perm, pc, acc);
+    bvh_centroid_kernel<<<nc, kThreads, 0, st>>>(d_chunks, perm, pc, acc);
     FK_BVH_LAUNCHED("bvh centroids");
-    bucket_kernel<<<nc, kThreads, 0, st>>>(d_chunks, perm, pc, plo, phi, acc);
+    bvh_bucket_kernel<<<nc, kThreads, 0, st>>>(d_chunks, perm, pc, plo, phi, acc);
     FK_BVH_LAUNCHED("bvh buckets");
-    choose_kernel<<<(nt + 63) / 64, 64, 0, st>>>(d_tasks, nt, acc, d_splits);
+    bvh_choose_kernel<<<(nt + 63) / 64, 64, 0, st>>>(d_tasks, nt, acc, d_splits);
     FK_BVH_LAUNCHED("bvh choose");
-    side_kernel<<<nc, kThreads, 0, st>>>(d_chunks, perm, pm, plo, phi, d_splits, acc, d_chunk_left);
+    bvh_side_kernel<<<nc, kThreads, 0, st>>>(d_chunks, perm, pm, plo, phi, d_splits, acc, d_chunk_left);
     FK_BVH_LAUNCHED("bvh sides");
     hleft.resize(nc);
     hside.resize((size_t)nt * kTaskWords);
@@ -854,9 +854,9 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
       FK_BVH_TRY(up(d_offs, split_offs.data(), 4 * (size_t)ns * 2));
       FK_BVH_TRY(up(d_node_left, hnode_left.data(), 4 * (size_t)nt));
       FK_BVH_TRY(up(d_task_b, htask_b.data(), 4 * (size_t)nt));
-      scatter_kernel<<<ns, kThreads, 0, st>>>(d_chunks, d_node_left, perm, tmp, pm, d_splits, d_offs, d_task_b);
+      bvh_scatter_kernel<<<ns, kThreads, 0, st>>>(d_chunks, d_node_left, perm, tmp, pm, d_splits, d_offs, d_task_b);
       FK_BVH_LAUNCHED("bvh scatter");
-      copy_back_kernel<<<ns, kThreads, 0, st>>>(d_chunks, tmp, perm);
+      bvh_copy_back_kernel<<<ns, kThreads, 0, st>>>(d_chunks, tmp, perm);
       FK_BVH_LAUNCHED("bvh copy back");
     }
     std::vector<Level> next;
@@ -897,10 +897,10 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
       return done2(rc);
     cudaError_t e = up(d_small, small.data(), sizeof(SmallTask) * nsm);
     if (e != cudaSuccess) return done2(fk_cuda_fail(ctx, e, "device BVH build: subtrees"));
-    small_kernel<<<(nsm + 63) / 64, 64, 0, st>>>(d_small, nsm, perm, scratch, frames, pc, pm, plo, phi, dnodes,
+    bvh_small_kernel<<<(nsm + 63) / 64, 64, 0, st>>>(d_small, nsm, perm, scratch, frames, pc, pm, plo, phi, dnodes,
                                                 max_tris, max_depth, d_status);
     if ((rc = fk_after_launch(ctx, "bvh subtrees")) != FK_OK) return done2(rc);
-    small_roots_kernel<<<(nsm + 127) / 128, 128, 0, st>>>(d_small, nsm, dnodes, d_roots);
+    bvh_small_roots_kernel<<<(nsm + 127) / 128, 128, 0, st>>>(d_small, nsm, dnodes, d_roots);
     if ((rc = fk_after_launch(ctx, "bvh subtree roots")) != FK_OK) return done2(rc);
     e = cudaMemcpyAsync(roots.data(), d_roots, sizeof(DNode) * nsm, cudaMemcpyDeviceToHost, st);
     uint32_t status = 0;
@@ -999,7 +999,7 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
     }
     cudaError_t e = up(d_recs, recs.data(), sizeof(FlatRec) * recs.size());
     if (e == cudaSuccess) {
-      host_records_kernel<<<((uint32_t)recs.size() + 127) / 128, 128, 0, st>>>(d_recs, (uint32_t)recs.size(), o.lo,
+      bvh_host_records_kernel<<<((uint32_t)recs.size() + 127) / 128, 128, 0, st>>>(d_recs, (uint32_t)recs.size(), o.lo,
                                                                                o.hi, o.jump);
       rc = fk_after_launch(ctx, "bvh top records");
     } else {
@@ -1010,7 +1010,7 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
     cudaError_t e = up(d_small, small.data(), sizeof(SmallTask) * nsm);  // with their preorder indices
     if (e == cudaSuccess) {
       // the subtree stacks are free again: their frames hold the walk's (slot, preorder) pairs
-      small_flatten_kernel<<<(nsm + 63) / 64, 64, 0, st>>>(d_small, nsm, dnodes, reinterpret_cast<uint32_t*>(frames),
+      bvh_small_flatten_kernel<<<(nsm + 63) / 64, 64, 0, st>>>(d_small, nsm, dnodes, reinterpret_cast<uint32_t*>(frames),
                                                             o.lo, o.hi, o.jump, nn, d_status);
       rc = fk_after_launch(ctx, "bvh flatten");
     } else {
@@ -1018,7 +1018,7 @@ int build_bvh_device(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32
     }
   }
   if (rc == FK_OK && nf) {
-    corners_kernel<<<(nf + 255) / 256, 256, 0, st>>>(nf, perm, d_tris, d_verts, d_pos, d_nrm, o.pos4, o.nrm4);
+    bvh_corners_kernel<<<(nf + 255) / 256, 256, 0, st>>>(nf, perm, d_tris, d_verts, d_pos, d_nrm, o.pos4, o.nrm4);
     rc = fk_after_launch(ctx, "bvh corners");
   }
   if (rc == FK_OK) {

@@ -184,7 +184,7 @@ __device__ __forceinline__ void centre_bounds(const uint32_t* acc, float cmin[3]
 }
 
 // ------------------------------------------------------------ level passes
-__global__ void init_kernel(uint32_t* acc, uint32_t* bins, uint32_t nt) {
+__global__ void sah_init_kernel(uint32_t* acc, uint32_t* bins, uint32_t nt) {
   const size_t na = (size_t)nt * kAccWords, nb = (size_t)nt * kNodeBins;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < na + nb; i += (size_t)gridDim.x * blockDim.x) {
     if (i < na) acc[i] = acc_is_min((int)(i % kAccWords)) ? 0xffffffffu : 0u;
@@ -192,7 +192,7 @@ __global__ void init_kernel(uint32_t* acc, uint32_t* bins, uint32_t nt) {
   }
 }
 
-__global__ void __launch_bounds__(kThreads) bounds_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
+__global__ void __launch_bounds__(kThreads) sah_bounds_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
                                                           const float4* __restrict__ lo, const float4* __restrict__ hi,
                                                           uint32_t* acc) {
   const Chunk c = chunks[blockIdx.x];
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(kThreads) bounds_kernel(const Chunk* chunks, c
   }
 }
 
-__global__ void __launch_bounds__(kThreads) bin_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
+__global__ void __launch_bounds__(kThreads) sah_bin_kernel(const Chunk* chunks, const uint32_t* __restrict__ perm,
                                                        const float4* __restrict__ lo, const float4* __restrict__ hi,
                                                        const uint32_t* acc, uint32_t* bins) {
   __shared__ uint32_t sb[kNodeBins];
@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kThreads) bin_kernel(const Chunk* chunks, cons
   }
 }
 
-__global__ void __launch_bounds__(kThreads) split_kernel(const Task* tasks, uint32_t nt, const uint32_t* acc,
+__global__ void __launch_bounds__(kThreads) sah_split_kernel(const Task* tasks, uint32_t nt, const uint32_t* acc,
                                                          const uint32_t* bins, Split* splits, float4* wide) {
   const uint32_t t = (blockIdx.x * kThreads + threadIdx.x) >> 5;
   if (t >= nt) return;  // whole warps
@@ -296,7 +296,7 @@ __device__ __forceinline__ bool goes_left(const Split& s, uint32_t pos, const fl
   return bin_of(centre(comp(l, s.axis), comp(h, s.axis)), s.cmin, s.scale) <= s.bin;
 }
 
-__global__ void __launch_bounds__(kThreads) count_kernel(const Chunk* chunks, const Task* tasks,
+__global__ void __launch_bounds__(kThreads) sah_count_kernel(const Chunk* chunks, const Task* tasks,
                                                          const uint32_t* __restrict__ perm,
                                                          const float4* __restrict__ lo, const float4* __restrict__ hi,
                                                          const Split* splits, uint32_t* chunk_left) {
@@ -318,7 +318,7 @@ __global__ void __launch_bounds__(kThreads) count_kernel(const Chunk* chunks, co
 
 // offs[2 c], offs[2 c + 1]: leaves of the chunk's node that earlier chunks
 // send left / right.
-__global__ void __launch_bounds__(kThreads) scatter_kernel(const Chunk* chunks, const Task* tasks,
+__global__ void __launch_bounds__(kThreads) sah_scatter_kernel(const Chunk* chunks, const Task* tasks,
                                                            const uint32_t* __restrict__ perm_in, uint32_t* perm_out,
                                                            const float4* __restrict__ lo,
                                                            const float4* __restrict__ hi, const Split* splits,
@@ -370,7 +370,7 @@ struct WarpSmem {
 constexpr size_t kSmallSmem = sizeof(WarpSmem) * kSmallWarps;
 
 // status bits: 1 = a partition disagreed with its bins, 2 = stack overflow
-__global__ void __launch_bounds__(kSmallWarps * 32) small_kernel(const Task* tasks, uint32_t ns,
+__global__ void __launch_bounds__(kSmallWarps * 32) sah_small_kernel(const Task* tasks, uint32_t ns,
                                                                  const uint32_t* perm0, const uint32_t* perm1,
                                                                  const float4* __restrict__ lo,
                                                                  const float4* __restrict__ hi, float4* wide,
@@ -608,15 +608,15 @@ int build_sah_device(fk_ctx* ctx, const float4* lo, const float4* hi, const std:
     FK_SAH_TRY(cudaMemcpyAsync(chunks, hchunks.data(), sizeof(Chunk) * nc, cudaMemcpyHostToDevice, st));
     const uint32_t init_blocks = std::min<uint32_t>((uint32_t)(((size_t)nt * (kAccWords + kNodeBins) + kThreads - 1) / kThreads),
                                                     (uint32_t)ctx->sm_count * 8);
-    init_kernel<<<init_blocks, kThreads, 0, st>>>(acc, bins, nt);
+    sah_init_kernel<<<init_blocks, kThreads, 0, st>>>(acc, bins, nt);
     if ((rc = fk_after_launch(ctx, "sah init")) != FK_OK) return fail(rc);
-    bounds_kernel<<<nc, kThreads, 0, st>>>(chunks, perm[src], lo, hi, acc);
+    sah_bounds_kernel<<<nc, kThreads, 0, st>>>(chunks, perm[src], lo, hi, acc);
     if ((rc = fk_after_launch(ctx, "sah bounds")) != FK_OK) return fail(rc);
-    bin_kernel<<<nc, kThreads, 0, st>>>(chunks, perm[src], lo, hi, acc, bins);
+    sah_bin_kernel<<<nc, kThreads, 0, st>>>(chunks, perm[src], lo, hi, acc, bins);
     if ((rc = fk_after_launch(ctx, "sah bins")) != FK_OK) return fail(rc);
-    split_kernel<<<(nt * 32 + kThreads - 1) / kThreads, kThreads, 0, st>>>(tasks, nt, acc, bins, splits, wide);
+    sah_split_kernel<<<(nt * 32 + kThreads - 1) / kThreads, kThreads, 0, st>>>(tasks, nt, acc, bins, splits, wide);
     if ((rc = fk_after_launch(ctx, "sah split")) != FK_OK) return fail(rc);
-    count_kernel<<<nc, kThreads, 0, st>>>(chunks, tasks, perm[src], lo, hi, splits, chunk_left);
+    sah_count_kernel<<<nc, kThreads, 0, st>>>(chunks, tasks, perm[src], lo, hi, splits, chunk_left);
     if ((rc = fk_after_launch(ctx, "sah count")) != FK_OK) return fail(rc);
     hsplits.resize(nt);
     hleft.resize(nc);
@@ -641,7 +641,7 @@ int build_sah_device(fk_ctx* ctx, const float4* lo, const float4* hi, const std:
       if (total_left) return fail(fk_fail(ctx, FK_ERR_DEVICE, "surface-area build: partition disagrees with bins"));
     }
     FK_SAH_TRY(cudaMemcpyAsync(offs, hoffs.data(), 8 * (size_t)nc, cudaMemcpyHostToDevice, st));
-    scatter_kernel<<<nc, kThreads, 0, st>>>(chunks, tasks, perm[src], perm[src ^ 1], lo, hi, splits, offs);
+    sah_scatter_kernel<<<nc, kThreads, 0, st>>>(chunks, tasks, perm[src], perm[src ^ 1], lo, hi, splits, offs);
     if ((rc = fk_after_launch(ctx, "sah scatter")) != FK_OK) return fail(rc);
     std::vector<Task> next;
     for (uint32_t t = 0; t < nt; ++t) {
@@ -661,7 +661,7 @@ int build_sah_device(fk_ctx* ctx, const float4* lo, const float4* hi, const std:
   if (rc != FK_OK) return fail(rc);
   cudaError_t e = cudaMemcpyAsync(dsmall, small.data(), sizeof(Task) * small.size(), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem);
+    e = cudaFuncSetAttribute(sah_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSmallSmem);
   if (e != cudaSuccess) {
     fk_dev_free(ctx, dsmall);
     return fail(fk_cuda_fail(ctx, e, "surface-area build: small subtrees"));
@@ -669,7 +669,7 @@ int build_sah_device(fk_ctx* ctx, const float4* lo, const float4* hi, const std:
   const uint32_t ns = (uint32_t)small.size();
   const uint32_t blocks = std::max<uint32_t>(1, std::min<uint32_t>((ns + kSmallWarps - 1) / kSmallWarps,
                                                                     (uint32_t)ctx->sm_count * 16));
-  small_kernel<<<blocks, kSmallWarps * 32, kSmallSmem, st>>>(dsmall, ns, perm[0], perm[1], lo, hi, wide, words,
+  sah_small_kernel<<<blocks, kSmallWarps * 32, kSmallSmem, st>>>(dsmall, ns, perm[0], perm[1], lo, hi, wide, words,
                                                               words + 1);
   rc = fk_after_launch(ctx, "sah small subtrees");
   uint32_t hw[2] = {0, 0};
