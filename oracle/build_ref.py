@@ -13,6 +13,14 @@ reference tree (default /root/reference, override with FORNOS_REF_ROOT):
                                            file needs MSVC-only overloads);
   * 3rdParty/glad/glad.c                   GL entry-point table the above refer
                                            to (never called: no GL context);
+  * Src/image.cpp, 3rdParty/tinyexr/tinyexr.cc
+                                           the image export (PNG / TGA through
+                                           stb_image_write, EXR through tinyexr),
+                                           with its exportNormalImage renamed
+                                           ref_exportNormalImage: CompressedMapUV's
+                                           constructor calls that name for a
+                                           debug file (Src/compute.cpp:413-415),
+                                           which the driver keeps a no-op;
   * Shaders/*.comp                         rewritten on the fly to C++ (buffer and
                                            uniform declarations become thread-
                                            local globals,
@@ -144,8 +152,18 @@ def main():
          os.path.join(REF, "3rdParty", "glad", "glad.c"), "-o", o])
     objs.append(o)
 
+    o = os.path.join(OBJ, "image.o")
+    run(CXX + shim + inc + ["-I" + os.path.join(REF, "3rdParty", "tinyexr"),
+                            "-DexportNormalImage=ref_exportNormalImage", "-c", os.path.join(src, "image.cpp"), "-o", o])
+    objs.append(o)
+
+    o = os.path.join(OBJ, "tinyexr.o")
+    run(CXX + ["-c", os.path.join(REF, "3rdParty", "tinyexr", "tinyexr.cc"), "-o", o])
+    objs.append(o)
+
     o = os.path.join(OBJ, "host_driver.o")
-    run(CXX + shim + inc + ["-c", os.path.join(HERE, "ref_host_driver.cpp"), "-o", o])
+    run(CXX + shim + inc + ["-I" + os.path.join(REF, "3rdParty", "tinyexr"),
+                            "-c", os.path.join(HERE, "ref_host_driver.cpp"), "-o", o])
     objs.append(o)
 
     tu = "#include \"ref_glsl.h\"\n"

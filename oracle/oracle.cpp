@@ -28,6 +28,7 @@
 // Src/math.h and Shaders/*.comp) compiled by oracle/build_ref.py into oracle/_ref,
 // and by the committed fixtures in tests/golden/ generated from that build.
 
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
@@ -970,6 +971,138 @@ int orc_tangent_transform(const float* n3, const float* t3, const float* b3, uin
     F3 d1 = mk(T.z * N.y - T.y * N.z, T.x * N.z - N.x * T.z, N.x * T.y - T.x * N.y);
     F3 d2 = mk(T.y * B.z - T.z * B.y, T.z * B.x - T.x * B.z, T.x * B.y - T.y * B.x);
     st3(io3 + 3 * (size_t)i, normalize(mk(dot(v, d0), dot(v, d1), dot(v, d2))));
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------- export
+// Src/image.cpp:22-405: compressed texel values scattered into a W x H image
+// (rows flipped: texel (x, y) lands in row h - y - 1), quantized to RGB8 or
+// kept as float, and, for RGB8, dilated.  dilateRGB runs its pixels in row
+// order; this restatement keeps that order, so a source centre that is itself
+// an uncovered pixel gives the value it has at that point of the scan.
+
+// (uint8_t) of a float as x86-64 code converts it: truncation to int32
+// (0x80000000 for NaN and out-of-range values), low byte kept.
+static inline uint8_t u8_of(float v) {
+  if (!(v > -2147483648.0f && v < 2147483648.0f)) return 0;
+  return (uint8_t)(int32_t)v;
+}
+
+// dilateRGB (Src/image.cpp:127-182) on an RGB8 image in file row order.
+static void dilate_rgb(uint8_t* data, int w, int h, const std::vector<uint8_t>& valid, int max_dist) {
+  static const int off[8][2] = {{1, 0}, {-1, 0}, {0, 1}, {0, -1}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+  for (int y = 0; y < h; ++y)
+    for (int x = 0; x < w; ++x) {
+      if (valid[x + (size_t)y * w]) continue;
+      bool filled = false;
+      for (int dist = 1; dist < max_dist && !filled; ++dist)
+        for (int k = 0; k < 8; ++k) {
+          const int cx = x + off[k][0] * dist, cy = y + off[k][1] * dist;
+          if (!(cx > 0 && cy > 0 && cx < w - 1 && cy < h - 1)) continue;
+          bool ok = true;
+          for (int q = 0; q < 8 && ok; ++q) ok = valid[(cx + off[q][0]) + (size_t)(cy + off[q][1]) * w] != 0;
+          if (!ok) continue;
+          const size_t src = ((size_t)(h - cy - 1) * w + cx) * 3, dst = ((size_t)(h - y - 1) * w + x) * 3;
+          data[dst] = data[src];
+          data[dst + 1] = data[src + 1];
+          data[dst + 2] = data[src + 2];
+          filled = true;
+          break;
+        }
+    }
+}
+
+// exportFloatImage (Src/image.cpp:188-297).  rgb8 != 0: the PNG / TGA path
+// (out w x h x 3 bytes, dilated when dilate > 0); else the EXR path (out w x h
+// floats).  minmax gets the range it used.
+int orc_export_float(uint32_t w, uint32_t h, uint32_t count, const uint32_t* idx, const float* data, float flo,
+                     float fhi, int normalize, int dilate, int rgb8, void* out, float* minmax) {
+  float mn = FLT_MAX, mx = -FLT_MAX;
+  for (uint32_t i = 0; i < count; ++i) {
+    mn = std::fminf(mn, data[i]);
+    mx = std::fmaxf(mx, data[i]);
+  }
+  const bool filter = fhi > flo;
+  if (filter) {
+    mn = std::fmaxf(mn, flo);
+    mx = std::fminf(mx, fhi);
+  }
+  minmax[0] = mn;
+  minmax[1] = mx;
+  float scale = 1.0f, bias = 0.0f;
+  if (normalize && mn != FLT_MAX && mx != -FLT_MAX) {
+    scale = 1.0f / (mx - mn);
+    bias = -mn * scale;
+  }
+  if (rgb8) {
+    uint8_t* rgb = (uint8_t*)out;
+    std::memset(rgb, 0, (size_t)w * h * 3);
+    for (uint32_t i = 0; i < count; ++i) {
+      const float d = data[i];
+      const float df = filter && (d < flo || d > fhi) ? 0 : d;
+      const float t = df * scale + bias;
+      const uint8_t c = u8_of(std::min(std::max(t, 0.0f), 1.0f) * 255.0f);
+      const size_t x = idx[i] % w, y = idx[i] / w, p = ((h - y - 1) * w + x) * 3;
+      rgb[p] = rgb[p + 1] = rgb[p + 2] = c;
+    }
+    if (dilate > 0) {
+      std::vector<uint8_t> valid((size_t)w * h, 0);
+      for (uint32_t i = 0; i < count; ++i) valid[idx[i]] = 1;
+      dilate_rgb(rgb, (int)w, (int)h, valid, dilate);
+    }
+  } else {
+    float* f = (float*)out;
+    std::memset(f, 0, sizeof(float) * (size_t)w * h);
+    for (uint32_t i = 0; i < count; ++i) {
+      const float d = data[i];
+      const float df = filter ? std::fminf(std::fmaxf(d, flo), fhi) : d;
+      const float t = normalize ? df * scale + bias : df;
+      const size_t x = idx[i] % w, y = idx[i] / w;
+      f[(h - y - 1) * w + x] = t;
+    }
+  }
+  return 0;
+}
+
+// exportNormalImage's PNG / TGA path (Src/image.cpp:358-393): n * 0.5 + 0.5
+// to bytes, dilated when dilate > 0 over the pixels whose bytes are not all
+// zero.  The valid table uses y = index / h as the reference does (the same as
+// index / w for square maps); indices whose row would fall outside the image
+// are left invalid.
+int orc_export_normal(uint32_t w, uint32_t h, uint32_t count, const uint32_t* idx, const float* data3, int dilate,
+                      uint8_t* rgb) {
+  std::memset(rgb, 0, (size_t)w * h * 3);
+  for (uint32_t i = 0; i < count; ++i) {
+    const float nx = data3[3 * (size_t)i] * 0.5f + 0.5f, ny = data3[3 * (size_t)i + 1] * 0.5f + 0.5f,
+                nz = data3[3 * (size_t)i + 2] * 0.5f + 0.5f;
+    const size_t x = idx[i] % w, y = idx[i] / w, p = ((h - y - 1) * w + x) * 3;
+    rgb[p] = u8_of(nx * 255.0f);
+    rgb[p + 1] = u8_of(ny * 255.0f);
+    rgb[p + 2] = u8_of(nz * 255.0f);
+  }
+  if (dilate > 0) {
+    std::vector<uint8_t> valid((size_t)w * h, 0);
+    for (uint32_t i = 0; i < count; ++i) {
+      const size_t x = idx[i] % w, y = idx[i] / h;
+      if (y >= h) continue;
+      const size_t p = ((h - y - 1) * w + x) * 3;
+      valid[idx[i]] = (rgb[p] != 0) | (rgb[p + 1] != 0) | (rgb[p + 2] != 0);
+    }
+    dilate_rgb(rgb, (int)w, (int)h, valid, dilate);
+  }
+  return 0;
+}
+
+// exportVectorImage (Src/image.cpp:299-356): three float planes in file row
+// order, plane 0 = z, 1 = y, 2 = x (channels B, G, R).
+int orc_export_vector(uint32_t w, uint32_t h, uint32_t count, const uint32_t* idx, const float* data3, float* planes) {
+  std::memset(planes, 0, sizeof(float) * 3 * (size_t)w * h);
+  for (uint32_t i = 0; i < count; ++i) {
+    const size_t x = idx[i] % w, y = idx[i] / w, p = (h - y - 1) * w + x;
+    planes[p] = data3[3 * (size_t)i + 2];
+    planes[(size_t)w * h + p] = data3[3 * (size_t)i + 1];
+    planes[2 * (size_t)w * h + p] = data3[3 * (size_t)i];
   }
   return 0;
 }

@@ -186,6 +186,34 @@ class Oracle:
         self.lib.orc_tangent_transform(ptr(n3), ptr(t3), ptr(b3), _u32(len(io)), ptr(io))
         return io
 
+    # ---- image export (Src/image.cpp:22-405)
+    def export_float(self, w, h, idx, data, flo=0.0, fhi=0.0, normalize=True, dilate=0, rgb8=True):
+        """(image, (min, max)): h x w x 3 uint8 (rgb8) or h x w float32, file row order."""
+        idx = np.ascontiguousarray(idx, np.uint32)
+        data = np.ascontiguousarray(data, np.float32)
+        out = np.zeros((h, w, 3), np.uint8) if rgb8 else np.zeros((h, w), np.float32)
+        mm = np.zeros(2, np.float32)
+        self.lib.orc_export_float(_u32(w), _u32(h), _u32(len(idx)), ptr(idx, _u32p), ptr(data), ctypes.c_float(flo),
+                                  ctypes.c_float(fhi), _int(int(normalize)), _int(dilate), _int(int(rgb8)),
+                                  out.ctypes.data_as(_vp), ptr(mm))
+        return out, (float(mm[0]), float(mm[1]))
+
+    def export_normal(self, w, h, idx, data3, dilate=0):
+        idx = np.ascontiguousarray(idx, np.uint32)
+        data3 = np.ascontiguousarray(data3, np.float32)
+        out = np.zeros((h, w, 3), np.uint8)
+        self.lib.orc_export_normal(_u32(w), _u32(h), _u32(len(idx)), ptr(idx, _u32p), ptr(data3), _int(dilate),
+                                   out.ctypes.data_as(_vp))
+        return out
+
+    def export_vector(self, w, h, idx, data3):
+        """3 x h x w float32: planes B (z), G (y), R (x)."""
+        idx = np.ascontiguousarray(idx, np.uint32)
+        data3 = np.ascontiguousarray(data3, np.float32)
+        out = np.zeros((3, h, w), np.float32)
+        self.lib.orc_export_vector(_u32(w), _u32(h), _u32(len(idx)), ptr(idx, _u32p), ptr(data3), ptr(out))
+        return out
+
 
 class Reference:
     """The reference's own sources compiled on the host (oracle/_ref)."""
@@ -290,6 +318,29 @@ class Reference:
         io = np.ascontiguousarray(v3, np.float32).copy()
         self.lib.ref_shader_tangentspace(ptr(pixt), _u32(n), ptr(io))
         return io
+
+    # ---- image export: the reference writes the file (extension picks the format)
+    def export_float(self, path, w, h, idx, data, flo=0.0, fhi=0.0, normalize=True, dilate=0):
+        idx = np.ascontiguousarray(idx, np.uint32)
+        data = np.ascontiguousarray(data, np.float32)
+        mm = np.zeros(2, np.float32)
+        rc = self.lib.ref_export_float(_u32(w), _u32(h), _u32(len(idx)), ptr(idx, _u32p), ptr(data),
+                                       ctypes.c_char_p(path.encode()), ctypes.c_float(flo), ctypes.c_float(fhi),
+                                       _int(int(normalize)), _int(dilate), ptr(mm))
+        assert rc == 0
+        return float(mm[0]), float(mm[1])
+
+    def export_normal(self, path, w, h, idx, data3, dilate=0):
+        idx = np.ascontiguousarray(idx, np.uint32)
+        data3 = np.ascontiguousarray(data3, np.float32)
+        assert self.lib.ref_export_normal(_u32(w), _u32(h), _u32(len(idx)), ptr(idx, _u32p), ptr(data3),
+                                          ctypes.c_char_p(path.encode()), _int(dilate)) == 0
+
+    def export_vector(self, path, w, h, idx, data3):
+        idx = np.ascontiguousarray(idx, np.uint32)
+        data3 = np.ascontiguousarray(data3, np.float32)
+        assert self.lib.ref_export_vector(_u32(w), _u32(h), _u32(len(idx)), ptr(idx, _u32p), ptr(data3),
+                                          ctypes.c_char_p(path.encode())) == 0
 
 
 def pixels8(positions, directions):

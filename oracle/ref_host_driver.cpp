@@ -12,15 +12,21 @@
 #include "image.h"
 #include "mesh.h"
 #include <cstring>
+#include <omp.h>
 
 static unsigned int g_seed = 0;
 unsigned int std::fornos_seeded_device::operator()() { return g_seed; }
 
-// Logging and image export are not part of the path; silent stand-ins.
+// Logging is not part of the path; silent stand-ins.  exportNormalImage is the
+// name CompressedMapUV's constructor calls for a debug file
+// (Src/compute.cpp:413-415): a no-op here; the reference's function itself is
+// compiled as ref_exportNormalImage (oracle/build_ref.py).
 void logDebug(const std::string&, const std::string&) {}
 void logWarning(const std::string&, const std::string&) {}
 void logError(const std::string&, const std::string&) {}
 void exportNormalImage(const Vector3*, const CompressedMapUV*, const char*, int) {}
+void ref_exportNormalImage(const Vector3* data, const CompressedMapUV* map, const char* path, int dilate);
+void exportVectorImage(const Vector3* data, const CompressedMapUV* map, const char* path);
 GLuint LoadComputeShader_MeshMapping() { return 0; }
 GLuint LoadComputeShader_MeshMappingCullBackfaces() { return 0; }
 
@@ -177,6 +183,57 @@ int ref_samples(uint32_t spp, uint32_t perms, uint32_t seed, float* out4) {
   for (size_t i = 0; i < v.size(); ++i) {
     out4[4 * i] = v[i].x; out4[4 * i + 1] = v[i].y; out4[4 * i + 2] = v[i].z; out4[4 * i + 3] = 0.0f;
   }
+  return 0;
+}
+
+// A compressed map holding exactly the texels `idx` (ascending) of a w x h
+// map: CompressedMapUV keeps the texels whose direction has length > 0.5.
+static CompressedMapUV* make_cmap(uint32_t w, uint32_t h, uint32_t count, const uint32_t* idx) {
+  MapUV m(w, h);
+  for (uint32_t i = 0; i < count; ++i) m.directions[idx[i]] = Vector3(1.0f, 0.0f, 0.0f);
+  return new CompressedMapUV(&m);
+}
+
+// The export functions of Src/image.cpp:188-405, writing `path` (the
+// extension picks the format); dilation runs on one OpenMP thread, in row
+// order.
+int ref_export_float(uint32_t w, uint32_t h, uint32_t count, const uint32_t* idx, const float* data,
+                     const char* path, float flo, float fhi, int normalize, int dilate, float* minmax) {
+  CompressedMapUV* c = make_cmap(w, h, count, idx);
+  if (c->indices.size() != count) { delete c; return -1; }
+  const int threads = omp_get_max_threads();
+  omp_set_num_threads(1);
+  Vector2 mm;
+  exportFloatImage(data, c, path, Vector2(flo, fhi), normalize != 0, dilate, &mm);
+  omp_set_num_threads(threads);
+  minmax[0] = mm.x;
+  minmax[1] = mm.y;
+  delete c;
+  return 0;
+}
+
+int ref_export_normal(uint32_t w, uint32_t h, uint32_t count, const uint32_t* idx, const float* data3,
+                      const char* path, int dilate) {
+  CompressedMapUV* c = make_cmap(w, h, count, idx);
+  if (c->indices.size() != count) { delete c; return -1; }
+  std::vector<Vector3> v(count);
+  for (uint32_t i = 0; i < count; ++i) v[i] = Vector3(data3[3 * i], data3[3 * i + 1], data3[3 * i + 2]);
+  const int threads = omp_get_max_threads();
+  omp_set_num_threads(1);
+  ref_exportNormalImage(v.data(), c, path, dilate);
+  omp_set_num_threads(threads);
+  delete c;
+  return 0;
+}
+
+int ref_export_vector(uint32_t w, uint32_t h, uint32_t count, const uint32_t* idx, const float* data3,
+                      const char* path) {
+  CompressedMapUV* c = make_cmap(w, h, count, idx);
+  if (c->indices.size() != count) { delete c; return -1; }
+  std::vector<Vector3> v(count);
+  for (uint32_t i = 0; i < count; ++i) v[i] = Vector3(data3[3 * i], data3[3 * i + 1], data3[3 * i + 2]);
+  exportVectorImage(v.data(), c, path);
+  delete c;
   return 0;
 }
 
