@@ -42,6 +42,11 @@ class Tuning(ctypes.Structure):
     _fields_ = [("refill", c_u32), ("leaf_batch", c_u32), ("speculate", c_u32), ("reserved", c_u32)]
 
 
+class ExportParams(ctypes.Structure):
+    _fields_ = [("mode", c_int), ("filter_lo", c_float), ("filter_hi", c_float), ("normalize", c_int),
+                ("dilate", c_int)]
+
+
 class SceneInfo(ctypes.Structure):
     _fields_ = [("node_count", c_u32), ("corner_count", c_u32), ("depth", c_u32), ("leaf_count", c_u32),
                 ("device_bytes", c_u64)]
@@ -175,6 +180,9 @@ _SIGS = {
                                           c_u32, c_int, ctypes.POINTER(c_u64)]),
     "fk_bvh_build_flat": (c_int, [c_vp, c_vp, c_u32, c_u32, c_vp, c_u32, ctypes.POINTER(c_u32), f32p, f32p]),
     "fk_scene_build": (c_int, [c_vp, c_vp, c_u32, c_u32, ctypes.POINTER(c_vp)]),
+    "fk_export_image": (c_int, [c_vp, c_vp, c_vp, ctypes.POINTER(ExportParams), c_vp, f32p]),
+    "fk_image_write_rgb8": (c_int, [ctypes.c_char_p, c_u32, c_u32, c_vp]),
+    "fk_image_write_exr": (c_int, [ctypes.c_char_p, c_u32, c_u32, c_u32, f32p]),
     "fk_diag_scene_tree": (c_int, [c_vp, c_vp, c_int, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
     "fk_diag_sah_host": (c_int, [c_vp, c_u32, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
     "fk_denoiser_create": (c_int, [c_vp, ctypes.POINTER(c_vp)]),

@@ -388,6 +388,42 @@ class TexelMap:
             pass
 
 
+EXPORT_FLOAT_RGB8, EXPORT_FLOAT_F32, EXPORT_NORMAL_RGB8, EXPORT_VECTOR_F32 = 0, 1, 2, 3
+
+
+def export_image(ctx, tmap, data, mode, filter_range=(0.0, 0.0), normalize=True, dilate=0):
+    """Image export of Src/image.cpp:22-405 on the device (fk_export_image):
+    `data` holds 1 float per texel (FLOAT modes) or 3 (NORMAL / VECTOR), in the
+    map's order.  Returns (image, (min, max)): h x w x 3 uint8 for the RGB8
+    modes, h x w float32 (FLOAT_F32) or 3 x h x w float32 (VECTOR_F32, planes B,
+    G, R), rows as written to the file; (min, max) for the FLOAT modes."""
+    w, h = tmap.width, tmap.height
+    shape, dt = {EXPORT_FLOAT_RGB8: ((h, w, 3), np.uint8), EXPORT_NORMAL_RGB8: ((h, w, 3), np.uint8),
+                 EXPORT_FLOAT_F32: ((h, w), np.float32), EXPORT_VECTOR_F32: ((3, h, w), np.float32)}[mode]
+    img = ctx.buffer(int(np.prod(shape)) * np.dtype(dt).itemsize)
+    p = L.ExportParams(mode, filter_range[0], filter_range[1], int(normalize), dilate)
+    mm = np.zeros(2, np.float32)
+    _check(ctx.lib.fk_export_image(ctx.handle, tmap.handle, data.handle, ctypes.byref(p), img.handle, _f32(mm)), ctx,
+           "fk_export_image")
+    out = img.download(dt, shape)
+    img.free()
+    return out, (float(mm[0]), float(mm[1]))
+
+
+def write_image(path, image):
+    """Writes an exported image: h x w x 3 uint8 as .png / .tga, h x w or
+    3 x h x w float32 as .exr (HALF channels B, or B, G, R)."""
+    image = np.ascontiguousarray(image)
+    lib = L.load()
+    if image.dtype == np.uint8:
+        h, w, _ = image.shape
+        _check(lib.fk_image_write_rgb8(path.encode(), w, h, image.ctypes.data))
+    else:
+        planes = np.ascontiguousarray(image.astype(np.float32).reshape(-1, *image.shape[-2:]))
+        _check(lib.fk_image_write_exr(path.encode(), planes.shape[2], planes.shape[1], planes.shape[0],
+                                      _f32(planes)))
+
+
 def sah_tree_host(nodes):
     """(records, depth) of the surface-area inner tree computed on the host
     (fk_diag_sah_host), the records fk_scene_upload builds on the device."""

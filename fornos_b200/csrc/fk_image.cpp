@@ -1,0 +1,210 @@
+// Host writers for exported images: the files stbi_write_png, stbi_write_tga
+// (Src/image.cpp:222-243, 370-390) and tinyexr's SaveEXRImageToFile
+// (:245-296, 299-356) produce in the reference, pixel for pixel.  PNG as
+// 8-bit RGB with filter-0 rows in stored deflate blocks; TGA as uncompressed
+// 24-bit BGR with a bottom-left origin; EXR as a single-part scanline file
+// without compression, one scanline per block, HALF channels converted as
+// tinyexr converts FLOAT pixels when HALF is requested.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "fk_internal.h"
+
+namespace {
+
+bool ends_with(const std::string& s, const char* tail) {
+  const size_t n = std::strlen(tail);
+  return s.size() >= n && s.compare(s.size() - n, n, tail) == 0;
+}
+
+uint32_t crc32(const uint8_t* p, size_t n) {
+  static uint32_t table[256];
+  static bool ready = false;
+  if (!ready) {
+    for (uint32_t i = 0; i < 256; ++i) {
+      uint32_t c = i;
+      for (int k = 0; k < 8; ++k) c = (c & 1) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
+      table[i] = c;
+    }
+    ready = true;
+  }
+  uint32_t crc = 0xFFFFFFFFu;
+  for (size_t i = 0; i < n; ++i) crc = table[(crc ^ p[i]) & 0xFF] ^ (crc >> 8);
+  return ~crc;
+}
+
+void put_be32(std::vector<uint8_t>& o, uint32_t v) {
+  o.push_back((uint8_t)(v >> 24));
+  o.push_back((uint8_t)(v >> 16));
+  o.push_back((uint8_t)(v >> 8));
+  o.push_back((uint8_t)v);
+}
+void put_le(std::vector<uint8_t>& o, uint64_t v, int bytes) {
+  for (int k = 0; k < bytes; ++k) o.push_back((uint8_t)(v >> (8 * k)));
+}
+
+void png_chunk(std::vector<uint8_t>& o, const char* type, const std::vector<uint8_t>& body) {
+  put_be32(o, (uint32_t)body.size());
+  const size_t start = o.size();
+  o.insert(o.end(), type, type + 4);
+  o.insert(o.end(), body.begin(), body.end());
+  put_be32(o, crc32(o.data() + start, body.size() + 4));
+}
+
+bool write_file(const char* path, const std::vector<uint8_t>& bytes) {
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return false;
+  const bool ok = std::fwrite(bytes.data(), 1, bytes.size(), f) == bytes.size();
+  return std::fclose(f) == 0 && ok;
+}
+
+int write_png(const char* path, uint32_t w, uint32_t h, const uint8_t* rgb) {
+  std::vector<uint8_t> raw;
+  raw.reserve((size_t)h * (3 * (size_t)w + 1));
+  for (uint32_t y = 0; y < h; ++y) {
+    raw.push_back(0);  // filter: none
+    raw.insert(raw.end(), rgb + (size_t)y * 3 * w, rgb + (size_t)(y + 1) * 3 * w);
+  }
+  std::vector<uint8_t> z = {0x78, 0x01};  // zlib header: deflate, no preset dictionary
+  size_t pos = 0;
+  do {
+    const size_t n = std::min<size_t>(65535, raw.size() - pos);
+    z.push_back(pos + n == raw.size() ? 1 : 0);  // stored block, final flag
+    put_le(z, n, 2);
+    put_le(z, (uint16_t)~n, 2);
+    z.insert(z.end(), raw.begin() + pos, raw.begin() + pos + n);
+    pos += n;
+  } while (pos < raw.size());
+  uint32_t a = 1, b = 0;  // Adler-32 of the uncompressed data
+  for (uint8_t c : raw) {
+    a = (a + c) % 65521;
+    b = (b + a) % 65521;
+  }
+  put_be32(z, (b << 16) | a);
+  std::vector<uint8_t> o = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n'};
+  std::vector<uint8_t> ihdr;
+  put_be32(ihdr, w);
+  put_be32(ihdr, h);
+  ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});  // 8-bit RGB, deflate, filter method 0, no interlace
+  png_chunk(o, "IHDR", ihdr);
+  png_chunk(o, "IDAT", z);
+  png_chunk(o, "IEND", {});
+  return write_file(path, o) ? FK_OK : FK_ERR_INVALID;
+}
+
+int write_tga(const char* path, uint32_t w, uint32_t h, const uint8_t* rgb) {
+  if (w > 65535 || h > 65535) return FK_ERR_INVALID;
+  std::vector<uint8_t> o(18, 0);
+  o[2] = 2;  // uncompressed true colour
+  o[12] = (uint8_t)w;
+  o[13] = (uint8_t)(w >> 8);
+  o[14] = (uint8_t)h;
+  o[15] = (uint8_t)(h >> 8);
+  o[16] = 24;
+  o[17] = 0;  // bottom-left origin: the last buffer row is stored first
+  o.reserve(18 + 3 * (size_t)w * h);
+  for (uint32_t r = h; r-- > 0;)
+    for (uint32_t x = 0; x < w; ++x) {
+      const uint8_t* p = rgb + 3 * ((size_t)r * w + x);
+      o.push_back(p[2]);
+      o.push_back(p[1]);
+      o.push_back(p[0]);
+    }
+  return write_file(path, o) ? FK_OK : FK_ERR_INVALID;
+}
+
+// FLOAT to HALF as tinyexr converts pixels for a HALF channel: the mantissa
+// truncated and rounded up in magnitude when the first dropped bit is set,
+// float denormals to zero, NaN to a quiet NaN, overflow to infinity.
+uint16_t half_of(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  const uint32_t sign = (u >> 16) & 0x8000u, m = u & 0x7FFFFFu;
+  const int e = (int)((u >> 23) & 0xFF);
+  if (e == 0) return (uint16_t)sign;
+  if (e == 255) return (uint16_t)(sign | 0x7C00u | (m ? 0x200u : 0u));
+  const int ne = e - 127 + 15;
+  if (ne >= 31) return (uint16_t)(sign | 0x7C00u);
+  if (ne <= 0) {
+    if (14 - ne > 24) return (uint16_t)sign;
+    const uint32_t mant = m | 0x800000u;
+    uint32_t hm = mant >> (14 - ne);
+    if ((mant >> (13 - ne)) & 1u) ++hm;
+    return (uint16_t)(sign | hm);
+  }
+  uint32_t hv = ((uint32_t)ne << 10) | (m >> 13);
+  if (m & 0x1000u) ++hv;
+  return (uint16_t)(sign | hv);
+}
+
+void attr(std::vector<uint8_t>& o, const char* name, const char* type, const std::vector<uint8_t>& v) {
+  o.insert(o.end(), name, name + std::strlen(name) + 1);
+  o.insert(o.end(), type, type + std::strlen(type) + 1);
+  put_le(o, v.size(), 4);
+  o.insert(o.end(), v.begin(), v.end());
+}
+
+int write_exr(const char* path, uint32_t w, uint32_t h, uint32_t nplanes, const float* planes) {
+  if (nplanes != 1 && nplanes != 3) return FK_ERR_INVALID;
+  static const char* names[3] = {"B", "G", "R"};  // plane order = the header's (sorted) channel order
+  std::vector<uint8_t> o = {0x76, 0x2f, 0x31, 0x01, 2, 0, 0, 0};
+  std::vector<uint8_t> ch;
+  for (uint32_t c = 0; c < nplanes; ++c) {
+    ch.insert(ch.end(), names[c], names[c] + 2);
+    put_le(ch, 1, 4);                   // HALF
+    ch.insert(ch.end(), {0, 0, 0, 0});  // pLinear, reserved
+    put_le(ch, 1, 4);                   // x sampling
+    put_le(ch, 1, 4);                   // y sampling
+  }
+  ch.push_back(0);
+  attr(o, "channels", "chlist", ch);
+  attr(o, "compression", "compression", {0});
+  std::vector<uint8_t> box;
+  put_le(box, 0, 4);
+  put_le(box, 0, 4);
+  put_le(box, w - 1, 4);
+  put_le(box, h - 1, 4);
+  attr(o, "dataWindow", "box2i", box);
+  attr(o, "displayWindow", "box2i", box);
+  attr(o, "lineOrder", "lineOrder", {0});
+  const float one = 1.0f, zero = 0.0f;
+  std::vector<uint8_t> f1(4), v2(8, 0);
+  std::memcpy(f1.data(), &one, 4);
+  std::memcpy(v2.data(), &zero, 4);
+  std::memcpy(v2.data() + 4, &zero, 4);
+  attr(o, "pixelAspectRatio", "float", f1);
+  attr(o, "screenWindowCenter", "v2f", v2);
+  attr(o, "screenWindowWidth", "float", f1);
+  o.push_back(0);
+  const size_t table = o.size(), block = 8 + (size_t)nplanes * w * 2;
+  for (uint32_t y = 0; y < h; ++y) put_le(o, table + 8 * (size_t)h + y * block, 8);
+  for (uint32_t y = 0; y < h; ++y) {
+    put_le(o, y, 4);
+    put_le(o, (uint64_t)nplanes * w * 2, 4);
+    for (uint32_t c = 0; c < nplanes; ++c)
+      for (uint32_t x = 0; x < w; ++x) put_le(o, half_of(planes[((size_t)c * h + y) * w + x]), 2);
+  }
+  return write_file(path, o) ? FK_OK : FK_ERR_INVALID;
+}
+
+}  // namespace
+
+extern "C" {
+
+int fk_image_write_rgb8(const char* path, uint32_t w, uint32_t h, const uint8_t* rgb) {
+  if (!path || !rgb || w == 0 || h == 0) return FK_ERR_INVALID;
+  const std::string p(path);
+  if (ends_with(p, ".png")) return write_png(path, w, h, rgb);
+  if (ends_with(p, ".tga")) return write_tga(path, w, h, rgb);
+  return FK_ERR_INVALID;
+}
+
+int fk_image_write_exr(const char* path, uint32_t w, uint32_t h, uint32_t planes, const float* data) {
+  if (!path || !data || w == 0 || h == 0 || !ends_with(path, ".exr")) return FK_ERR_INVALID;
+  return write_exr(path, w, h, planes, data);
+}
+
+}  // extern "C"

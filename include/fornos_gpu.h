@@ -458,6 +458,49 @@ typedef struct fk_bake_out {
 
 int fk_bake(fk_ctx* ctx, const fk_bake_desc* desc, fk_bake_out* out);
 
+/* ------------------------------------------------------------ image export
+ * exportFloatImage / exportNormalImage / exportVectorImage (Src/image.cpp:22-405)
+ * on the device: the texel map's values (1 float per texel, or 3 for the
+ * NORMAL / VECTOR modes, in the map's order) scattered into the W x H image
+ * the reference writes, rows flipped (texel (x, y) in row H - y - 1):
+ *   FK_EXPORT_FLOAT_RGB8   PNG / TGA path: min / max over the values, the
+ *                          filter range (filter_hi > filter_lo: values outside
+ *                          become 0, the range clamps the min / max), optional
+ *                          normalisation, (uint8)(clamp(t, 0, 1) * 255) in all
+ *                          three channels; W x H x 3 bytes;
+ *   FK_EXPORT_FLOAT_F32    EXR path: clamped to the filter range, optionally
+ *                          normalised; W x H floats;
+ *   FK_EXPORT_NORMAL_RGB8  PNG / TGA path of normal maps: (uint8)((n * 0.5 +
+ *                          0.5) * 255) per channel; W x H x 3 bytes;
+ *   FK_EXPORT_VECTOR_F32   EXR path of vector maps: planes B (z), G (y), R (x);
+ *                          3 x W x H floats.
+ * dilate > 0 (RGB8 modes): dilateRGB's fill of uncovered pixels from the
+ * nearest centre (distance < dilate, 8 directions) whose 8 neighbours are
+ * covered, with the result of its row-order scan.  minmax (FLOAT modes, may be
+ * NULL) gets the range used.  `image` holds at least the bytes above. */
+#define FK_EXPORT_FLOAT_RGB8 0
+#define FK_EXPORT_FLOAT_F32 1
+#define FK_EXPORT_NORMAL_RGB8 2
+#define FK_EXPORT_VECTOR_F32 3
+typedef struct fk_export_params {
+  int mode;
+  float filter_lo, filter_hi;
+  int normalize;
+  int dilate;
+} fk_export_params;
+int fk_export_image(fk_ctx* ctx, const fk_texel_map* map, const fk_buf* data, const fk_export_params* params,
+                    fk_buf* image, float* minmax);
+
+/* Host writers of exported images (stbi_write_png / stbi_write_tga /
+ * tinyexr's SaveEXRImageToFile in Src/image.cpp): an RGB8 image (rows in
+ * buffer order) as PNG (".png", stored deflate blocks) or TGA (".tga",
+ * uncompressed, bottom-left origin); float planes as a scanline EXR without
+ * compression, channels "B" (1 plane) or "B", "G", "R" (3 planes), stored as
+ * HALF with tinyexr's conversion (rounded up in magnitude on the first dropped
+ * bit).  The decoded pixels equal the reference's files'. */
+int fk_image_write_rgb8(const char* path, uint32_t width, uint32_t height, const uint8_t* rgb);
+int fk_image_write_exr(const char* path, uint32_t width, uint32_t height, uint32_t planes, const float* data);
+
 /* ------------------------------------------------------------ diagnostics
  * FP32 throughput of independent add / multiply / min chains on this device
  * (one operation counted per instruction), the denominator of the traversal
