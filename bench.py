@@ -138,17 +138,33 @@ class Prepared:
         t0 = time.perf_counter()
         lo, hi = wl["gen"](seed)
         self.gen_s = time.perf_counter() - t0
+        self.lo, self.hi = lo, hi
+        t0 = time.perf_counter()
         self.hm = api.Mesh(hi)
         self.hm.compute_vertex_normals()
         self.lm = api.Mesh(lo)
         self.lm.compute_tangent_space()
         self.dm = self.lm.copy()
         self.dm.compute_vertex_normals_aggressive()
+        self.prep_s = time.perf_counter() - t0
         t0 = time.perf_counter()
         self.bvh = api.BVH.create_binary(self.hm, 8, 8192)
         self.bvh_s = time.perf_counter() - t0
         self.nodes, self.pos4, self.nrm4 = self.bvh.flatten(self.hm)
         self.triangles = hi.triangle_count
+
+
+def device_preprocess(ctx, prep):
+    """The host preprocessing of Prepared run by the device generators
+    (fk_mesh_compute_normals_device / fk_mesh_compute_tangent_space_device)."""
+    from fornos_b200 import api
+    hm = api.Mesh(prep.hi)
+    hm.compute_normals_device(ctx, api.NORMALS_VERTEX)
+    lm = api.Mesh(prep.lo)
+    lm.compute_tangent_space_device(ctx)
+    dm = lm.copy()
+    dm.compute_normals_device(ctx, api.NORMALS_WELDED)
+    return hm, lm, dm
 
 
 def reduce_over_ranks(ms, rays, world, device):
@@ -205,6 +221,15 @@ def run_fornos(args, wl, rank, world):
     api.Scene.build(ctx, prep.hm, 8, 8192).free()
     ctx.sync()
     scene_build_ms = (time.perf_counter() - t0) * 1e3
+    # the same preprocessing on the device (informational; first call warms the pool)
+    device_preprocess(ctx, prep)
+    t0 = time.perf_counter()
+    dprep = device_preprocess(ctx, prep)
+    prep_device_ms = (time.perf_counter() - t0) * 1e3
+    dh, hh = dprep[0].arrays(), prep.hm.arrays()
+    if not (np.array_equal(dh.vertices, hh.vertices) and np.array_equal(dh.normals, hh.normals, equal_nan=True)):
+        raise RuntimeError("device preprocessing differs from the host's")
+    del dprep
     scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
     if args.tree == "reference":
         scene.set_tree(api.TREE_REFERENCE)
@@ -341,7 +366,9 @@ def run_fornos(args, wl, rank, world):
                    "rays_counted": "2 mapping + spp each for AO, bent normals, thickness (AO and bent normals "
                                    "share one traversal)",
                    "l2": "inputs larger than L2 (scene %.0f MB resident)" % (info["device_bytes"] / 1e6),
-                   "bvh_build_s": round(prep.bvh_s, 3), "scene_build_device_ms": round(scene_build_ms, 1), "raster_ms": round(raster_ms, 3),
+                   "bvh_build_s": round(prep.bvh_s, 3), "scene_build_device_ms": round(scene_build_ms, 1),
+                   "preprocess_host_ms": round(prep.prep_s * 1e3, 1), "preprocess_device_ms": round(prep_device_ms, 1),
+                   "raster_ms": round(raster_ms, 3),
                    "parallelism": "replicas" if world > 1 else "single"},
         "e2e": {"value": round(rays_all / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mrays/s",
                 "ms_per_step": round(e2e_ms, 3), "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},

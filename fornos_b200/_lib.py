@@ -118,6 +118,8 @@ _SIGS = {
     "fk_mesh_compute_vertex_normals": (c_int, [c_vp]),
     "fk_mesh_compute_vertex_normals_welded": (c_int, [c_vp]),
     "fk_mesh_compute_tangent_space": (c_int, [c_vp]),
+    "fk_mesh_compute_normals_device": (c_int, [c_vp, c_vp, c_int]),
+    "fk_mesh_compute_tangent_space_device": (c_int, [c_vp, c_vp]),
     "fk_bvh_build": (c_int, [c_vp, c_u32, c_u32, ctypes.POINTER(c_vp)]),
     "fk_bvh_free": (c_int, [c_vp]),
     "fk_bvh_flatten_sizes": (c_int, [c_vp, u32p, u32p]),

@@ -20,6 +20,7 @@ MISS = 0xFFFFFFFF
 AO, BN, THICK, AO_BN = 0, 1, 2, 3
 TRAVERSE_AUTO, TRAVERSE_ORDERED, TRAVERSE_SKIP, TRAVERSE_ORDERED4 = 0, 1, 2, 3
 TREE_REFERENCE, TREE_SAH = 0, 1
+NORMALS_FACE, NORMALS_VERTEX, NORMALS_WELDED = 0, 1, 2
 SCHEDULE_STATIC, SCHEDULE_DYNAMIC = 0x10, 0x20  # or-ed into `traverse`
 EXACT_BOX_TESTS = 0x100  # or-ed into `traverse`: divide in every box test
 GATHER_HEIGHT, GATHER_POSITION, GATHER_NORMAL = 0, 1, 2
@@ -200,6 +201,15 @@ class Mesh:
 
     def compute_tangent_space(self):
         _check(self.lib.fk_mesh_compute_tangent_space(self.handle))
+
+    def compute_normals_device(self, ctx, method):
+        """The normal generator `method` (NORMALS_FACE / NORMALS_VERTEX /
+        NORMALS_WELDED) run on the device; the mesh ends as the host
+        generator leaves it."""
+        _check(self.lib.fk_mesh_compute_normals_device(ctx.handle, self.handle, int(method)), ctx)
+
+    def compute_tangent_space_device(self, ctx):
+        _check(self.lib.fk_mesh_compute_tangent_space_device(ctx.handle, self.handle), ctx)
 
     def arrays(self):
         d = L.MeshDesc()

@@ -127,6 +127,19 @@ int fk_mesh_compute_vertex_normals(fk_mesh* mesh);                    /* Src/mes
 int fk_mesh_compute_vertex_normals_welded(fk_mesh* mesh);             /* Src/mesh.cpp:680 (Aggressive) */
 int fk_mesh_compute_tangent_space(fk_mesh* mesh);                     /* Src/mesh.cpp:724 */
 
+/* The same generators on the device (sort-and-reduce kernels on ctx's
+ * stream): the mesh's arrays are uploaded, processed and written back, with
+ * results equal to the host calls above bit for bit (NaN payloads aside).
+ * method: FK_NORMALS_FACE (Mesh::computeFaceNormals, Src/mesh.cpp:627),
+ * FK_NORMALS_VERTEX (computeVertexNormals, :650) or FK_NORMALS_WELDED
+ * (computeVertexNormalsAggressive, :680).  Index errors: FK_ERR_INVALID,
+ * mesh unchanged. */
+#define FK_NORMALS_FACE 0
+#define FK_NORMALS_VERTEX 1
+#define FK_NORMALS_WELDED 2
+int fk_mesh_compute_normals_device(fk_ctx* ctx, fk_mesh* mesh, int method);
+int fk_mesh_compute_tangent_space_device(fk_ctx* ctx, fk_mesh* mesh);  /* Mesh::computeTangentSpace, :724 */
+
 /* ------------------------------------------------------------ BVH (host)
  * BVH::createBinary (Src/bvh.cpp:283-314): 16-bucket split, leaves of at
  * most max_tris_per_node triangles, depth limit max_depth (8192 in
