@@ -113,6 +113,7 @@ _SIGS = {
     "fk_mesh_create": (c_int, [ctypes.POINTER(MeshDesc), ctypes.POINTER(c_vp)]),
     "fk_mesh_describe": (c_int, [c_vp, ctypes.POINTER(MeshDesc)]),
     "fk_mesh_copy": (c_int, [c_vp, ctypes.POINTER(c_vp)]),
+    "fk_mesh_load": (c_int, [ctypes.c_char_p, ctypes.POINTER(c_vp)]),
     "fk_mesh_free": (c_int, [c_vp]),
     "fk_mesh_compute_face_normals": (c_int, [c_vp]),
     "fk_mesh_compute_vertex_normals": (c_int, [c_vp]),

@@ -7,6 +7,7 @@ run_step / get_results / progress.  FornosRunner (Src/fornos.h:129-149)
 drives a whole bake from FornosParameters-like settings.
 """
 import ctypes
+import os
 
 import numpy as np
 
@@ -184,6 +185,13 @@ class Mesh:
                 self.lib.fk_mesh_free(self.handle)
         except Exception:
             pass
+
+    @classmethod
+    def load(cls, path):
+        """Mesh::loadFile: an .obj or .ply file as the reference's loader reads it."""
+        h = L.c_vp()
+        _check(L.load().fk_mesh_load(os.fsencode(path), ctypes.byref(h)), what="fk_mesh_load(%s)" % path)
+        return cls(handle=h.value)
 
     def copy(self):
         h = L.c_vp()

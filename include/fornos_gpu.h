@@ -121,6 +121,13 @@ int fk_mesh_create(const fk_mesh_desc* desc, fk_mesh** out);
  * mesh changes or is freed). */
 int fk_mesh_describe(const fk_mesh* mesh, fk_mesh_desc* out);
 int fk_mesh_copy(const fk_mesh* mesh, fk_mesh** out);                 /* Mesh::createCopy */
+/* Mesh::loadFile (Src/mesh.cpp:597-603): ".obj" through the Wavefront reader
+ * (:235-455), ".ply" through the PLY reader (:515-590, tinyply 2.0); the mesh
+ * the reference's loader returns, array for array.  FK_ERR_INVALID for a file
+ * the reference rejects, another extension, or a mesh whose corners name
+ * positions the file lacks; an OBJ file that cannot be opened gives an empty
+ * mesh, as in the reference. */
+int fk_mesh_load(const char* path, fk_mesh** out);
 int fk_mesh_free(fk_mesh* mesh);
 int fk_mesh_compute_face_normals(fk_mesh* mesh);                      /* Src/mesh.cpp:627 */
 int fk_mesh_compute_vertex_normals(fk_mesh* mesh);                    /* Src/mesh.cpp:650 */

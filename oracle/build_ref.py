@@ -9,8 +9,13 @@ reference tree (default /root/reference, override with FORNOS_REF_ROOT):
   * Src/meshmapping.cpp                    #included by ref_host_driver.cpp to
                                            reach fillMeshData (anonymous namespace);
   * Src/mesh.cpp lines 38-41 and 619-768   the Vector3 ordering and the normal /
-                                           tangent generators (the rest of the
-                                           file needs MSVC-only overloads);
+                                           tangent generators;
+  * Src/mesh.cpp lines 1-37 and 42-617,    the OBJ / PLY loaders, with two
+    3rdParty/tinyply/tinyply.cpp           MSVC-only constructs spelled for g++
+                                           (std::find_if over the overloaded
+                                           std::isspace takes ::isspace, and a
+                                           lambda bound to `auto &` is bound to
+                                           `auto`); nothing else changes;
   * 3rdParty/glad/glad.c                   GL entry-point table the above refer
                                            to (never called: no GL context);
   * Src/image.cpp, 3rdParty/tinyexr/tinyexr.cc
@@ -147,6 +152,22 @@ def main():
     run(CXX + shim + inc + ["-x", "c++", "-c", "-", "-o", o], part)
     objs.append(o)
 
+    # the loaders: includes, then everything between the Vector3 ordering and
+    # the generators; the two rewrites only make MSVC-accepted code compile
+    mesh_cpp = os.path.join(src, "mesh.cpp")
+    loader = "#line 1 \"%s\"\n" % mesh_cpp + "\n".join(lines[0:37]) + "\n#line 42 \"%s\"\n" % mesh_cpp + \
+        "\n".join(lines[41:617]) + "\n"
+    for old, new in (("std::find_if(begin, end, std::isspace)", "std::find_if(begin, end, ::isspace)"),
+                     ("auto &get_face_vertex_idx =", "auto get_face_vertex_idx =")):
+        assert loader.count(old) == 1, old
+        loader = loader.replace(old, new)
+    tiny = os.path.join(REF, "3rdParty", "tinyply")
+    o = os.path.join(OBJ, "mesh_loaders.o")
+    run(CXX + shim + inc + ["-I" + tiny, "-x", "c++", "-c", "-", "-o", o], loader)
+    objs.append(o)
+    o = os.path.join(OBJ, "tinyply.o")
+    run(CXX + ["-c", os.path.join(tiny, "tinyply.cpp"), "-o", o])
+    objs.append(o)
     o = os.path.join(OBJ, "glad.o")
     run(["gcc", "-O2", "-fPIC", "-w", "-I" + os.path.join(REF, "3rdParty", "glad", "include"), "-c",
          os.path.join(REF, "3rdParty", "glad", "glad.c"), "-o", o])

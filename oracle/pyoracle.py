@@ -226,6 +226,28 @@ class Reference:
         L = self.lib
         L.ref_scene_build.restype = _vp
         L.ref_raster.restype = _vp
+        L.ref_mesh_load.restype = _vp
+        L.ref_mesh_load.argtypes = [ctypes.c_char_p]
+        L.ref_mesh_sizes.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64)]
+        L.ref_mesh_arrays.argtypes = [_vp] + [_vp] * 5
+        L.ref_mesh_free.argtypes = [_vp]
+
+    def load_mesh(self, path):
+        """Mesh::loadFile (Src/mesh.cpp:597-603): the loaded arrays as
+        (positions, texcoords, normals, vertices, triangles), or None when the
+        loader returns null.  Never call it on a PLY file without s / t or
+        without normals: the reference's loader dereferences a null buffer
+        there."""
+        h = self.lib.ref_mesh_load(os.fsencode(path))
+        if not h:
+            return None
+        n = (ctypes.c_uint64 * 5)()
+        self.lib.ref_mesh_sizes(h, n)
+        arrs = [np.zeros((n[0], 3), np.float32), np.zeros((n[1], 2), np.float32), np.zeros((n[2], 3), np.float32),
+                np.zeros((n[3], 3), np.uint32), np.zeros((n[4], 3), np.uint32)]
+        self.lib.ref_mesh_arrays(h, *[a.ctypes.data_as(_vp) for a in arrs])
+        self.lib.ref_mesh_free(h)
+        return tuple(arrs)
 
     def normals(self, m, which):
         code = {"face": 0, "vertex": 1, "welded": 2}[which]

@@ -237,4 +237,42 @@ int ref_export_vector(uint32_t w, uint32_t h, uint32_t count, const uint32_t* id
   return 0;
 }
 
+// Mesh::loadFile (Src/mesh.cpp:597-603).  ref_mesh_load returns the mesh or
+// null; ref_mesh_sizes gives position, texcoord, normal, vertex and triangle
+// counts; ref_mesh_arrays copies the arrays out (positions / normals 3
+// floats, texcoords 2, vertices and triangles 3 u32 each).
+void* ref_mesh_load(const char* path) { return Mesh::loadFile(path); }
+
+void ref_mesh_sizes(const void* h, uint64_t* n) {
+  const Mesh* m = static_cast<const Mesh*>(h);
+  n[0] = m->positions.size();
+  n[1] = m->texcoords.size();
+  n[2] = m->normals.size();
+  n[3] = m->vertices.size();
+  n[4] = m->triangles.size();
+}
+
+void ref_mesh_arrays(const void* h, float* pos, float* uv, float* nrm, uint32_t* vtx, uint32_t* tri) {
+  const Mesh* m = static_cast<const Mesh*>(h);
+  for (size_t i = 0; i < m->positions.size(); ++i) {
+    pos[3 * i] = m->positions[i].x; pos[3 * i + 1] = m->positions[i].y; pos[3 * i + 2] = m->positions[i].z;
+  }
+  for (size_t i = 0; i < m->texcoords.size(); ++i) { uv[2 * i] = m->texcoords[i].x; uv[2 * i + 1] = m->texcoords[i].y; }
+  for (size_t i = 0; i < m->normals.size(); ++i) {
+    nrm[3 * i] = m->normals[i].x; nrm[3 * i + 1] = m->normals[i].y; nrm[3 * i + 2] = m->normals[i].z;
+  }
+  for (size_t i = 0; i < m->vertices.size(); ++i) {
+    vtx[3 * i] = m->vertices[i].positionIndex;
+    vtx[3 * i + 1] = m->vertices[i].texcoordIndex;
+    vtx[3 * i + 2] = m->vertices[i].normalIndex;
+  }
+  for (size_t i = 0; i < m->triangles.size(); ++i) {
+    tri[3 * i] = m->triangles[i].vertexIndex0;
+    tri[3 * i + 1] = m->triangles[i].vertexIndex1;
+    tri[3 * i + 2] = m->triangles[i].vertexIndex2;
+  }
+}
+
+void ref_mesh_free(void* h) { delete static_cast<Mesh*>(h); }
+
 }  // extern "C"
