@@ -14,7 +14,9 @@ same bake through fk_bake from pinned host arrays (uploads and result copies
 inside the timed region).  Multi-GPU: one process per GPU, each baking its
 own seeded replica of the workload (weak scaling, no data-path collective).
 
-The default line also carries the denoised-vs-plain comparison at 4096x4096
+The default line also carries fk_run's time from mesh files to image files
+(`files_to_images`: the workload written as PLY, all six maps written as PNG /
+EXR) and the denoised-vs-plain comparison at 4096x4096
 (`denoise`); --workload batch measures 64 batched jobs and --workload denoise
 the comparison alone.  --tree reference walks the reference's inner BVH nodes
 instead of the surface-area tree built at upload.
@@ -165,6 +167,65 @@ def device_preprocess(ctx, prep):
     dm = lm.copy()
     dm.compute_normals_device(ctx, api.NORMALS_WELDED)
     return hm, lm, dm
+
+
+def write_ply(path, m):
+    """A binary little-endian PLY of a MeshArrays mesh with one PLY vertex per
+    mesh vertex (x y z nx ny nz s t as floats) and uint triangle lists: the
+    layout the reference's PLY reader expects."""
+    v = m.vertices.astype(np.int64)
+    rec = np.zeros(len(v), dtype=[("p", "<f4", 3), ("n", "<f4", 3), ("t", "<f4", 2)])
+    rec["p"] = m.positions[v[:, 0]]
+    if len(m.normals):
+        rec["n"] = m.normals[np.minimum(v[:, 2], len(m.normals) - 1)]
+    if len(m.texcoords):
+        rec["t"] = m.texcoords[np.minimum(v[:, 1], len(m.texcoords) - 1)]
+    face = np.zeros(m.triangle_count, dtype=[("c", "u1"), ("i", "<u4", 3)])
+    face["c"] = 3
+    face["i"] = m.triangles
+    head = ("ply\nformat binary_little_endian 1.0\nelement vertex %d\nproperty float x\nproperty float y\n"
+            "property float z\nproperty float nx\nproperty float ny\nproperty float nz\nproperty float s\n"
+            "property float t\nelement face %d\nproperty list uchar uint vertex_indices\nend_header\n"
+            % (len(v), m.triangle_count))
+    with open(path, "wb") as fh:
+        fh.write(head.encode())
+        fh.write(rec.tobytes())
+        fh.write(face.tobytes())
+    return os.path.getsize(path)
+
+
+def files_to_images(ctx, prep, wl, seed):
+    """fk_run (FornosRunner::start + run) on the workload written as PLY files:
+    mesh files in, PNG / EXR maps out, every step on the device (load and the
+    image encoding on the host).  Informational; one timed run after one
+    warm-up run."""
+    import tempfile
+
+    from fornos_b200 import api
+    with tempfile.TemporaryDirectory() as d:
+        lo_p, hi_p = os.path.join(d, "lo.ply"), os.path.join(d, "hi.ply")
+        size = write_ply(lo_p, prep.lo) + write_ply(hi_p, prep.hm.arrays())
+        smp = dict(enabled=1, sample_count=wl["spp"], min_distance=wl["min_d"], max_distance=wl["max_d"])
+        out = {"height": dict(enabled="height" in wl["bakers"], output_path=os.path.join(d, "height.png"),
+                              max_distance=wl["max_d"]),
+               "positions": dict(enabled="position" in wl["bakers"], output_path=os.path.join(d, "positions.exr")),
+               "normals": dict(enabled="normals" in wl["bakers"], output_path=os.path.join(d, "normals.png")),
+               "ao": dict(smp, enabled="ao" in wl["bakers"], output_path=os.path.join(d, "ao.png")),
+               "bent_normals": dict(smp, enabled="bn" in wl["bakers"], output_path=os.path.join(d, "bn.png")),
+               "thickness": dict(smp, enabled="thick" in wl["bakers"], output_path=os.path.join(d, "thick.png"))}
+        kw = dict(lo_poly_mesh_path=lo_p, hi_poly_mesh_path=hi_p, hi_poly_mesh_normal=api.NORMAL_COMPUTE_PER_VERTEX,
+                  tex_width=wl["tex"], tex_height=wl["tex"], seed=seed, **out)
+        try:
+            api.run(ctx, **kw)
+            t0 = time.perf_counter()
+            api.run(ctx, **kw)
+            ms = (time.perf_counter() - t0) * 1e3
+        except Exception as e:  # reported, never fatal to the bench line
+            return {"error": str(e)[:200]}
+        written = sorted(f for f in os.listdir(d) if not f.endswith(".ply"))
+    return {"ms": round(ms, 1), "input_bytes": int(size), "outputs": written,
+            "steps": "PLY load, hi vertex normals, lo tangents, welded copy, raster, BVH build, mapping, "
+                     "six solvers, export with dilation 16, PNG / EXR writing"}
 
 
 def reduce_over_ranks(ms, rays, world, device):
@@ -775,6 +836,8 @@ def main():
         mr, rays, dt, m = cpu.run()
         result["cpu_baseline"] = {"value": round(mr, 4), "unit": "Mrays/s", "cores": cpu.cores, "kind": cpu.kind,
                                   "sample": cpu.describe(rays, m)}
+    if rank == 0 and world == 1:
+        result["files_to_images"] = files_to_images(state[4], state[0], wl, args.seed)
     if rank == 0 and world == 1 and args.workload == "plane2048" and not args.no_denoise:
         prep, _, _, _, ctx, stream, scene = state
         result["denoise"] = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed, args.denoise_tex)

@@ -47,6 +47,21 @@ class ExportParams(ctypes.Structure):
                 ("dilate", c_int)]
 
 
+class RunSolver(ctypes.Structure):
+    _fields_ = [("enabled", c_int), ("output_path", ctypes.c_char_p), ("sample_count", c_u32),
+                ("min_distance", c_float), ("max_distance", c_float), ("tangent_space", c_int),
+                ("normalize_output", c_int)]
+
+
+class RunParams(ctypes.Structure):
+    _fields_ = [("lo_poly_mesh_path", ctypes.c_char_p), ("hi_poly_mesh_path", ctypes.c_char_p),
+                ("lo_poly_mesh_normal", c_int), ("hi_poly_mesh_normal", c_int), ("bvh_tris_per_node", c_u32),
+                ("tex_width", c_u32), ("tex_height", c_u32), ("tex_dilation", c_int), ("ignore_backfaces", c_int),
+                ("mapping", c_int), ("mapping_edge", c_float), ("height", RunSolver), ("positions", RunSolver),
+                ("normals", RunSolver), ("ao", RunSolver), ("bent_normals", RunSolver), ("thickness", RunSolver),
+                ("seed", c_u32), ("traverse", c_int)]
+
+
 class SceneInfo(ctypes.Structure):
     _fields_ = [("node_count", c_u32), ("corner_count", c_u32), ("depth", c_u32), ("leaf_count", c_u32),
                 ("device_bytes", c_u64)]
@@ -167,6 +182,8 @@ _SIGS = {
     "fk_solver_result_buffer": (c_vp, [c_vp]),
     "fk_solver_free": (c_int, [c_vp]),
     "fk_bake": (c_int, [c_vp, ctypes.POINTER(BakeDesc), ctypes.POINTER(BakeOut)]),
+    "fk_run_params_default": (None, [ctypes.POINTER(RunParams)]),
+    "fk_run": (c_int, [c_vp, ctypes.POINTER(RunParams)]),
     "fk_batch_create": (c_int, [c_vp, ctypes.POINTER(BatchJob), c_u32, c_int, ctypes.POINTER(c_vp)]),
     "fk_batch_info": (c_int, [c_vp, ctypes.POINTER(c_u64), u32p, u32p]),
     "fk_batch_tune": (c_int, [c_vp, c_u64, ctypes.POINTER(Tuning), ctypes.POINTER(c_int)]),

@@ -717,6 +717,47 @@ def bake(ctx, nodes, pos4, nrm4, width, height, pix8, pixt12, indices, outputs, 
     _check(ctx.lib.fk_bake(ctx.handle, ctypes.byref(d), ctypes.byref(o)), ctx, "fk_bake")
 
 
+NORMAL_IMPORT, NORMAL_COMPUTE_PER_FACE, NORMAL_COMPUTE_PER_VERTEX = 0, 1, 2
+RUN_SOLVERS = ("height", "positions", "normals", "ao", "bent_normals", "thickness")
+
+
+def run_params(**fields):
+    """FornosParameters (Src/fornos.h:29-110) as fk_run_params: the
+    reference's defaults, overridden by `fields`.  Shared fields by name
+    (lo_poly_mesh_path, hi_poly_mesh_path, lo_poly_mesh_normal,
+    hi_poly_mesh_normal, bvh_tris_per_node, tex_width, tex_height,
+    tex_dilation, ignore_backfaces, mapping, mapping_edge, seed, traverse);
+    solvers (height, positions, normals, ao, bent_normals, thickness) as dicts
+    of enabled, output_path, sample_count, min_distance, max_distance,
+    tangent_space, normalize_output."""
+    p = L.RunParams()
+    L.load().fk_run_params_default(ctypes.byref(p))
+    keep = []
+    for k, v in fields.items():
+        if k in RUN_SOLVERS:
+            sv = getattr(p, k)
+            for sk, x in v.items():
+                if sk == "output_path":
+                    x = os.fsencode(x) if x is not None else None
+                    keep.append(x)
+                setattr(sv, sk, x)
+        elif k.endswith("_path"):
+            x = os.fsencode(v) if v is not None else None
+            keep.append(x)
+            setattr(p, k, x)
+        else:
+            setattr(p, k, v)
+    p._keep = keep
+    return p
+
+
+def run(ctx, **fields):
+    """fk_run: FornosRunner::start + run to completion, mesh files in, image
+    files out (fields as run_params)."""
+    p = run_params(**fields)
+    _check(ctx.lib.fk_run(ctx.handle, ctypes.byref(p)), ctx, "fk_run")
+
+
 # ------------------------------------------------------------------ batches and tuning
 class Batch:
     """Batched hemisphere jobs in one persistent launch (fk_batch_*).

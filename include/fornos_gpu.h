@@ -478,6 +478,53 @@ typedef struct fk_bake_out {
 
 int fk_bake(fk_ctx* ctx, const fk_bake_desc* desc, fk_bake_out* out);
 
+/* ------------------------------------------------------------ runner
+ * FornosRunner::start, then FornosRunner::run until every task has finished
+ * (Src/fornos.cpp:53-251), with the fields of FornosParameters
+ * (Src/fornos.h:29-110): mesh files in, image files out.  Meshes load with
+ * fk_mesh_load, normals / tangents / the welded direction copy are computed
+ * on the device, the texel map by fk_raster_uv, the BVH by fk_scene_build
+ * (bvh_tris_per_node, depth 8192); each enabled solver's result is exported
+ * as its task's finish() exports it (height: filter [0, max_distance],
+ * normalize_output, dilation; positions: EXR only; normals and bent normals:
+ * normal image, EXR as a vector image; AO and thickness: normalised,
+ * dilation) and written by the path's extension (.png, .tga, .exr; other
+ * extensions write nothing, as in the reference).  Sample tables come from
+ * `seed`.  Errors: "Missing low poly mesh", "Low poly mesh is missing
+ * texture coordinates or normals information" (fk_last_error). */
+#define FK_NORMAL_IMPORT 0             /* NormalImport::Import */
+#define FK_NORMAL_COMPUTE_PER_FACE 1   /* NormalImport::ComputePerFace */
+#define FK_NORMAL_COMPUTE_PER_VERTEX 2 /* NormalImport::ComputePerVertex */
+typedef struct fk_run_solver {
+  int enabled;
+  const char* output_path;
+  uint32_t sample_count;   /* AO, bent normals, thickness */
+  float min_distance;      /* AO, bent normals, thickness */
+  float max_distance;      /* AO, bent normals, thickness; height: the filter's upper end */
+  int tangent_space;       /* normals, bent normals */
+  int normalize_output;    /* height */
+} fk_run_solver;
+typedef struct fk_run_params {
+  const char* lo_poly_mesh_path;
+  const char* hi_poly_mesh_path;  /* NULL or "": the low-poly mesh */
+  int lo_poly_mesh_normal;        /* FK_NORMAL_* */
+  int hi_poly_mesh_normal;
+  uint32_t bvh_tris_per_node;
+  uint32_t tex_width, tex_height;
+  int tex_dilation;
+  int ignore_backfaces;
+  int mapping;                    /* FK_MAP_* (MeshMappingMethod) */
+  float mapping_edge;
+  fk_run_solver height, positions, normals, ao, bent_normals, thickness;
+  uint32_t seed;
+  int traverse;                   /* FK_TRAVERSE_* */
+} fk_run_params;
+/* The defaults of FornosParameters (8 triangles per node, 2048 x 2048,
+ * dilation 16, back faces ignored, Smooth mapping with edge 0.05, 256
+ * samples in [0.01, 10], tangent space on, height normalised). */
+void fk_run_params_default(fk_run_params* params);
+int fk_run(fk_ctx* ctx, const fk_run_params* params);
+
 /* ------------------------------------------------------------ image export
  * exportFloatImage / exportNormalImage / exportVectorImage (Src/image.cpp:22-405)
  * on the device: the texel map's values (1 float per texel, or 3 for the

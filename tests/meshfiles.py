@@ -165,3 +165,17 @@ def random_ply_mesh(seed, n=30, m=40):
     fnrm = rng.normal(size=(m, 3)).astype(np.float32)
     faces = [list(rng.integers(0, n, 3)) for _ in range(m)]
     return pos, uv, nrm, fnrm, faces
+
+
+def obj_of(mesh):
+    """An OBJ file of a MeshArrays mesh: v / vt / vn with the mesh's own
+    values ('%.9g' round-trips binary32), one v/t/n corner per vertex index.
+    Loading it gives one vertex per face corner with the mesh's positions,
+    texcoords and normals."""
+    out = ["v %.9g %.9g %.9g" % tuple(p) for p in mesh.positions]
+    out += ["vt %.9g %.9g" % tuple(t) for t in mesh.texcoords]
+    out += ["vn %.9g %.9g %.9g" % tuple(n) for n in mesh.normals]
+    v = mesh.vertices.astype(np.int64) + 1
+    for tri in mesh.triangles:
+        out.append("f " + " ".join("%d/%d/%d" % tuple(v[k]) for k in tri))
+    return "\n".join(out) + "\n"

@@ -238,3 +238,15 @@ def test_golden_fixtures(tmp_path):
             continue
         ref = tuple(g["arr_%d_%d" % (i, k)] for k in range(5))
         assert same_mesh(mine, ref), name
+
+
+def test_run_params_defaults():
+    """fk_run_params_default carries FornosParameters' defaults (Src/fornos.h)."""
+    p = api.run_params()
+    assert (p.bvh_tris_per_node, p.tex_width, p.tex_height, p.tex_dilation, p.ignore_backfaces) == (8, 2048, 2048, 16, 1)
+    assert p.mapping == api.MAP_SMOOTH and abs(p.mapping_edge - 0.05) < 1e-7
+    assert p.lo_poly_mesh_normal == p.hi_poly_mesh_normal == api.NORMAL_IMPORT
+    for s in (p.ao, p.bent_normals, p.thickness):
+        assert s.sample_count == 256 and abs(s.min_distance - 0.01) < 1e-7 and s.max_distance == 10.0
+    assert p.height.normalize_output == 1 and p.normals.tangent_space == 1 and p.bent_normals.tangent_space == 1
+    assert not any(getattr(p, k).enabled for k in api.RUN_SOLVERS)
