@@ -73,16 +73,16 @@ def composed(ctx, lo_path, hi_path, mapping, lo_normal, hi_normal, solvers, dila
 
     if "height" in solvers:
         b = ctx.buffer(4 * n)
-        api.gather(ctx, scene, api.GATHER_HEIGHT, coords, tidx, b)
+        api.gather(ctx, scene, api.GATHER_HEIGHT, coords, tidx, b, 0, n)
         s = solvers["height"]
         out["height"] = float_img(b, s["output_path"], 0.0, s.get("max_distance", 0.0), s.get("normalize_output", 1))
     if "positions" in solvers:
         b = ctx.buffer(12 * n)
-        api.gather(ctx, scene, api.GATHER_POSITION, coords, tidx, b)
+        api.gather(ctx, scene, api.GATHER_POSITION, coords, tidx, b, 0, n)
         out["positions"] = api.export_image(ctx, tmap, b, api.EXPORT_VECTOR_F32, (0.0, 0.0), False, 0)[0]
     if "normals" in solvers:
         b = ctx.buffer(12 * n)
-        api.gather(ctx, scene, api.GATHER_NORMAL, coords, tidx, b)
+        api.gather(ctx, scene, api.GATHER_NORMAL, coords, tidx, b, 0, n)
         if solvers["normals"].get("tangent_space", 1):
             api.tangent_space(ctx, tmap, b)
         out["normals"] = normal_img(b, solvers["normals"]["output_path"])
@@ -91,7 +91,8 @@ def composed(ctx, lo_path, hi_path, mapping, lo_normal, hi_normal, solvers, dila
             continue
         s = solvers[key]
         b = ctx.buffer((12 if kind == api.BN else 4) * n)
-        api.hemisphere(ctx, scene, coords, tidx, kind, SPP, s["min_distance"], s["max_distance"], samples, b)
+        api.hemisphere(ctx, scene, coords, tidx, kind, SPP, s["min_distance"], s["max_distance"], samples, b,
+                       count=n)
         if kind == api.BN:
             if s.get("tangent_space", 1):
                 api.tangent_space(ctx, tmap, b)
@@ -151,6 +152,8 @@ def test_runner_images(ctx, tmp_path, mapping, lo_normal, exts):
     for key, img in want.items():
         path = solvers[key]["output_path"]
         assert os.path.exists(path), key
+        if key in ("height", "positions", "normals"):  # maps with content on any covered texel
+            assert np.count_nonzero(img) > img.size // 4, key
         assert same_file(path, img), key
 
 
