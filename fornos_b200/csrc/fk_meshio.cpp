@@ -316,23 +316,78 @@ class PlyReader {
       ascii_.str(buf_.substr(at_));
       ascii_.imbue(std::locale::classic());
     }
-    for (const auto& el : elems_)
+    for (const auto& el : elems_) {
+      // each property's request buffer, found once per element
+      std::vector<std::vector<uint8_t>*> sink(el.props.size(), nullptr);
+      for (size_t k = 0; k < el.props.size(); ++k) {
+        auto it = keys_.find(el.name + "-" + el.props[k].name);
+        if (it == keys_.end()) continue;
+        sink[k] = &reqs_[it->second].bytes;
+        if (binary_ && !el.props[k].list && el.props[k].type != kInvalid) {
+          const size_t more = el.size * (size_t)kStride[el.props[k].type];
+          if (more <= buf_.size() - at_) sink[k]->reserve(sink[k]->size() + more);  // never past the file's bytes
+        }
+      }
+      if (binary_ && fixed_layout(el)) {  // scalars only: fixed-size records, copied without per-value calls
+        size_t rec = 0;
+        for (const auto& p : el.props) rec += (size_t)kStride[p.type];
+        if (rec && el.size > (buf_.size() - at_) / rec) throw BadPly();
+        // per destination buffer, its properties' (record offset, size) in header order: one
+        // instance's values land together, as the value-by-value path appends them
+        std::vector<std::pair<std::vector<uint8_t>*, std::vector<std::pair<size_t, size_t>>>> groups;
+        size_t off = 0;
+        for (size_t k = 0; k < el.props.size(); ++k) {
+          const size_t n = (size_t)kStride[el.props[k].type];
+          if (sink[k]) {
+            size_t g = 0;
+            while (g < groups.size() && groups[g].first != sink[k]) ++g;
+            if (g == groups.size()) groups.push_back({sink[k], {}});
+            groups[g].second.push_back({off, n});
+          }
+          off += n;
+        }
+        const uint8_t* base = reinterpret_cast<const uint8_t*>(buf_.data()) + at_;
+        for (auto& g : groups) {
+          size_t per = 0;
+          for (const auto& f : g.second) per += f.second;
+          const size_t old = g.first->size();
+          g.first->resize(old + el.size * per);
+          uint8_t* dst = g.first->data() + old;
+          for (size_t i = 0; i < el.size; ++i)
+            for (const auto& f : g.second) {
+              const uint8_t* src = base + i * rec + f.first;
+              if (big_)
+                for (size_t b = 0; b < f.second; ++b) dst[b] = src[f.second - 1 - b];
+              else
+                std::memcpy(dst, src, f.second);
+              dst += f.second;
+            }
+        }
+        at_ += el.size * rec;
+        continue;
+      }
       for (size_t i = 0; i < el.size; ++i)
-        for (const auto& p : el.props) {
-          auto it = keys_.find(el.name + "-" + p.name);
-          std::vector<uint8_t>* out = it == keys_.end() ? nullptr : &reqs_[it->second].bytes;
+        for (size_t k = 0; k < el.props.size(); ++k) {
+          const PlyProp& p = el.props[k];
           if (p.list) {
             const uint64_t n = count(p.count_type);
-            for (uint64_t k = 0; k < n; ++k) value(p.type, out);
+            for (uint64_t j = 0; j < n; ++j) value(p.type, sink[k]);
           } else {
-            value(p.type, out);
+            value(p.type, sink[k]);
           }
         }
+    }
   }
 
   const Request& req(int id) const { return reqs_[id]; }
 
  private:
+  static bool fixed_layout(const PlyElem& el) {
+    for (const auto& p : el.props)
+      if (p.list || p.type == kInvalid) return false;
+    return true;
+  }
+
   // One value of type t; stored (native byte order) when out is given.
   void value(PlyType t, std::vector<uint8_t>* out) {
     uint8_t v[8] = {0};
