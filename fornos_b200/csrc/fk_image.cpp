@@ -20,20 +20,53 @@ bool ends_with(const std::string& s, const char* tail) {
   return s.size() >= n && s.compare(s.size() - n, n, tail) == 0;
 }
 
-uint32_t crc32(const uint8_t* p, size_t n) {
-  static uint32_t table[256];
-  static bool ready = false;
-  if (!ready) {
+// CRC-32 (ISO 3309, reflected polynomial 0xEDB88320) by slicing-by-8: eight
+// table lookups per 8 input bytes (Kounavis and Berry, 2008).
+struct Crc32 {
+  uint32_t t[8][256];
+  Crc32() {
     for (uint32_t i = 0; i < 256; ++i) {
       uint32_t c = i;
       for (int k = 0; k < 8; ++k) c = (c & 1) ? 0xEDB88320u ^ (c >> 1) : c >> 1;
-      table[i] = c;
+      t[0][i] = c;
     }
-    ready = true;
+    for (int k = 1; k < 8; ++k)
+      for (uint32_t i = 0; i < 256; ++i) t[k][i] = (t[k - 1][i] >> 8) ^ t[0][t[k - 1][i] & 0xFF];
   }
-  uint32_t crc = 0xFFFFFFFFu;
-  for (size_t i = 0; i < n; ++i) crc = table[(crc ^ p[i]) & 0xFF] ^ (crc >> 8);
-  return ~crc;
+  uint32_t update(uint32_t crc, const uint8_t* p, size_t n) const {  // crc: running value, not inverted
+    for (; n >= 8; p += 8, n -= 8) {
+      uint32_t a, b;
+      std::memcpy(&a, p, 4);  // little-endian host
+      std::memcpy(&b, p + 4, 4);
+      a ^= crc;
+      crc = t[7][a & 0xFF] ^ t[6][(a >> 8) & 0xFF] ^ t[5][(a >> 16) & 0xFF] ^ t[4][a >> 24] ^ t[3][b & 0xFF] ^
+            t[2][(b >> 8) & 0xFF] ^ t[1][(b >> 16) & 0xFF] ^ t[0][b >> 24];
+    }
+    for (; n; --n, ++p) crc = t[0][(crc ^ *p) & 0xFF] ^ (crc >> 8);
+    return crc;
+  }
+};
+
+uint32_t crc32(const uint8_t* p, size_t n) {
+  static const Crc32 table;
+  return ~table.update(0xFFFFFFFFu, p, n);
+}
+
+// Adler-32 (RFC 1950) with the modulo deferred over runs of 5552 bytes, the
+// longest run whose sums cannot overflow 32 bits.
+uint32_t adler32(const uint8_t* p, size_t n) {
+  uint32_t a = 1, b = 0;
+  while (n) {
+    size_t run = n < 5552 ? n : 5552;
+    n -= run;
+    for (; run; --run) {
+      a += *p++;
+      b += a;
+    }
+    a %= 65521;
+    b %= 65521;
+  }
+  return (b << 16) | a;
 }
 
 void put_be32(std::vector<uint8_t>& o, uint32_t v) {
@@ -62,13 +95,14 @@ bool write_file(const char* path, const std::vector<uint8_t>& bytes) {
 }
 
 int write_png(const char* path, uint32_t w, uint32_t h, const uint8_t* rgb) {
-  std::vector<uint8_t> raw;
-  raw.reserve((size_t)h * (3 * (size_t)w + 1));
+  const size_t row = 3 * (size_t)w;
+  std::vector<uint8_t> raw((size_t)h * (row + 1));
   for (uint32_t y = 0; y < h; ++y) {
-    raw.push_back(0);  // filter: none
-    raw.insert(raw.end(), rgb + (size_t)y * 3 * w, rgb + (size_t)(y + 1) * 3 * w);
+    raw[(size_t)y * (row + 1)] = 0;  // filter: none
+    std::memcpy(&raw[(size_t)y * (row + 1) + 1], rgb + (size_t)y * row, row);
   }
   std::vector<uint8_t> z = {0x78, 0x01};  // zlib header: deflate, no preset dictionary
+  z.reserve(2 + raw.size() + 5 * (raw.size() / 65535 + 1) + 4);
   size_t pos = 0;
   do {
     const size_t n = std::min<size_t>(65535, raw.size() - pos);
@@ -78,12 +112,7 @@ int write_png(const char* path, uint32_t w, uint32_t h, const uint8_t* rgb) {
     z.insert(z.end(), raw.begin() + pos, raw.begin() + pos + n);
     pos += n;
   } while (pos < raw.size());
-  uint32_t a = 1, b = 0;  // Adler-32 of the uncompressed data
-  for (uint8_t c : raw) {
-    a = (a + c) % 65521;
-    b = (b + a) % 65521;
-  }
-  put_be32(z, (b << 16) | a);
+  put_be32(z, adler32(raw.data(), raw.size()));  // of the uncompressed data
   std::vector<uint8_t> o = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n'};
   std::vector<uint8_t> ihdr;
   put_be32(ihdr, w);
@@ -181,11 +210,19 @@ int write_exr(const char* path, uint32_t w, uint32_t h, uint32_t nplanes, const 
   o.push_back(0);
   const size_t table = o.size(), block = 8 + (size_t)nplanes * w * 2;
   for (uint32_t y = 0; y < h; ++y) put_le(o, table + 8 * (size_t)h + y * block, 8);
+  size_t at = o.size();
+  o.resize(at + (size_t)h * block);
   for (uint32_t y = 0; y < h; ++y) {
-    put_le(o, y, 4);
-    put_le(o, (uint64_t)nplanes * w * 2, 4);
-    for (uint32_t c = 0; c < nplanes; ++c)
-      for (uint32_t x = 0; x < w; ++x) put_le(o, half_of(planes[((size_t)c * h + y) * w + x]), 2);
+    const uint32_t head[2] = {y, (uint32_t)(nplanes * w * 2)};  // little-endian host
+    std::memcpy(&o[at], head, 8);
+    at += 8;
+    for (uint32_t c = 0; c < nplanes; ++c) {
+      const float* src = planes + ((size_t)c * h + y) * w;
+      for (uint32_t x = 0; x < w; ++x, at += 2) {
+        const uint16_t v = half_of(src[x]);
+        std::memcpy(&o[at], &v, 2);
+      }
+    }
   }
   return write_file(path, o) ? FK_OK : FK_ERR_INVALID;
 }
