@@ -57,6 +57,11 @@ constexpr uint32_t kNone = 0xFFFFFFFFu;
 bool read_file(const char* path, std::string& out) {
   FILE* f = std::fopen(path, "rb");
   if (!f) return false;
+  if (std::fseek(f, 0, SEEK_END) == 0) {  // one read of the whole file where its size is known
+    const long size = std::ftell(f);
+    if (size > 0) out.reserve((size_t)size);
+    std::rewind(f);
+  }
   char chunk[1 << 16];
   size_t n;
   while ((n = std::fread(chunk, 1, sizeof(chunk), f)) > 0) out.append(chunk, n);
@@ -371,7 +376,25 @@ class PlyReader {
           const PlyProp& p = el.props[k];
           if (p.list) {
             const uint64_t n = count(p.count_type);
-            for (uint64_t j = 0; j < n; ++j) value(p.type, sink[k]);
+            if (binary_ && p.type != kInvalid) {  // the list's items in one copy, byte-swapped per item
+              const size_t st = (size_t)kStride[p.type];
+              if (n > (buf_.size() - at_) / st) throw BadPly();
+              if (sink[k]) {
+                const size_t old = sink[k]->size();
+                sink[k]->resize(old + n * st);
+                uint8_t* dst = sink[k]->data() + old;
+                const uint8_t* src = reinterpret_cast<const uint8_t*>(buf_.data()) + at_;
+                if (big_) {
+                  for (size_t j = 0; j < n; ++j)
+                    for (size_t b = 0; b < st; ++b) dst[j * st + b] = src[j * st + st - 1 - b];
+                } else {
+                  std::memcpy(dst, src, n * st);
+                }
+              }
+              at_ += n * st;
+            } else {
+              for (uint64_t j = 0; j < n; ++j) value(p.type, sink[k]);
+            }
           } else {
             value(p.type, sink[k]);
           }
@@ -505,11 +528,11 @@ int load_ply(const char* path, fk_mesh& m) {
     const int fs = kStride[f.type];
     if (f.type == kInvalid || f.type == kF32 || f.type == kF64) return FK_ERR_INVALID;
     if (f.bytes.size() < (size_t)fs * 3 * f.count) return FK_ERR_INVALID;
-    m.vertices.reserve(9 * f.count);
-    m.triangles.reserve(3 * f.count);
+    m.vertices.resize(9 * f.count);
+    m.triangles.resize(3 * f.count);
     uint32_t normal = kNone;
     for (size_t i = 0; i < f.count; ++i) {
-      const uint32_t v0 = (uint32_t)(m.vertices.size() / 3);
+      const uint32_t v0 = (uint32_t)(3 * i);
       if (from == kFace) normal = (uint32_t)i * 3;
       for (size_t j = 0; j < 3; ++j) {
         const uint8_t* q = f.bytes.data() + (size_t)fs * (3 * i + j);
@@ -523,9 +546,14 @@ int load_ply(const char* path, fk_mesh& m) {
           default: vi = *q; break;  // kU8
         }
         if (from == kVertex) normal = vi;
-        m.vertices.insert(m.vertices.end(), {vi, uvs >= 0 ? vi : kNone, normal});
+        uint32_t* vx = &m.vertices[9 * i + 3 * j];
+        vx[0] = vi;
+        vx[1] = uvs >= 0 ? vi : kNone;
+        vx[2] = normal;
       }
-      m.triangles.insert(m.triangles.end(), {v0, v0 + 1, v0 + 2});
+      m.triangles[3 * i] = v0;
+      m.triangles[3 * i + 1] = v0 + 1;
+      m.triangles[3 * i + 2] = v0 + 2;
     }
     return FK_OK;
   } catch (const BadPly&) {

@@ -17,6 +17,7 @@
 // std::random_device); AO and bent normals with equal sample parameters
 // share one traversal.
 #include <cstring>
+#include <future>
 #include <string>
 #include <vector>
 
@@ -138,10 +139,12 @@ int fk_run(fk_ctx* ctx, const fk_run_params* p) {
   if ((rc = o.alloc(16 * nn, &coords)) != FK_OK || (rc = o.alloc(4 * nn, &tidx)) != FK_OK) return rc;
   if ((rc = fk_meshmap(ctx, o.scene, o.map, p->ignore_backfaces, 0, n, coords, tidx)) != FK_OK) return rc;
 
-  // exports: one device image buffer per call, then the writer of the path's format
+  // exports: one device image buffer, reused; each downloaded image is encoded
+  // and written on a thread of its own while the device runs the next
+  // solvers (the futures are waited for before any return)
   fk_buf* image = nullptr;
   if ((rc = o.alloc(12 * (size_t)w * h, &image)) != FK_OK) return rc;
-  std::vector<uint8_t> host(12 * (size_t)w * h);
+  std::vector<std::pair<std::string, std::future<int>>> writes;
   auto export_map = [&](const fk_buf* data, const char* path, bool vec3, bool vector_only, float lo_f, float hi_f,
                         int normalize, int dilate) -> int {
     const Format f = format_of(path);
@@ -156,11 +159,16 @@ int fk_run(fk_ctx* ctx, const fk_run_params* p) {
     float minmax[2];
     int r = fk_export_image(ctx, o.map, data, &ep, image, minmax);
     const size_t bytes = f == kRgb8 ? 3 * (size_t)w * h : (vec3 ? 12 : 4) * (size_t)w * h;
+    std::vector<float> host((bytes + 3) / 4);
     if (r == FK_OK) r = fk_buf_download(ctx, image, 0, host.data(), bytes);
     if (r != FK_OK) return r;
-    r = f == kRgb8 ? fk_image_write_rgb8(path, w, h, host.data())
-                   : fk_image_write_exr(path, w, h, vec3 ? 3 : 1, reinterpret_cast<const float*>(host.data()));
-    return r == FK_OK ? FK_OK : fk_fail(ctx, r, std::string("fk_run: cannot write ") + path);
+    const uint32_t planes = vec3 ? 3 : 1;
+    std::string file(path);
+    writes.emplace_back(file, std::async(std::launch::async, [host = std::move(host), file, f, w, h, planes]() {
+      return f == kRgb8 ? fk_image_write_rgb8(file.c_str(), w, h, reinterpret_cast<const uint8_t*>(host.data()))
+                        : fk_image_write_exr(file.c_str(), w, h, planes, host.data());
+    }));
+    return FK_OK;
   };
   auto gather = [&](int kind, size_t width, int tangent, fk_buf** out) -> int {
     int r = o.alloc(4 * width * nn, out);
@@ -235,6 +243,10 @@ int fk_run(fk_ctx* ctx, const fk_run_params* p) {
         (rc = export_map(th_out, th.output_path, false, false, 0.0f, 0.0f, 1, p->tex_dilation)) != FK_OK)
       return rc;
   }
+  rc = FK_OK;
+  for (auto& wr : writes)
+    if (wr.second.get() != FK_OK) rc = fk_fail(ctx, FK_ERR_INVALID, "fk_run: cannot write " + wr.first);
+  if (rc != FK_OK) return rc;
   FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   int st = 0;
   FK_CUDA(ctx, cudaMemcpy(&st, ctx->status, sizeof(int), cudaMemcpyDeviceToHost));
