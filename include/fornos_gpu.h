@@ -685,7 +685,7 @@ int fk_denoise_apply(fk_denoiser* d, const fk_texel_map* map, const fk_buf* imag
                      const fk_buf* ao_in, const fk_buf* bn_in, uint32_t offset, uint32_t count, fk_buf* ao_out,
                      fk_buf* bn_out);
 
-/* The denoised AO + bent-normal bake with the plain bake as its judge:
+/* The denoised AO + bent-normal bake, checked against the plain bake:
  *   1. AO + BN at low_samples over every texel;
  *   2. features, network;
  *   3. per tile of tile x tile texels, verify_cells^2 spot checks (the first
