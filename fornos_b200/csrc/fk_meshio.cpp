@@ -333,6 +333,11 @@ class PlyReader {
           if (more <= buf_.size() - at_) sink[k]->reserve(sink[k]->size() + more);  // never past the file's bytes
         }
       }
+      if (binary_ && zero_width(el)) {  // unknown-type scalars only: no bytes to read, however many instances
+        for (const auto* sk : sink)
+          if (sk && el.size) throw BadPly();  // a requested unknown-type value (tinyply throws on the first)
+        continue;
+      }
       if (binary_ && fixed_layout(el)) {  // scalars only: fixed-size records, copied without per-value calls
         size_t rec = 0;
         for (const auto& p : el.props) rec += (size_t)kStride[p.type];
@@ -392,6 +397,8 @@ class PlyReader {
                 }
               }
               at_ += n * st;
+            } else if (binary_) {  // unknown item type: no bytes per item
+              if (sink[k] && n) throw BadPly();
             } else {
               for (uint64_t j = 0; j < n; ++j) value(p.type, sink[k]);
             }
@@ -405,6 +412,11 @@ class PlyReader {
   const Request& req(int id) const { return reqs_[id]; }
 
  private:
+  static bool zero_width(const PlyElem& el) {
+    for (const auto& p : el.props)
+      if (p.list || p.type != kInvalid) return false;
+    return true;
+  }
   static bool fixed_layout(const PlyElem& el) {
     for (const auto& p : el.props)
       if (p.list || p.type == kInvalid) return false;

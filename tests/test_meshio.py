@@ -250,3 +250,55 @@ def test_run_params_defaults():
         assert s.sample_count == 256 and abs(s.min_distance - 0.01) < 1e-7 and s.max_distance == 10.0
     assert p.height.normalize_output == 1 and p.normals.tangent_space == 1 and p.bent_normals.tangent_space == 1
     assert not any(getattr(p, k).enabled for k in api.RUN_SOLVERS)
+
+
+def test_ply_zero_width_data_is_not_looped(tmp_path):
+    """Binary elements or lists whose items have an unknown type hold no bytes:
+    skipped at once however large the count, rejected when requested."""
+    import struct
+    import time
+    hdr = lambda body: ("ply\nformat binary_little_endian 1.0\n" + body + "end_header\n").encode()
+    v = "".join("property float %s\n" % k for k in ("x", "y", "z", "s", "t", "nx", "ny", "nz"))
+    vdata = b"".join(struct.pack("<8f", i, 0, 0, 0, 0, 0, 0, 1) for i in range(3))
+    fdata = struct.pack("<B3I", 3, 0, 1, 2)
+    files = {
+        "element": hdr("element vertex 3\n" + v + "element face 1\nproperty list uchar uint vertex_indices\n"
+                       "element junk 999999999999\nproperty half q\n") + vdata + fdata,
+        "list": hdr("element vertex 3\n" + v + "element face 1\nproperty list uint half junk\n"
+                    "property list uchar uint vertex_indices\n") + vdata + struct.pack("<I", 4000000000) + fdata,
+    }
+    for name, data in files.items():
+        t = time.time()
+        m = load(write(tmp_path, name + ".ply", data))
+        assert time.time() - t < 5 and m is not None and len(m[4]) == 1, name
+    requested = hdr("element vertex 3\n" + v.replace("float x", "half x") + "element face 1\n"
+                    "property list uchar uint vertex_indices\n") + vdata + fdata
+    assert load(write(tmp_path, "req.ply", requested)) is None
+
+
+def test_mutated_files_load_or_reject(tmp_path):
+    """Seeded byte mutations, truncations and splices of valid OBJ / PLY files:
+    each loads into a valid mesh or is rejected, never more."""
+    rng = np.random.default_rng(2024)
+    pos, uv, nrm, fnrm, faces = MF.random_ply_mesh(1, n=12, m=10)
+    bases = [(".ply", MF.ply_bytes(pos, faces, fmt=f, uv=uv, nrm=nrm)) for f in
+             ("binary_little_endian", "binary_big_endian", "ascii")]
+    bases += [(".obj", MF.obj_text(3, c, n_pos=8, n_faces=6).encode()) for c in ("v", "vt", "vn", "vtn")]
+    loaded = 0
+    for it in range(400):
+        ext, data = bases[it % len(bases)]
+        b = bytearray(data)
+        for _ in range(int(rng.integers(1, 4))):
+            k = int(rng.integers(3))
+            if k == 0:
+                b[int(rng.integers(len(b)))] = int(rng.integers(256))
+            elif k == 1:
+                b = b[:int(rng.integers(1, len(b)))]
+            else:
+                i = int(rng.integers(len(b) + 1))
+                b[i:i] = bytes(rng.integers(0, 256, int(rng.integers(1, 9)), dtype=np.uint8))
+        m = load(write(tmp_path, "f" + ext, bytes(b)))
+        if m is not None:
+            loaded += 1
+            assert len(m[3]) == 0 or int(m[3][:, 0].max()) < len(m[0])
+    assert loaded > 0
