@@ -722,7 +722,7 @@ RUN_SOLVERS = ("height", "positions", "normals", "ao", "bent_normals", "thicknes
 
 
 def run_params(**fields):
-    """FornosParameters (Src/fornos.h:29-110) as fk_run_params: the
+    """FornosParameters (Src/fornos.h:35-123) as fk_run_params: the
     reference's defaults, overridden by `fields`.  Shared fields by name
     (lo_poly_mesh_path, hi_poly_mesh_path, lo_poly_mesh_normal,
     hi_poly_mesh_normal, bvh_tris_per_node, tex_width, tex_height,

@@ -1,7 +1,7 @@
-// Mesh files: Mesh::loadFile (Src/mesh.cpp:597-603) with its Wavefront OBJ
-// reader (Mesh::loadWavefrontObj, :235-455) and its PLY reader
-// (Mesh::loadPly, :515-590) on top of tinyply 2.0's header and data parsing
-// (3rdParty/tinyply/tinyply.cpp:266-599).  A file gives the mesh the
+// Mesh files: Mesh::loadFile (Src/mesh.cpp:612-617) with its Wavefront OBJ
+// reader (Mesh::loadWavefrontObj, :235-456) and its PLY reader
+// (Mesh::loadPly, :515-601) on top of tinyply 2.0's header and data parsing
+// (3rdParty/tinyply/tinyply.cpp:186-603).  A file gives the mesh the
 // reference's loader gives, array for array, whenever that mesh is valid
 // (every face corner names an existing position); a file the reference
 // rejects is rejected (FK_ERR_INVALID).
@@ -26,7 +26,7 @@
 // last key, as tinyply's shared buffer does.  Faces are read as consecutive
 // triples of the flattened index lists (the reference's loop; polygons with
 // more corners are not split into fans); a face normal's index is 3 x the face
-// (Src/mesh.cpp:571).  Where the reference's result is unusable this loader
+// (Src/mesh.cpp:582).  Where the reference's result is unusable this loader
 // defines one:
 //   * no s t or no normals: the reference dereferences a null buffer; here the
 //     texcoords / normals stay empty and the vertices' indices are UINT32_MAX,
@@ -492,7 +492,7 @@ class PlyReader {
   std::istringstream ascii_;
 };
 
-// copyPlyData (Src/mesh.cpp:459-513): float or double tuples of width w
+// copyPlyData (Src/mesh.cpp:460-513): float or double tuples of width w
 // narrowed to float; other types give nothing.
 bool tuples(const Request* r, int w, std::vector<float>& out) {
   out.clear();

@@ -59,7 +59,7 @@ Format format_of(const char* path) {
   return kNone;
 }
 
-// NormalImport (Src/fornos.h:31).
+// NormalImport (Src/fornos.h:35).
 int import_normals(fk_ctx* ctx, fk_mesh* m, int how) {
   if (how == FK_NORMAL_COMPUTE_PER_FACE) return fk_mesh_compute_normals_device(ctx, m, FK_NORMALS_FACE);
   if (how == FK_NORMAL_COMPUTE_PER_VERTEX) return fk_mesh_compute_normals_device(ctx, m, FK_NORMALS_VERTEX);

@@ -121,8 +121,8 @@ int fk_mesh_create(const fk_mesh_desc* desc, fk_mesh** out);
  * mesh changes or is freed). */
 int fk_mesh_describe(const fk_mesh* mesh, fk_mesh_desc* out);
 int fk_mesh_copy(const fk_mesh* mesh, fk_mesh** out);                 /* Mesh::createCopy */
-/* Mesh::loadFile (Src/mesh.cpp:597-603): ".obj" through the Wavefront reader
- * (:235-455), ".ply" through the PLY reader (:515-590, tinyply 2.0); the mesh
+/* Mesh::loadFile (Src/mesh.cpp:612-617): ".obj" through the Wavefront reader
+ * (:235-456), ".ply" through the PLY reader (:515-601, tinyply 2.0); the mesh
  * the reference's loader returns, array for array.  FK_ERR_INVALID for a file
  * the reference rejects, another extension, or a mesh whose corners name
  * positions the file lacks; an OBJ file that cannot be opened gives an empty
@@ -481,7 +481,7 @@ int fk_bake(fk_ctx* ctx, const fk_bake_desc* desc, fk_bake_out* out);
 /* ------------------------------------------------------------ runner
  * FornosRunner::start, then FornosRunner::run until every task has finished
  * (Src/fornos.cpp:53-251), with the fields of FornosParameters
- * (Src/fornos.h:29-110): mesh files in, image files out.  Meshes load with
+ * (Src/fornos.h:35-123): mesh files in, image files out.  Meshes load with
  * fk_mesh_load, normals / tangents / the welded direction copy are computed
  * on the device, the texel map by fk_raster_uv, the BVH by fk_scene_build
  * (bvh_tris_per_node, depth 8192); each enabled solver's result is exported

@@ -235,7 +235,7 @@ class Reference:
         L.ref_mesh_free.argtypes = [_vp]
 
     def load_mesh(self, path):
-        """Mesh::loadFile (Src/mesh.cpp:597-603): the loaded arrays as
+        """Mesh::loadFile (Src/mesh.cpp:612-617): the loaded arrays as
         (positions, texcoords, normals, vertices, triangles), or None when the
         loader returns null.  Never call it on a PLY file without s / t or
         without normals: the reference's loader dereferences a null buffer

@@ -237,7 +237,7 @@ int ref_export_vector(uint32_t w, uint32_t h, uint32_t count, const uint32_t* id
   return 0;
 }
 
-// Mesh::loadFile (Src/mesh.cpp:597-603).  ref_mesh_load returns the mesh or
+// Mesh::loadFile (Src/mesh.cpp:612-617).  ref_mesh_load returns the mesh or
 // null; ref_mesh_sizes gives position, texcoord, normal, vertex and triangle
 // counts; ref_mesh_arrays copies the arrays out (positions / normals 3
 // floats, texcoords 2, vertices and triangles 3 u32 each).

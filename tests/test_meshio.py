@@ -1,5 +1,5 @@
 """Mesh files (fk_mesh_load) against the reference's own loaders
-(Mesh::loadFile, Src/mesh.cpp:235-603, and tinyply 2.0, compiled from source
+(Mesh::loadFile, Src/mesh.cpp:235-617, and tinyply 2.0, compiled from source
 in oracle/_ref): positions, texcoords and normals bit for bit, vertex and
 triangle tables exactly, and the same files rejected.  Without the reference
 build the committed golden fixtures (tests/golden/meshio.npz, made by
