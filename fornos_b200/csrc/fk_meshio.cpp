@@ -92,7 +92,8 @@ struct Corner {
 bool obj_float(const char*& s, float& v, bool required = true) {
   char* end;
   errno = 0;
-  v = (float)strtod_l(s, &end, c_numeric());
+  const locale_t c = c_numeric();
+  v = (float)(c ? strtod_l(s, &end, c) : std::strtod(s, &end));  // without a C locale object: the process's
   if (required && end == s) return false;
   s = end;
   return errno == 0;
