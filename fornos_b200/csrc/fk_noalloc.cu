@@ -13,8 +13,7 @@
 // Host code cannot pass the array's name to a kernel: on the host that name is
 // only a stand-in, not a device address.  The device address is obtained once
 // per device with cudaGetSymbolAddress, with that device current, on the first
-// call made on that device; that first call should therefore come before any
-// stream capture.  All calls share the one array, which keeps whatever the last
+// call made on that device.  All calls share the one array, which keeps whatever the last
 // call left in it: the queue and status words are cleared at the start of each
 // call (the distance slots are always written before they are read), and calls
 // whose work overlaps on the GPU (different streams, or threads on one device

@@ -319,8 +319,7 @@ int fk_gather(fk_ctx* ctx, const fk_scene* scene, int kind, const fk_buf* coords
  * samples4 as fk_samples_cosine fills them, outputs as fk_hemisphere writes
  * them); `stream` is a cudaStream_t (NULL = default stream).  The scene's
  * device must be current.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress), so make it before any stream capture.
- * Every call reuses the same array: calls whose work may overlap on the GPU
+ * device address (cudaGetSymbolAddress).  Every call reuses the same array: calls whose work may overlap on the GPU
  * race on it and must be serialised by the caller. */
 #define FK_NOALLOC_MAX_RAYS (1u << 22)
 int fk_hemisphere_noalloc(const fk_scene* scene, const float* coords4, const uint32_t* tidx, int kind,
