@@ -3,8 +3,10 @@
 Names follow the reference's host API: Mesh (Src/mesh.h), BVH.create_binary
 (Src/bvh.h), TexelMap = MapUV + CompressedMapUV (Src/compute.h), MeshMapping
 (Src/meshmapping.h) and the six solvers (Src/solver_*.h) with init /
-run_step / get_results / progress.  FornosRunner (Src/fornos.h:129-149)
-drives a whole bake from FornosParameters-like settings.
+run_step / get_results / progress.  Mesh.load is Mesh::loadFile (OBJ / PLY).
+FornosRunner::start + run (Src/fornos.cpp:53-251) is run(ctx, **fields),
+with the fields of FornosParameters (Src/fornos.h:35-123): mesh files in,
+image files out (fk_run); bake() is the same bake from host arrays.
 """
 import ctypes
 import os
