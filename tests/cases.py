@@ -69,3 +69,14 @@ def bits(a):
 def same_bits(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return a.shape == b.shape and np.array_equal(bits(a), bits(b))
+
+
+def record(test, **values):
+    """Appends one JSON line of measured values to tests/.out/records.jsonl
+    (ignored by git): figures a test bounds, kept for reading after a run."""
+    import json
+    import os
+    d = os.path.join(os.path.dirname(os.path.abspath(__file__)), ".out")
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "records.jsonl"), "a") as fh:
+        fh.write(json.dumps(dict(test=test, **{k: float(v) for k, v in values.items()})) + "\n")

@@ -11,7 +11,7 @@ import pytest
 
 from fornos_b200 import api
 from tests import cases
-from tests.cases import bits, same_bits
+from tests.cases import bits, record, same_bits
 
 pytestmark = pytest.mark.gpu
 
@@ -139,12 +139,14 @@ def test_hemisphere_ordered_matches(ctx, oracle, name, kind, sched):
     ref, rhits, tidx = oracle_hemi(oracle, c, mm, kind, samples, spp, lo, hi)
     hit = tidx != api.MISS
     exact_hits = hits[hit] == rhits[hit]
-    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
-    assert (~exact_hits).mean() <= 1e-3
     if kind == api.BN:
         ok = np.all(bits(out[hit]) == bits(ref[hit]), axis=1)
     else:
         ok = bits(out[hit]) == bits(ref[hit])
+    record("ordered:%s:%d:%d" % (name, kind, sched), texels=hit.sum(), hit_diff=(~exact_hits).mean(),
+           out_diff=(~ok).mean())
+    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
+    assert (~exact_hits).mean() <= 1e-3
     assert (~ok).mean() <= 1e-3
 
 
@@ -163,6 +165,7 @@ def test_hemisphere_ordered4_matches(ctx, oracle, name, kind, exact):
     ref, rhits, tidx = oracle_hemi(oracle, c, mm, k, samples, spp, lo, hi)
     hit = tidx != api.MISS
     out, hits = got[0], got[1]
+    record("ordered4:%s:%d:%d" % (name, kind, exact), texels=hit.sum(), hit_diff=(hits[hit] != rhits[hit]).mean())
     assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
     assert (hits[hit] != rhits[hit]).mean() <= 1e-3
     ok = bits(out[hit]) == bits(ref[hit])
@@ -197,6 +200,8 @@ def test_either_inner_tree_matches(ctx, oracle, name, kind, trav, tree):
     if trav == api.TRAVERSE_SKIP:
         assert np.array_equal(hits[hit], rhits[hit]) and same_bits(out[hit], ref[hit])
         return
+    record("tree:%s:%d:%d:%d" % (name, kind, trav, tree), texels=hit.sum(),
+           hit_diff=(hits[hit] != rhits[hit]).mean())
     assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
     assert (hits[hit] != rhits[hit]).mean() <= 1e-3
     ok = bits(out[hit]) == bits(ref[hit])
