@@ -146,8 +146,8 @@ def test_hemisphere_ordered_matches(ctx, oracle, name, kind, sched):
     record("ordered:%s:%d:%d" % (name, kind, sched), texels=hit.sum(), hit_diff=(~exact_hits).mean(),
            out_diff=(~ok).mean())
     assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
-    assert (~exact_hits).mean() <= 1e-3
-    assert (~ok).mean() <= 1e-3
+    assert (~exact_hits).mean() <= 1e-4  # at most 0.01 % of texels
+    assert (~ok).mean() <= 1e-4
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -167,7 +167,7 @@ def test_hemisphere_ordered4_matches(ctx, oracle, name, kind, exact):
     out, hits = got[0], got[1]
     record("ordered4:%s:%d:%d" % (name, kind, exact), texels=hit.sum(), hit_diff=(hits[hit] != rhits[hit]).mean())
     assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
-    assert (hits[hit] != rhits[hit]).mean() <= 1e-3
+    assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
     ok = bits(out[hit]) == bits(ref[hit])
     if kind == api.BN:
         ok = np.all(ok, axis=1)
@@ -203,7 +203,7 @@ def test_either_inner_tree_matches(ctx, oracle, name, kind, trav, tree):
     record("tree:%s:%d:%d:%d" % (name, kind, trav, tree), texels=hit.sum(),
            hit_diff=(hits[hit] != rhits[hit]).mean())
     assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
-    assert (hits[hit] != rhits[hit]).mean() <= 1e-3
+    assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
     ok = bits(out[hit]) == bits(ref[hit])
     if kind == api.BN:
         ok = np.all(ok, axis=1)
