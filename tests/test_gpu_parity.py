@@ -165,12 +165,13 @@ def test_hemisphere_ordered4_matches(ctx, oracle, name, kind, exact):
     ref, rhits, tidx = oracle_hemi(oracle, c, mm, k, samples, spp, lo, hi)
     hit = tidx != api.MISS
     out, hits = got[0], got[1]
-    record("ordered4:%s:%d:%d" % (name, kind, exact), texels=hit.sum(), hit_diff=(hits[hit] != rhits[hit]).mean())
-    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
-    assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
     ok = bits(out[hit]) == bits(ref[hit])
     if kind == api.BN:
         ok = np.all(ok, axis=1)
+    record("ordered4:%s:%d:%d" % (name, kind, exact), texels=hit.sum(), hit_diff=(hits[hit] != rhits[hit]).mean(),
+           out_diff=(~ok).mean())
+    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
+    assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
     assert (~ok).mean() <= 1e-3
     if kind == api.AO_BN:
         bref, bhits, _ = oracle_hemi(oracle, c, mm, api.BN, samples, spp, lo, hi)
@@ -200,13 +201,13 @@ def test_either_inner_tree_matches(ctx, oracle, name, kind, trav, tree):
     if trav == api.TRAVERSE_SKIP:
         assert np.array_equal(hits[hit], rhits[hit]) and same_bits(out[hit], ref[hit])
         return
-    record("tree:%s:%d:%d:%d" % (name, kind, trav, tree), texels=hit.sum(),
-           hit_diff=(hits[hit] != rhits[hit]).mean())
-    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
-    assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
     ok = bits(out[hit]) == bits(ref[hit])
     if kind == api.BN:
         ok = np.all(ok, axis=1)
+    record("tree:%s:%d:%d:%d" % (name, kind, trav, tree), texels=hit.sum(),
+           hit_diff=(hits[hit] != rhits[hit]).mean(), out_diff=(~ok).mean())
+    assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
+    assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
     assert (~ok).mean() <= 1e-3
 
 
