@@ -302,3 +302,17 @@ def test_mutated_files_load_or_reject(tmp_path):
             loaded += 1
             assert len(m[3]) == 0 or int(m[3][:, 0].max()) < len(m[0])
     assert loaded > 0
+
+
+def test_bench_ply_layout(reference, tmp_path):
+    """The binary PLY the benchmark's files-to-images step writes reads the same
+    through both loaders, with the mesh's own positions and texcoords."""
+    import bench
+    from fornos_b200 import workloads as W
+    lo, _ = W.plane_pair(seed=2, lo_quads=6, hi_quads=8, bumps=3)
+    p = str(tmp_path / "lo.ply")
+    bench.write_ply(p, lo)
+    mine, ref = load(p), reference.load_mesh(p)
+    assert same_mesh(mine, ref)
+    v = lo.vertices.astype(np.int64)
+    assert same_bits(mine[0], lo.positions[v[:, 0]]) and same_bits(mine[1], lo.texcoords[v[:, 1]])
