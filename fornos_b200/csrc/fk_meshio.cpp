@@ -37,6 +37,7 @@
 //   * data shorter than the header announces, or an ASCII value that does not
 //     parse: the reference goes on with zeros or uninitialised memory; here the
 //     file is rejected.
+#include <algorithm>
 #include <clocale>
 #include <cerrno>
 #include <cstdio>
@@ -46,6 +47,7 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "fk_internal.h"
@@ -114,21 +116,24 @@ bool rest_blank(const char* s) {
   return true;
 }
 
-int load_obj(const char* path, fk_mesh& m) {
-  std::string buf;
-  if (!read_file(path, buf)) return FK_OK;  // unreadable: empty mesh
+// One range of whole lines: its statements in file order.  `first_t` /
+// `first_n` are the index kinds of the range's first face corner, which every
+// later corner of the range must repeat.
+struct ObjRange {
   std::vector<float> pos, uv, nrm;
   std::vector<Corner> corners;
-  std::vector<std::pair<size_t, size_t>> faces;  // first corner, corner count
-  bool fixed = false, has_t = false, has_n = false;
-  size_t at = 0;
-  const size_t size = buf.size();
-  while (at < size) {
+  std::vector<uint32_t> face_corners;  // corners per face
+  bool any = false, first_t = false, first_n = false;
+  int rc = FK_OK;
+};
+
+void parse_obj_lines(std::string& buf, size_t at, size_t stop, ObjRange& r) {
+  while (at < stop) {
     size_t e = buf.find('\n', at);
-    if (e == std::string::npos) e = size;
+    if (e == std::string::npos || e > stop) e = stop;
     char* line = &buf[at];
     const size_t len = e - at;
-    if (e < size) buf[e] = '\0';  // C parsing stops at the line's end
+    if (e < buf.size() && buf[e] == '\n') buf[e] = '\0';  // C parsing stops at the line's end
     at = e + 1;
     size_t b = 0;
     while (b < len && blank(line[b])) ++b;
@@ -141,63 +146,143 @@ int load_obj(const char* path, fk_mesh& m) {
     if (tok[0] == '#') continue;
     if (tok[0] == 'v' && tl == 1) {
       float x, y, z, w;
-      if (!obj_float(s, x) || !obj_float(s, y) || !obj_float(s, z) || !obj_float(s, w, false) || !rest_blank(s))
-        return FK_ERR_INVALID;
-      pos.insert(pos.end(), {x, y, z});
+      if (!obj_float(s, x) || !obj_float(s, y) || !obj_float(s, z) || !obj_float(s, w, false) || !rest_blank(s)) {
+        r.rc = FK_ERR_INVALID;
+        return;
+      }
+      r.pos.insert(r.pos.end(), {x, y, z});
     } else if (tok[0] == 'v' && tl == 2 && tok[1] == 't') {
       float u, v, w;
-      if (!obj_float(s, u) || !obj_float(s, v) || !obj_float(s, w, false) || !rest_blank(s)) return FK_ERR_INVALID;
-      uv.insert(uv.end(), {u, v});
+      if (!obj_float(s, u) || !obj_float(s, v) || !obj_float(s, w, false) || !rest_blank(s)) {
+        r.rc = FK_ERR_INVALID;
+        return;
+      }
+      r.uv.insert(r.uv.end(), {u, v});
     } else if (tok[0] == 'v' && tl == 2 && tok[1] == 'n') {
       float i, j, k;
-      if (!obj_float(s, i) || !obj_float(s, j) || !obj_float(s, k) || !rest_blank(s)) return FK_ERR_INVALID;
-      nrm.insert(nrm.end(), {i, j, k});
+      if (!obj_float(s, i) || !obj_float(s, j) || !obj_float(s, k) || !rest_blank(s)) {
+        r.rc = FK_ERR_INVALID;
+        return;
+      }
+      r.nrm.insert(r.nrm.end(), {i, j, k});
     } else if (tok[0] == 'f' && tl == 1) {
-      const size_t first = corners.size();
+      const size_t first = r.corners.size();
       while (!rest_blank(s)) {
         Corner c{0, 0, 0};
-        if (!obj_int(s, c.p)) return FK_ERR_INVALID;
-        if (*s == '/') {
+        bool ok = obj_int(s, c.p);
+        if (ok && *s == '/') {
           ++s;
-          if (!obj_int(s, c.t, false)) return FK_ERR_INVALID;
+          ok = obj_int(s, c.t, false);
         }
-        if (*s == '/') {
+        if (ok && *s == '/') {
           ++s;
-          if (!obj_int(s, c.n)) return FK_ERR_INVALID;
+          ok = obj_int(s, c.n);
         }
-        if (!fixed) {
-          has_t = c.t != 0;
-          has_n = c.n != 0;
-          fixed = true;
-        } else if ((c.t != 0) != has_t || (c.n != 0) != has_n) {
-          return FK_ERR_INVALID;
+        if (ok && !r.any) {
+          r.first_t = c.t != 0;
+          r.first_n = c.n != 0;
+          r.any = true;
+        } else if (ok && ((c.t != 0) != r.first_t || (c.n != 0) != r.first_n)) {
+          ok = false;
         }
-        corners.push_back(c);
+        if (!ok) {
+          r.rc = FK_ERR_INVALID;
+          return;
+        }
+        r.corners.push_back(c);
         while (blank(*s)) ++s;
       }
-      faces.emplace_back(first, corners.size() - first);
+      r.face_corners.push_back((uint32_t)(r.corners.size() - first));
     }
     // vp, p, l and unknown statements are skipped
   }
-  m.positions.swap(pos);
-  m.texcoords.swap(uv);
-  m.normals.swap(nrm);
-  m.vertices.reserve(3 * corners.size());
-  for (const auto& f : faces) {
-    uint32_t first = kNone, prev = kNone;
-    for (size_t i = 0; i < f.second; ++i) {
-      const Corner& c = corners[f.first + i];
-      const uint32_t v = (uint32_t)(m.vertices.size() / 3);
-      m.vertices.insert(m.vertices.end(), {(uint32_t)(c.p - 1), c.t ? (uint32_t)(c.t - 1) : kNone,
-                                           c.n ? (uint32_t)(c.n - 1) : kNone});
-      if (first == kNone) {
-        first = v;
-      } else if (prev == kNone) {
-        prev = v;
-      } else {
-        m.triangles.insert(m.triangles.end(), {first, prev, v});
-        prev = v;
+}
+
+void parse_obj_range(std::string& buf, size_t at, size_t stop, ObjRange& r) {
+  try {
+    parse_obj_lines(buf, at, stop, r);
+  } catch (const std::bad_alloc&) {
+    r.rc = FK_ERR_NOMEM;
+  }
+}
+
+int load_obj(const char* path, fk_mesh& m) {
+  std::string buf;
+  if (!read_file(path, buf)) return FK_OK;  // unreadable: empty mesh
+  // Lines are independent but for the corner format the file's first corner
+  // fixes, so large files are parsed in ranges of whole lines on threads of
+  // their own and merged in file order; the format rule is then checked
+  // across ranges (each range already checked its corners against its own
+  // first one).  Any error anywhere rejects the file, as a sequential pass would.
+  const size_t size = buf.size();
+  const size_t min_range = (size_t)4 << 20;
+  size_t parts = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 32));
+  parts = std::max<size_t>(1, std::min(parts, size / min_range));
+  std::vector<size_t> cut(1, 0);
+  for (size_t k = 1; k < parts; ++k) {
+    size_t c = std::max(cut.back(), size * k / parts);
+    const size_t nl = buf.find('\n', c);
+    if (nl == std::string::npos) break;
+    cut.push_back(nl + 1);
+  }
+  cut.push_back(size);
+  std::vector<ObjRange> ranges(cut.size() - 1);
+  {
+    std::vector<std::thread> pool;
+    size_t started = 0;
+    try {
+      for (; ranges.size() > 1 && started < ranges.size(); ++started)
+        pool.emplace_back(parse_obj_range, std::ref(buf), cut[started], cut[started + 1], std::ref(ranges[started]));
+    } catch (const std::exception&) {  // no more threads: the rest on this one
+    }
+    for (size_t k = started; k < ranges.size(); ++k) parse_obj_range(buf, cut[k], cut[k + 1], ranges[k]);
+    for (auto& t : pool) t.join();
+  }
+  const ObjRange* lead = nullptr;
+  size_t np = 0, nt = 0, nn = 0, nc = 0, nf = 0;
+  for (const auto& r : ranges) {
+    if (r.rc != FK_OK) return r.rc;
+    if (r.any) {
+      if (!lead) lead = &r;
+      else if (r.first_t != lead->first_t || r.first_n != lead->first_n) return FK_ERR_INVALID;
+    }
+    np += r.pos.size();
+    nt += r.uv.size();
+    nn += r.nrm.size();
+    nc += r.corners.size();
+    nf += r.face_corners.size();
+  }
+  m.positions.reserve(np);
+  m.texcoords.reserve(nt);
+  m.normals.reserve(nn);
+  for (const auto& r : ranges) {
+    m.positions.insert(m.positions.end(), r.pos.begin(), r.pos.end());
+    m.texcoords.insert(m.texcoords.end(), r.uv.begin(), r.uv.end());
+    m.normals.insert(m.normals.end(), r.nrm.begin(), r.nrm.end());
+  }
+  m.vertices.resize(3 * nc);
+  m.triangles.reserve(3 * (nc > 2 * nf ? nc - 2 * nf : 0));
+  uint32_t v = 0;
+  for (const auto& r : ranges) {
+    size_t c0 = 0;
+    for (const uint32_t count : r.face_corners) {
+      uint32_t first = kNone, prev = kNone;
+      for (uint32_t i = 0; i < count; ++i, ++v) {  // every corner its own vertex, polygons as fans
+        const Corner& c = r.corners[c0 + i];
+        uint32_t* x = &m.vertices[3 * (size_t)v];
+        x[0] = (uint32_t)(c.p - 1);
+        x[1] = c.t ? (uint32_t)(c.t - 1) : kNone;
+        x[2] = c.n ? (uint32_t)(c.n - 1) : kNone;
+        if (first == kNone) {
+          first = v;
+        } else if (prev == kNone) {
+          prev = v;
+        } else {
+          m.triangles.insert(m.triangles.end(), {first, prev, v});
+          prev = v;
+        }
       }
+      c0 += count;
     }
   }
   return FK_OK;

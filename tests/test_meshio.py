@@ -316,3 +316,24 @@ def test_bench_ply_layout(reference, tmp_path):
     assert same_mesh(mine, ref)
     v = lo.vertices.astype(np.int64)
     assert same_bits(mine[0], lo.positions[v[:, 0]]) and same_bits(mine[1], lo.texcoords[v[:, 1]])
+
+
+def test_obj_large_file_in_ranges(reference, tmp_path):
+    """Files of more than a few MB are parsed in ranges of whole lines on
+    several threads and merged in file order: the same mesh as the reference's
+    loader, and the same rejections, including errors and a corner format that
+    only a later range sees, and a first range without faces."""
+    block = MF.obj_text(31, "vtn", n_pos=4000, n_faces=6000)
+    if not block.endswith("\n"):
+        block += "\n"
+    text = block * 12  # about 11 MB, every quirk in every range; indices are absolute, so they still resolve
+    rng = np.random.default_rng(8)
+    verts = "".join("v %.9g %.9g %.9g\n" % tuple(p) for p in rng.normal(size=(150000, 3)).astype(np.float32))
+    cases = {"blocks": text, "late syntax error": text + "v 1 2\n", "late corner format": text + "f 1 2 3\n",
+             "faceless first range": verts + text}
+    for name, body in cases.items():
+        p = write(tmp_path, "big.obj", body)
+        ref = reference.load_mesh(p)
+        mine = load(p)
+        assert same_mesh(mine, ref), name
+        assert (ref is None) == name.startswith("late"), name
