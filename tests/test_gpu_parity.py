@@ -172,7 +172,7 @@ def test_hemisphere_ordered4_matches(ctx, oracle, name, kind, exact):
            out_diff=(~ok).mean())
     assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
     assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
-    assert (~ok).mean() <= 1e-3
+    assert (~ok).mean() <= 1e-4
     if kind == api.AO_BN:
         bref, bhits, _ = oracle_hemi(oracle, c, mm, api.BN, samples, spp, lo, hi)
         assert (got[3][hit] != bhits[hit]).mean() <= 1e-3
@@ -208,7 +208,7 @@ def test_either_inner_tree_matches(ctx, oracle, name, kind, trav, tree):
            hit_diff=(hits[hit] != rhits[hit]).mean(), out_diff=(~ok).mean())
     assert np.abs(hits[hit].astype(np.int64) - rhits[hit]).max() <= 1
     assert (hits[hit] != rhits[hit]).mean() <= 1e-4  # at most 0.01 % of texels
-    assert (~ok).mean() <= 1e-3
+    assert (~ok).mean() <= 1e-4
 
 
 def test_ordered4_needs_the_dynamic_schedule(ctx, oracle):
