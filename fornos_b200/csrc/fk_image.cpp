@@ -119,7 +119,17 @@ int write_png(const char* path, uint32_t w, uint32_t h, const uint8_t* rgb) {
   put_be32(ihdr, h);
   ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});  // 8-bit RGB, deflate, filter method 0, no interlace
   png_chunk(o, "IHDR", ihdr);
-  png_chunk(o, "IDAT", z);
+  // the zlib stream over IDAT chunks of at most 1 GiB (a chunk's length is
+  // limited to 2^31 - 1 bytes; decoders join consecutive IDAT chunks)
+  const size_t kIdat = (size_t)1 << 30;
+  for (size_t at = 0; at < z.size(); at += kIdat) {
+    const size_t n = std::min(kIdat, z.size() - at);
+    put_be32(o, (uint32_t)n);
+    const size_t start = o.size();
+    o.insert(o.end(), {'I', 'D', 'A', 'T'});
+    o.insert(o.end(), z.begin() + at, z.begin() + at + n);
+    put_be32(o, crc32(o.data() + start, n + 4));
+  }
   png_chunk(o, "IEND", {});
   return write_file(path, o) ? FK_OK : FK_ERR_INVALID;
 }
