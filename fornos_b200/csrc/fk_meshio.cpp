@@ -252,6 +252,7 @@ int load_obj(const char* path, fk_mesh& m) {
     nc += r.corners.size();
     nf += r.face_corners.size();
   }
+  if (nc >= 0xFFFFFFFFull || np / 3 >= 0xFFFFFFFFull) return FK_ERR_INVALID;  // beyond 32-bit vertex / position indices
   m.positions.reserve(np);
   m.texcoords.reserve(nt);
   m.normals.reserve(nn);
@@ -623,6 +624,7 @@ int load_ply(const char* path, fk_mesh& m) {
         !tuples(norms >= 0 ? &r.req(norms) : nullptr, 3, m.normals))
       return FK_ERR_INVALID;
     const Request& f = r.req(faces);
+    if (f.count >= 0xFFFFFFFFull / 3) return FK_ERR_INVALID;  // corners beyond 32-bit vertex indices
     const int fs = kStride[f.type];
     if (f.type == kInvalid || f.type == kF32 || f.type == kF64) return FK_ERR_INVALID;
     if (f.bytes.size() < (size_t)fs * 3 * f.count) return FK_ERR_INVALID;
