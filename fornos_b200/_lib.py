@@ -202,6 +202,7 @@ _SIGS = {
     "fk_scene_build": (c_int, [c_vp, c_vp, c_u32, c_u32, ctypes.POINTER(c_vp)]),
     "fk_export_image": (c_int, [c_vp, c_vp, c_vp, ctypes.POINTER(ExportParams), c_vp, f32p]),
     "fk_image_write_rgb8": (c_int, [ctypes.c_char_p, c_u32, c_u32, c_vp]),
+    "fk_image_write_png": (c_int, [ctypes.c_char_p, c_u32, c_u32, c_vp, c_int]),
     "fk_image_write_exr": (c_int, [ctypes.c_char_p, c_u32, c_u32, c_u32, f32p]),
     "fk_diag_scene_tree": (c_int, [c_vp, c_vp, c_int, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),
     "fk_diag_sah_host": (c_int, [c_vp, c_u32, f32p, c_u32, ctypes.POINTER(c_u32), ctypes.POINTER(c_u32)]),

@@ -430,14 +430,18 @@ def export_image(ctx, tmap, data, mode, filter_range=(0.0, 0.0), normalize=True,
     return out, (float(mm[0]), float(mm[1]))
 
 
-def write_image(path, image):
-    """Writes an exported image: h x w x 3 uint8 as .png / .tga, h x w or
-    3 x h x w float32 as .exr (HALF channels B, or B, G, R)."""
+def write_image(path, image, png_level=None):
+    """Writes an exported image: h x w x 3 uint8 as .png (filtered and deflated;
+    png_level 0-9 picks the zlib level, 0 = stored) / .tga (run-length coded),
+    h x w or 3 x h x w float32 as .exr (HALF channels B, or B, G, R)."""
     image = np.ascontiguousarray(image)
     lib = L.load()
     if image.dtype == np.uint8:
         h, w, _ = image.shape
-        _check(lib.fk_image_write_rgb8(path.encode(), w, h, image.ctypes.data))
+        if png_level is not None and path.endswith(".png"):
+            _check(lib.fk_image_write_png(path.encode(), w, h, image.ctypes.data, int(png_level)))
+        else:
+            _check(lib.fk_image_write_rgb8(path.encode(), w, h, image.ctypes.data))
     else:
         planes = np.ascontiguousarray(image.astype(np.float32).reshape(-1, *image.shape[-2:]))
         _check(lib.fk_image_write_exr(path.encode(), planes.shape[2], planes.shape[1], planes.shape[0],

@@ -60,7 +60,7 @@ def build(force=False, verbose=False):
             print(p.stdout + p.stderr)
     if changed:
         cmd = [NVCC, "-shared", "-cudart", "static", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB] + \
-            objs + ["-lpthread"]
+            objs + ["-lpthread", "-lz"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -559,12 +559,17 @@ int fk_export_image(fk_ctx* ctx, const fk_texel_map* map, const fk_buf* data, co
 
 /* Host writers of exported images (stbi_write_png / stbi_write_tga /
  * tinyexr's SaveEXRImageToFile in Src/image.cpp): an RGB8 image (rows in
- * buffer order) as PNG (".png", stored deflate blocks) or TGA (".tga",
- * uncompressed, bottom-left origin); float planes as a scanline EXR without
+ * buffer order) as PNG (".png", rows filtered and deflated at zlib level 6)
+ * or TGA (".tga", run-length coded, bottom-left origin), the kinds of file
+ * stb_image_write writes; float planes as a scanline EXR without
  * compression, channels "B" (1 plane) or "B", "G", "R" (3 planes), stored as
  * HALF with tinyexr's conversion (rounded up in magnitude on the first dropped
  * bit).  The decoded pixels equal the reference's files'. */
 int fk_image_write_rgb8(const char* path, uint32_t width, uint32_t height, const uint8_t* rgb);
+/* PNG at a chosen zlib level: 0 stores the rows unfiltered (fastest, largest),
+ * 1-9 filter each row as stb_image_write does and deflate them
+ * (fk_image_write_rgb8 uses 6). */
+int fk_image_write_png(const char* path, uint32_t width, uint32_t height, const uint8_t* rgb, int level);
 int fk_image_write_exr(const char* path, uint32_t width, uint32_t height, uint32_t planes, const float* data);
 
 /* ------------------------------------------------------------ diagnostics
