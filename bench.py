@@ -3,7 +3,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fornos|reference]
                     [--workload plane2048|sphere512|icosphere4096|plane250|batch|denoise]
                     [--traverse auto|ordered|skip|ordered4] [--schedule auto|static|dynamic]
-                    [--tree sah|reference] [--no-denoise] [--denoise-tex T] [--no-cpu-baseline]
+                    [--tree sah|reference] [--no-denoise] [--no-batch] [--denoise-tex T] [--no-cpu-baseline]
 
 One step = one full plain bake of the workload with every input resident in
 HBM: mesh mapping (2 rays / texel), height, position and tangent-space normal
@@ -16,9 +16,13 @@ own seeded replica of the workload (weak scaling, no data-path collective).
 
 The default line also carries fk_run's time from mesh files to image files
 (`files_to_images`: the workload written as PLY, all six maps written as PNG /
-EXR) and the denoised-vs-plain comparison at 4096x4096
-(`denoise`); --workload batch measures 64 batched jobs and --workload denoise
-the comparison alone.  --tree reference walks the reference's inner BVH nodes
+EXR), the denoised-vs-plain comparison at 4096x4096 (`denoise`) and the
+batched-bake comparison over the first 16 jobs of the batch workload
+(`batch`); --workload batch measures all 64 batched jobs and --workload
+denoise the comparison alone.  With the CPU baseline on, `parity` compares
+the timed bake's outputs with the reference's at the CPU run's texels, and
+the denoise and batch objects carry the same check of their plain and
+batched paths.  --tree reference walks the reference's inner BVH nodes
 instead of the surface-area tree built at upload.
 
 --impl reference times the reference's own CPU implementation of the path
@@ -49,10 +53,10 @@ WORKLOADS = {
         gen=lambda seed: W.plane_pair(seed=seed, lo_quads=64, hi_quads=1024, bumps=200),
         tex=2048, spp=256, min_d=0.001, max_d=0.3, bakers=("height", "position", "normals", "ao", "bn", "thick")),
     "sphere512": dict(
-        desc="plain bake, 512x512: 32x16 UV-sphere low-poly, 512x256 perturbed UV-sphere high-poly, height, "
-             "tangent-space normals, AO 64 spp (min 0.001, max 0.5)",
+        desc="plain bake, 512x512: 32x16 UV-sphere low-poly, 512x256 perturbed UV-sphere high-poly, mapping with "
+             "maximum distance 0.1, height, tangent-space normals, AO 64 spp (min 0.001, max 0.5)",
         gen=lambda seed: W.sphere_pair(seed=seed),
-        tex=512, spp=64, min_d=0.001, max_d=0.5, bakers=("height", "normals", "ao")),
+        tex=512, spp=64, min_d=0.001, max_d=0.5, map_max=0.1, bakers=("height", "normals", "ao")),
     "icosphere4096": dict(
         desc="plain large bake, 4096x4096: subdivision-3 icosphere low-poly (cube-projection UVs), "
              "subdivision-9 icosphere high-poly (5,242,880 tris, 6-octave gradient noise), AO / bent normals / "
@@ -78,6 +82,12 @@ NCU_TRAFFIC = {"plane250": 257.6e6, "plane2048": 4.08e9}
 def rays_per_texel(wl):
     spp = wl["spp"]
     return 2 + spp * sum(k in wl["bakers"] for k in ("ao", "bn", "thick"))
+
+
+def traversals_per_texel(wl):
+    """Rays actually traced per texel: AO and bent normals share one traversal."""
+    b = wl["bakers"]
+    return 2 + wl["spp"] * ((("ao" in b) or ("bn" in b)) + ("thick" in b))
 
 
 # ---------------------------------------------------------------- clocks
@@ -298,12 +308,14 @@ def run_fornos(args, wl, rank, world):
     samples = api.samples_cosine(spp, api.PERMS, args.seed)
     sbuf = ctx.upload(samples)
     B = {k: ctx.buffer(w * max(n, 1)) for k, w in (("coords", 16), ("tidx", 4), ("height", 4), ("position", 12),
-                                                  ("normals", 12), ("ao", 4), ("bn", 12), ("thick", 4))}
+                                                  ("normals", 12), ("ao", 4), ("bn", 12), ("thick", 4),
+                                                  ("hits_ao", 4), ("hits_bn", 4), ("hits_thick", 4))}
+    map_max = wl.get("map_max", api.FLT_MAX)
     bakers = wl["bakers"]
     hemi_events = []
 
     def step(record):
-        api.meshmap(ctx, scene, tmap, True, B["coords"], B["tidx"])
+        api.meshmap(ctx, scene, tmap, True, B["coords"], B["tidx"], max_dist=map_max)
         if "height" in bakers:
             api.gather(ctx, scene, api.GATHER_HEIGHT, B["coords"], B["tidx"], B["height"], 0, n)
         if "position" in bakers:
@@ -318,7 +330,8 @@ def run_fornos(args, wl, rank, world):
             a.record(stream)
             api.hemisphere(ctx, scene, B["coords"], B["tidx"], kind, spp, lo_d, hi_d, sbuf,
                            B["ao"] if kind != api.BN else B["bn"], B["bn"] if kind == api.AO_BN else None,
-                           None, None, 0, n, traverse=trav)
+                           B["hits_ao"] if kind != api.BN else B["hits_bn"],
+                           B["hits_bn"] if kind == api.AO_BN else None, 0, n, traverse=trav)
             b.record(stream)
             launches.append((a, b, kind))
             if "bn" in bakers:
@@ -327,7 +340,7 @@ def run_fornos(args, wl, rank, world):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             api.hemisphere(ctx, scene, B["coords"], B["tidx"], api.THICK, spp, lo_d, hi_d, sbuf, B["thick"],
-                           None, None, None, 0, n, traverse=trav)
+                           None, B["hits_thick"], None, 0, n, traverse=trav)
             b.record(stream)
             launches.append((a, b, api.THICK))
         if record:
@@ -385,7 +398,8 @@ def run_fornos(args, wl, rank, world):
     kw = dict(height_map="height" in bakers, position_map="position" in bakers, normals_map="normals" in bakers,
               ao=sampler if "ao" in bakers else None,
               bent_normals=dict(sampler, tangent_space=True) if "bn" in bakers else None,
-              thickness=sampler if "thick" in bakers else None, traverse=trav)
+              thickness=sampler if "thick" in bakers else None, traverse=trav,
+              mapping_max_distance=wl.get("map_max", 0.0))
 
     def e2e_step():
         api.bake(ctx, h_nodes, h_pos, h_nrm, tex, tex, h_pix, h_pixt, h_idx, out_arrays, **kw)
@@ -423,9 +437,11 @@ def run_fornos(args, wl, rank, world):
         "config": {"workload": args.workload, "desc": wl["desc"], "texels": n, "texture": tex, "spp": spp,
                    "high_poly_triangles": prep.triangles, "bvh_nodes": info["node_count"],
                    "bvh_depth": info["depth"], "traverse": args.traverse, "schedule": args.schedule, "tree": args.tree,
-                   "rays_per_texel": rays_per_texel(wl),
-                   "rays_counted": "2 mapping + spp each for AO, bent normals, thickness (AO and bent normals "
-                                   "share one traversal)",
+                   "rays_per_texel": rays_per_texel(wl), "traversals_per_texel": traversals_per_texel(wl),
+                   "rays_counted": "2 mapping + spp each for AO, bent normals, thickness, as the reference traces "
+                                   "them; AO and bent normals share one traversal here, so the rays traced are "
+                                   "traversals_per_texel per texel (value x traversals_per_texel / rays_per_texel "
+                                   "Mrays/s)",
                    "l2": "inputs larger than L2 (scene %.0f MB resident)" % (info["device_bytes"] / 1e6),
                    "bvh_build_s": round(prep.bvh_s, 3), "scene_build_device_ms": round(scene_build_ms, 1),
                    "preprocess_host_ms": round(prep.prep_s * 1e3, 1), "preprocess_device_ms": round(prep_device_ms, 1),
@@ -476,13 +492,15 @@ DENOISE = dict(tex=4096, low=16, full=1024, label=4096, min_d=0.001, max_d=0.3, 
                mae_texels=65536)
 
 
-def denoise_compare(ctx, stream, prep, scene, weights, seed, tex=4096):
+def denoise_compare(ctx, stream, prep, scene, weights, seed, tex=4096, check=None):
     """AO + bent normals of the plane workload's scene at tex x tex texels
     (4096 for the reported comparison; smaller sizes serve as profiling cases):
     the plain 1024-sample bake against the verified 16-sample + network bake
     (spot checks and per-tile fallback included), each timed with CUDA events
     over one whole pass, and each scored by mean absolute error against
-    4096-sample values on 65,536 random texels with a mapping hit."""
+    4096-sample values on 65,536 random texels with a mapping hit.  check:
+    called with the plain bake's texel map and buffers (the CPU-baseline
+    leg's parity check of the plain path)."""
     import torch
 
     from fornos_b200 import api
@@ -515,6 +533,7 @@ def denoise_compare(ctx, stream, prep, scene, weights, seed, tex=4096):
                                             None, None, off, cnt)
     plain(0, max(1, n // 100))  # warm-up on 1 % of the texels
     t_plain, _, clk_plain = timed(lambda: plain(0, n))
+    plain_parity = check(tm, coords, tidx, pao, pbn, d, seed + 12) if check else None
     dao, dbn = ctx.buffer(4 * n), ctx.buffer(12 * n)
     bake = lambda: dn.bake(scene, tm, coords, tidx, low, full, dao, dbn, low_samples=d["low"],
                            full_samples=d["full"], min_distance=d["min_d"], max_distance=d["max_d"], tile=d["tile"],
@@ -580,6 +599,8 @@ def denoise_compare(ctx, stream, prep, scene, weights, seed, tex=4096):
         "network_kernel": net,
     }
     res["speedup"] = round(t_plain / t_dn, 2)
+    if plain_parity is not None:
+        res["plain_parity"] = plain_parity
     for b in (tm, coords, tidx, low, full, label, pao, pbn, dao, dbn, lao, lbn):
         b.free()
     dn.free()
@@ -625,20 +646,63 @@ class CpuBaseline:
         self.stride = max(1, n // 64)
 
     def run(self, stride=None):
+        """One timed pass over every stride-th texel: the reference's mapping,
+        then its sampling shaders.  The reference's mapping has no distance
+        limit; a workload's limit m is applied to its result (hits at t >= m
+        become misses), which is what walks started at m return (grazing hits
+        on box faces aside).  The outputs are kept in self.last for the
+        parity check."""
         stride = stride or self.stride
         n, impl = self.n, self.impl
         sel = np.arange(0, n, stride, dtype=np.uint32)
         t0 = time.perf_counter()
         c_sel, t_sel = impl.meshmap(self.nodes, self.pos4, self.pix8[sel], True)
+        if self.wl.get("map_max") is not None:
+            far = (t_sel != 0xFFFFFFFF) & ~(c_sel[:, 0] < np.float32(self.wl["map_max"]))
+            t_sel[far] = 0xFFFFFFFF
+            c_sel[far] = (np.finfo(np.float32).max, 0.0, 0.0, 0.0)
         coords = np.zeros((n, 4), np.float32)
         tidx = np.full(n, 0xFFFFFFFF, np.uint32)
         coords[sel], tidx[sel] = c_sel, t_sel
+        outs = {}
         for k in self.kinds:
-            impl.hemisphere(k, self.nodes, self.pos4, self.nrm4, coords, tidx, self.samples, self.spp,
-                            self.wl["min_d"], self.wl["max_d"], texels=sel)
+            r = impl.hemisphere(k, self.nodes, self.pos4, self.nrm4, coords, tidx, self.samples, self.spp,
+                                self.wl["min_d"], self.wl["max_d"], texels=sel)
+            outs[k] = r[0] if isinstance(r, tuple) else r
         dt = time.perf_counter() - t0
+        self.last = dict(sel=sel, coords=c_sel, tidx=t_sel, outs=outs)
         rays = len(sel) * (2 + self.spp * len(self.kinds))
         return rays / dt / 1e6, rays, dt, len(sel)
+
+    def parity(self, B, n, cmap):
+        """The GPU bake's buffers (B, n texels) at the texels of the last run
+        against the reference's outputs there (oracle/parity.py)."""
+        from oracle import parity
+        L = self.last
+        sel, hit = L["sel"], L["tidx"] != parity.MISS
+        take = lambda name, w, dt=np.float32: B[name].download(dt, n if w == 1 else (n, w))[sel]
+        rep = {"texels": int(len(sel)),
+               "mapping": parity.mapping(L["coords"], L["tidx"], take("coords", 4), take("tidx", 1, np.uint32))}
+        if self.wl.get("map_max") is not None:
+            rep["mapping"]["note"] = ("the reference's mapping has no distance limit: its hits at t >= %g are "
+                                      "dropped before comparing" % self.wl["map_max"])
+        if 0 in L["outs"]:
+            rep["ao"] = parity.sampled(L["outs"][0], take("ao", 1), hit, self.spp,
+                                       gpu_hits=take("hits_ao", 1, np.uint32))
+        if 1 in L["outs"]:
+            bn = L["outs"][1]
+            if "bn" in self.wl["bakers"]:  # the bench bake stores bent normals in tangent space
+                bn = self.impl.tangent_transform(cmap["normals"][sel], cmap["tangents"][sel],
+                                                 cmap["bitangents"][sel], bn)
+            rep["bn"] = parity.sampled(bn, take("bn", 3), hit)
+        if 2 in L["outs"]:
+            rep["thick"] = parity.sampled(L["outs"][2], take("thick", 1), hit)
+        rep["meets_bar"] = parity.meets_bar(rep)
+        rep["bar"] = ("texel map, hit indices, barycentrics bit-exact; sampled outputs bit-exact on all but "
+                      "<= 0.01% of texels, occluder counts within one sample")
+        rep["compared_with"] = "%s (%s)" % ("oracle/_ref: the reference's shaders compiled on the host"
+                                             if self.kind == "reference" else "the oracle restatement", self.kind)
+        return rep
 
     def calibrate(self, budget_s):
         """Chooses the texel stride so one run takes about budget_s seconds."""
@@ -654,6 +718,42 @@ class CpuBaseline:
         return "every %d-th of %d compressed texels (%d texels, %d rays): mapping + %s at %d spp" % (
             self.stride, self.n, m, rays, " + ".join({0: "AO", 1: "BN", 2: "thickness"}[k] for k in self.kinds),
             self.spp)
+
+
+def plain_path_check(cpu, prep, texels=1024):
+    """Parity check of the denoise comparison's plain 1024-sample AO + bent
+    normal bake: the reference's mapping and sampling shaders (cpu.impl) on
+    `texels` random texels with a mapping hit, against the GPU buffers."""
+    from oracle import parity
+
+    def check(tm, coords, tidx, pao, pbn, d, sample_seed):
+        n = tm.count
+        g_t = tidx.download(np.uint32, n)
+        rng = np.random.default_rng(sample_seed)
+        sel = np.sort(rng.choice(np.nonzero(g_t != parity.MISS)[0], min(texels, n), replace=False)).astype(np.uint32)
+        cm = tm.download()
+        pix8 = np.zeros((len(sel), 8), np.float32)
+        pix8[:, 0:3], pix8[:, 4:7] = cm["positions"][sel], cm["directions"][sel]
+        impl = cpu.impl
+        c_sel, t_sel = impl.meshmap(prep.nodes, prep.pos4, pix8, True)
+        rep = {"texels": int(len(sel)), "samples": d["full"],
+               "mapping": parity.mapping(c_sel, t_sel, coords.download(np.float32, (n, 4))[sel], g_t[sel])}
+        full_c = np.zeros((n, 4), np.float32)
+        full_t = np.full(n, parity.MISS, np.uint32)
+        full_c[sel], full_t[sel] = c_sel, t_sel
+        table = impl.samples(d["full"], 4096, sample_seed)
+        hit = t_sel != parity.MISS
+        for k, name, buf, w in ((0, "ao", pao, 1), (1, "bn", pbn, 3)):
+            r = impl.hemisphere(k, prep.nodes, prep.pos4, prep.nrm4, full_c, full_t, table, d["full"], d["min_d"],
+                                d["max_d"], texels=sel)
+            r = r[0] if isinstance(r, tuple) else r
+            g = buf.download(np.float32, n if w == 1 else (n, 3))[sel]
+            rep[name] = parity.sampled(r, g, hit, d["full"] if k == 0 else None)
+        rep["meets_bar"] = parity.meets_bar(rep)
+        rep["compared_with"] = cpu.kind
+        return rep
+
+    return check
 
 
 def run_reference_arm(args, wl):
@@ -700,41 +800,48 @@ def batch_jobs(seed, count):
     return jobs
 
 
-def run_batch_bench(args):
-    """64 jobs: per-job fk_hemisphere launches vs one batched persistent launch
-    (default schedule, autotuned, and autotuned + CUDA graph).  AO only."""
+def batch_compare(ctx, stream, seed, njobs, check=None):
+    """The batched-bake comparison over `njobs` jobs of batch_jobs(seed):
+    per-job fk_hemisphere launches (context defaults, then the tuned
+    schedule) against one batched persistent launch (default schedule,
+    autotuned, autotuned in a CUDA graph).  AO only.  Scenes are built on the
+    device (fk_scene_build); check(job, outputs) is the CPU-baseline leg's
+    oracle comparison of one job."""
     import torch
 
     from fornos_b200 import api
-    torch.cuda.set_device(0)
-    stream = torch.cuda.Stream()
-    ctx = api.Context(0)
-    ctx.set_stream(stream.cuda_stream)
-    specs = batch_jobs(args.seed, args.batch_jobs)
+    specs = batch_jobs(seed, njobs)
     jobs, keep = [], []
     tables = {}
+    t_prep = time.perf_counter()
     for s in specs:
-        wl = dict(gen=s["gen"], tex=s["tex"])
-        prep = Prepared(wl, s["seed"])
-        tm = api.TexelMap.from_meshes(ctx, prep.lm, prep.dm, s["tex"], s["tex"])
-        scene = api.Scene(ctx, prep.nodes, prep.pos4, prep.nrm4)
+        lo, hi = s["gen"](s["seed"])
+        hm = api.Mesh(hi)
+        hm.compute_vertex_normals()
+        lm = api.Mesh(lo)
+        lm.compute_tangent_space()
+        dm = lm.copy()
+        dm.compute_vertex_normals_aggressive()
+        tm = api.TexelMap.from_meshes(ctx, lm, dm, s["tex"], s["tex"])
+        scene = api.Scene.build(ctx, hm, 8, 8192)
         n = tm.count
         coords, tidx = ctx.buffer(16 * n), ctx.buffer(4 * n)
         api.meshmap(ctx, scene, tm, True, coords, tidx)
         if s["spp"] not in tables:
-            tables[s["spp"]] = ctx.upload(api.samples_cosine(s["spp"], api.PERMS, args.seed))
+            tables[s["spp"]] = ctx.upload(api.samples_cosine(s["spp"], api.PERMS, seed))
         jobs.append(dict(scene=scene, coords=coords, tidx=tidx, texel_count=n, spp=s["spp"], min_distance=s["min_d"],
                          max_distance=s["max_d"], samples=tables[s["spp"]], out0=ctx.buffer(4 * n),
-                         hits0=ctx.buffer(4 * n), triangles=prep.triangles, tex=s["tex"]))
-        keep.append((tm, prep))
+                         hits0=ctx.buffer(4 * n), triangles=hi.triangle_count, tex=s["tex"], seed=s["seed"],
+                         mesh=hm, tmap=tm))
+        keep.append((tm, lm, dm))
     ctx.sync()
+    prep_s = time.perf_counter() - t_prep
     rays = sum(j["texel_count"] * j["spp"] for j in jobs)
-
     clocks = {}
 
     def timed(fn, name):
-        # one pass per call (tens of seconds of GPU work, every job's scene and
-        # texels already resident), with the SM clock sampled during it
+        # one pass per call, every job's scene and texels already resident,
+        # with the SM clock sampled during it
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         with ClockSampler(0) as clk, torch.cuda.stream(stream):
             stream.synchronize()
@@ -745,13 +852,15 @@ def run_batch_bench(args):
         clocks.setdefault(name, []).append(clk.summary())
         return a.elapsed_time(b)
 
-    def per_job():
+    def per_job(traverse=0):
         for j in jobs:
             api.hemisphere(ctx, j["scene"], j["coords"], j["tidx"], api.AO, j["spp"], j["min_distance"],
-                           j["max_distance"], j["samples"], j["out0"], None, j["hits0"], None, 0, j["texel_count"])
+                           j["max_distance"], j["samples"], j["out0"], None, j["hits0"], None, 0, j["texel_count"],
+                           traverse=traverse)
 
     outs = [dict(out0=ctx.buffer(4 * j["texel_count"]), hits0=ctx.buffer(4 * j["texel_count"])) for j in jobs]
     batch = api.Batch(ctx, [dict(j, **o) for j, o in zip(jobs, outs)], api.AO)
+    default = ctx.get_tuning()
     # per-job and batched passes alternate, twice, so that neither arm runs on
     # a cooler GPU than the other; each arm keeps its faster pass
     t_jobs, t_batch = [], []
@@ -761,28 +870,124 @@ def run_batch_bench(args):
     want = [(j["out0"].download(np.float32, j["texel_count"]), j["hits0"].download(np.uint32, j["texel_count"]))
             for j in jobs]
     tuned = batch.tune()
-    t_tuned = timed(lambda: batch.run(), "batch_tuned")
+    # the same tuned schedule for per-job launches and the batch
+    ctx.set_tuning(refill=tuned["refill"], leaf_batch=tuned["leaf_batch"], speculate=tuned["speculate"])
+    t_jobs_tuned, t_tuned, t_graph = [], [], []
     batch.capture()
-    t_graph = timed(lambda: batch.replay(), "batch_tuned_graph")
-    t_jobs, t_batch = min(t_jobs), min(t_batch)
-    identical = all(np.array_equal(o["out0"].download(np.float32, j["texel_count"]).view(np.uint32), w[0].view(np.uint32))
+    for _ in range(2):
+        t_jobs_tuned.append(timed(lambda: per_job(tuned["traverse"]), "per_job_tuned"))
+        t_tuned.append(timed(lambda: batch.run(), "batch_tuned"))
+        t_graph.append(timed(lambda: batch.replay(), "batch_tuned_graph"))
+    ctx.set_tuning(**default)
+    t_jobs, t_batch, t_jobs_tuned, t_tuned, t_graph = (min(v) for v in (t_jobs, t_batch, t_jobs_tuned, t_tuned,
+                                                                        t_graph))
+    identical = all(np.array_equal(o["out0"].download(np.float32, j["texel_count"]).view(np.uint32),
+                                   w[0].view(np.uint32))
                     and np.array_equal(o["hits0"].download(np.uint32, j["texel_count"]), w[1])
                     for j, o, w in zip(jobs, outs, want))
     mr = lambda ms: round(rays / (ms * 1e-3) / 1e6, 2)
-    return {
-        "metric": "Mrays/s (batched AO bake of %d jobs)" % len(jobs), "value": mr(t_graph), "unit": "Mrays/s",
-        "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generated meshes)",
-        "config": {"workload": "batch%d" % len(jobs), "rays": rays,
-                   "texels": sum(j["texel_count"] for j in jobs),
-                   "triangles": [j["triangles"] for j in jobs], "textures": [j["tex"] for j in jobs],
-                   "spp": [j["spp"] for j in jobs]},
-        "per_job_launches": {"ms": round(t_jobs, 2), "mrays": mr(t_jobs)},
+    res = {
+        "jobs": len(jobs), "rays": rays, "texels": sum(j["texel_count"] for j in jobs),
+        "triangles": [j["triangles"] for j in jobs], "textures": [j["tex"] for j in jobs],
+        "spp": [j["spp"] for j in jobs], "prep_s": round(prep_s, 1),
+        "per_job_launches": {"ms": round(t_jobs, 2), "mrays": mr(t_jobs), "tuning": default},
         "batch_default": {"ms": round(t_batch, 2), "mrays": mr(t_batch)},
+        "per_job_tuned": {"ms": round(t_jobs_tuned, 2), "mrays": mr(t_jobs_tuned)},
         "batch_tuned": {"ms": round(t_tuned, 2), "mrays": mr(t_tuned), "tuning": tuned},
         "batch_tuned_graph": {"ms": round(t_graph, 2), "mrays": mr(t_graph), "info": batch.info()},
+        "graph_vs_per_job_tuned": round(t_jobs_tuned / t_graph, 4),
         "batch_equals_per_job": bool(identical),
         "clocks": clocks,
     }
+    if check is not None:
+        k = int(np.argmin([j["triangles"] for j in jobs]))  # the smallest job: its reference run is quick
+        res["oracle_check"] = check(jobs[k], outs[k], k)
+    return res
+
+
+def batch_check(cpu_kind="reference", texels=256):
+    """Oracle comparison of one batched job (the CPU-baseline leg): the
+    reference's AO shader (oracle/_ref, else the oracle) on `texels` random
+    texels with a mapping hit, fed the job's own mapping and scene arrays,
+    against the batch's outputs there."""
+    from fornos_b200 import api
+    from oracle import parity, pyoracle
+
+    def check(job, out, k):
+        impl = None
+        if cpu_kind == "reference":
+            try:
+                impl = pyoracle.Reference()
+            except OSError:
+                impl = None
+        kind = "reference" if impl is not None else "port"
+        impl = impl or pyoracle.Oracle()
+        n = job["texel_count"]
+        ctx = job["scene"].ctx
+        nodes, pos4, nrm4 = api.BVH.build_flat_device(ctx, job["mesh"], 8, 8192)
+        coords, tidx = job["coords"].download(np.float32, (n, 4)), job["tidx"].download(np.uint32, n)
+        hit = np.nonzero(tidx != parity.MISS)[0]
+        sel = np.sort(np.random.default_rng(k).choice(hit, min(texels, len(hit)), replace=False)).astype(np.uint32)
+        table = job["samples"].download(np.float32, (4096 * job["spp"], 4))
+        r = impl.hemisphere(0, nodes, pos4, nrm4, coords, tidx, table, job["spp"], job["min_distance"],
+                            job["max_distance"], texels=sel)
+        r = r[0] if isinstance(r, tuple) else r
+        got = out["out0"].download(np.float32, n)[sel]
+        rep = parity.sampled(r, got, np.ones(len(sel), bool), job["spp"],
+                             gpu_hits=out["hits0"].download(np.uint32, n)[sel])
+        rep.update(job=k, triangles=job["triangles"], compared_with=kind, meets_bar=parity.meets_bar({"ao": rep}))
+        return rep
+
+    return check
+
+
+def run_batch_bench(args):
+    """C4 alone: the batched-bake comparison as its own JSON line."""
+    import torch
+
+    from fornos_b200 import api
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    ctx = api.Context(0)
+    ctx.set_stream(stream.cuda_stream)
+    r = batch_compare(ctx, stream, args.seed, args.batch_jobs, None if args.no_cpu_baseline else batch_check())
+    return {
+        "metric": "Mrays/s (batched AO bake of %d jobs)" % r["jobs"], "value": r["batch_tuned_graph"]["mrays"],
+        "unit": "Mrays/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+        "data": "synthetic (seeded generated meshes)",
+        "config": {"workload": "batch%d" % r["jobs"], "rays": r["rays"], "texels": r["texels"]},
+        "batch": r,
+    }
+
+
+def side_workload(args, name, steps=2, warmup=1):
+    """Another workload's plain bake, measured as the headline's is (device
+    steps, e2e through fk_bake, the trace kernels' roofline) with fewer steps;
+    with the CPU baseline on, its parity against the reference's outputs on a
+    strided texel sample (about 4 s of CPU work)."""
+    import copy
+    wl = WORKLOADS[name]
+    a = copy.copy(args)
+    a.steps, a.warmup, a.workload = steps, warmup, name
+    r, state = run_fornos(a, wl, 0, 1)
+    out = {k: r[k] for k in ("value", "unit", "ms_per_step", "e2e", "clocks")}
+    out["config"] = {k: r["config"][k] for k in ("desc", "texels", "texture", "spp", "high_poly_triangles",
+                                                 "rays_per_texel", "traversals_per_texel")}
+    out["roofline"] = {k: r["roofline"][k] for k in ("achieved", "peak", "unit", "frac", "kernel_ms_per_step")}
+    if not args.no_cpu_baseline:
+        prep, tmap = state[0], state[1]
+        cmap = tmap.download()
+        cpu = CpuBaseline(wl, args.seed, prep, cmap)
+        cpu.calibrate(4.0)
+        mr, rays, dt, m = cpu.run()
+        out["cpu_baseline"] = {"value": round(mr, 4), "unit": "Mrays/s", "cores": cpu.cores, "kind": cpu.kind,
+                               "sample": cpu.describe(rays, m)}
+        out["parity"] = cpu.parity(state[2], state[3], cmap)
+    for b in state[2].values():
+        b.free()
+    state[6].free()
+    state[1].free()
+    return out
 
 
 def main():
@@ -802,6 +1007,11 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoised-vs-plain comparison")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-bake comparison of the default line")
+    ap.add_argument("--side", default="sphere512",
+                    help="other workloads measured in the default line (comma-separated; empty: none)")
+    ap.add_argument("--line-batch-jobs", type=int, default=16,
+                    help="jobs of the default line's batched-bake comparison (--workload batch: --batch-jobs)")
     ap.add_argument("--denoise-tex", type=int, default=4096,
                     help="texture size of the denoised-vs-plain comparison (4096 reported; smaller for profiling)")
     ap.add_argument("--denoiser", default=os.path.join(ROOT, "fornos_b200", "data", "denoiser_plane2048.npz"))
@@ -831,16 +1041,29 @@ def main():
     result, state = run_fornos(args, wl, rank, world)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         prep, tmap = state[0], state[1]
-        cpu = CpuBaseline(wl, args.seed, prep, tmap.download())
+        cmap = tmap.download()
+        cpu = CpuBaseline(wl, args.seed, prep, cmap)
         cpu.calibrate(args.cpu_seconds)
         mr, rays, dt, m = cpu.run()
         result["cpu_baseline"] = {"value": round(mr, 4), "unit": "Mrays/s", "cores": cpu.cores, "kind": cpu.kind,
                                   "sample": cpu.describe(rays, m)}
+        # the timed bake's own outputs (last timed step) at the CPU run's texels
+        result["parity"] = cpu.parity(state[2], state[3], cmap)
     if rank == 0 and world == 1:
         result["files_to_images"] = files_to_images(state[4], state[0], wl, args.seed)
     if rank == 0 and world == 1 and args.workload == "plane2048" and not args.no_denoise:
         prep, _, _, _, ctx, stream, scene = state
-        result["denoise"] = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed, args.denoise_tex)
+        check = plain_path_check(cpu, prep) if not args.no_cpu_baseline else None
+        result["denoise"] = denoise_compare(ctx, stream, prep, scene, args.denoiser, args.seed, args.denoise_tex,
+                                            check)
+    if rank == 0 and world == 1 and args.workload == "plane2048" and args.side:
+        result["side_workloads"] = {}
+        for name in args.side.split(","):
+            result["side_workloads"][name] = side_workload(args, name)
+    if rank == 0 and world == 1 and args.workload == "plane2048" and not args.no_batch:
+        ctx, stream = state[4], state[5]
+        result["batch"] = batch_compare(ctx, stream, args.seed, args.line_batch_jobs,
+                                        None if args.no_cpu_baseline else batch_check())
     if rank == 0:
         print(json.dumps(result))
     if world > 1:

@@ -39,7 +39,8 @@ class SolverParams(ctypes.Structure):
 
 
 class Tuning(ctypes.Structure):
-    _fields_ = [("refill", c_u32), ("leaf_batch", c_u32), ("speculate", c_u32), ("reserved", c_u32)]
+    _fields_ = [("refill", c_u32), ("leaf_batch", c_u32), ("speculate", c_u32), ("ray_order", c_u32),
+                ("top_records", c_u32), ("l2_persist", c_u32), ("block_threads", c_u32), ("stack_depth", c_u32)]
 
 
 class ExportParams(ctypes.Structure):
@@ -78,7 +79,7 @@ class BakeDesc(ctypes.Structure):
                 ("pix8", f32p), ("pixt12", f32p), ("indices", u32p), ("cull_backfaces", c_int),
                 ("height_enabled", c_int), ("position_enabled", c_int), ("normals_enabled", c_int),
                 ("normals_tangent_space", c_int), ("ao", BakeSampler), ("bent_normals", BakeSampler),
-                ("thickness", BakeSampler), ("traverse", c_int)]
+                ("thickness", BakeSampler), ("traverse", c_int), ("mapping_max_distance", c_float)]
 
 
 class BatchJob(ctypes.Structure):
@@ -150,7 +151,7 @@ _SIGS = {
     "fk_texel_map_download": (c_int, [c_vp, c_vp, f32p, f32p, u32p]),
     "fk_texel_map_free": (c_int, [c_vp, c_vp]),
     "fk_samples_cosine": (c_int, [c_u32, c_u32, c_u32, f32p]),
-    "fk_meshmap": (c_int, [c_vp, c_vp, c_vp, c_int, c_u32, c_u32, c_vp, c_vp]),
+    "fk_meshmap": (c_int, [c_vp, c_vp, c_vp, c_int, c_float, c_u32, c_u32, c_vp, c_vp]),
     "fk_hemisphere": (c_int, [c_vp, c_vp, c_vp, c_vp, c_int, ctypes.POINTER(SampleParams), c_vp, c_u32, c_u32,
                               c_int, c_vp, c_vp, c_vp, c_vp]),
     "fk_hemisphere_texels": (c_int, [c_vp, c_vp, c_vp, c_vp, c_u32, c_int, ctypes.POINTER(SampleParams), c_vp, c_vp,

@@ -18,6 +18,7 @@ from .workloads import MeshArrays
 
 OK = 0
 MISS = 0xFFFFFFFF
+FLT_MAX = float(np.finfo(np.float32).max)
 
 # kinds (include/fornos_gpu.h)
 AO, BN, THICK, AO_BN = 0, 1, 2, 3
@@ -55,6 +56,10 @@ def _check(rc, ctx=None, what=""):
         if ctx is not None and ctx.handle:
             msg = (what + ": " if what else "") + L.load().fk_last_error(ctx.handle).decode()
         raise FornosError(rc, msg)
+
+
+def _tuning_dict(t):
+    return {name: int(getattr(t, name)) for name, _ in L.Tuning._fields_}
 
 
 # ------------------------------------------------------------------ context
@@ -99,14 +104,16 @@ class Context:
     def launches(self):
         return int(self.lib.fk_launch_count(self.handle))
 
-    def set_tuning(self, refill=16, leaf_batch=8, speculate=1):
-        t = L.Tuning(refill, leaf_batch, speculate, 0)
+    def set_tuning(self, **knobs):
+        """fk_ctx_set_tuning: the given knobs (fk_tuning field names), the
+        others as they are now."""
+        t = L.Tuning(**dict(self.get_tuning(), **knobs))
         _check(self.lib.fk_ctx_set_tuning(self.handle, ctypes.byref(t)), self, "fk_ctx_set_tuning")
 
     def get_tuning(self):
         t = L.Tuning()
         _check(self.lib.fk_ctx_get_tuning(self.handle, ctypes.byref(t)), self)
-        return {"refill": t.refill, "leaf_batch": t.leaf_batch, "speculate": t.speculate}
+        return _tuning_dict(t)
 
     def buffer(self, nbytes):
         return Buffer(self, nbytes)
@@ -470,10 +477,13 @@ def samples_cosine(spp, perms=PERMS, seed=0):
 
 
 # ------------------------------------------------------------------ kernels
-def meshmap(ctx, scene, tmap, cull_backfaces, coords, tidx, offset=0, count=None):
+def meshmap(ctx, scene, tmap, cull_backfaces, coords, tidx, offset=0, count=None, max_dist=FLT_MAX):
+    """fk_meshmap: the mapping shaders over texels [offset, offset + count).
+    max_dist is the walks' initial closest distance (FLT_MAX reproduces the
+    reference); hits at or beyond it are not taken."""
     count = tmap.count - offset if count is None else count
-    _check(ctx.lib.fk_meshmap(ctx.handle, scene.handle, tmap.handle, int(cull_backfaces), offset, count, coords.handle,
-                              tidx.handle), ctx, "fk_meshmap")
+    _check(ctx.lib.fk_meshmap(ctx.handle, scene.handle, tmap.handle, int(cull_backfaces), max_dist, offset, count,
+                              coords.handle, tidx.handle), ctx, "fk_meshmap")
 
 
 def hemisphere(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, out0, out1=None, hits0=None, hits1=None,
@@ -703,17 +713,18 @@ def _sampler(cfg):
 
 def bake(ctx, nodes, pos4, nrm4, width, height, pix8, pixt12, indices, outputs, cull_backfaces=True,
          height_map=False, position_map=False, normals_map=False, normals_tangent_space=True, ao=None,
-         bent_normals=None, thickness=None, traverse=TRAVERSE_AUTO):
+         bent_normals=None, thickness=None, traverse=TRAVERSE_AUTO, mapping_max_distance=0.0):
     """fk_bake: one call from host arrays to host results.  `outputs` maps
     'coords4', 'tidx', 'height', 'position3', 'normals3', 'ao',
     'bent_normals3', 'thickness' to preallocated host arrays (pinned memory
     gives the fastest copies).  ao / bent_normals / thickness: dicts with
-    sample_count, min_distance, max_distance, seed (and tangent_space)."""
+    sample_count, min_distance, max_distance, seed (and tangent_space).
+    mapping_max_distance: fk_meshmap's max_dist (0: no limit)."""
     n = len(indices)
     d = L.BakeDesc(nodes.ctypes.data, len(nodes), _f32(pos4), _f32(nrm4), len(pos4), width, height, n, _f32(pix8),
                    _f32(pixt12), _u32(indices), int(cull_backfaces), int(height_map), int(position_map),
                    int(normals_map), int(normals_tangent_space), _sampler(ao), _sampler(bent_normals),
-                   _sampler(thickness), traverse)
+                   _sampler(thickness), traverse, mapping_max_distance)
     o = L.BakeOut()
     for name, ctype in (("coords4", L.f32p), ("tidx", L.u32p), ("height", L.f32p), ("position3", L.f32p),
                         ("normals3", L.f32p), ("ao", L.f32p), ("bent_normals3", L.f32p), ("thickness", L.f32p)):
@@ -793,7 +804,7 @@ class Batch:
         t, trav = L.Tuning(), L.c_int()
         _check(self.ctx.lib.fk_batch_tune(self.handle, sample_rays, ctypes.byref(t), ctypes.byref(trav)), self.ctx,
                "fk_batch_tune")
-        return {"refill": t.refill, "leaf_batch": t.leaf_batch, "traverse": trav.value}
+        return dict(_tuning_dict(t), traverse=trav.value)
 
     def run(self, traverse=0):
         _check(self.ctx.lib.fk_batch_run(self.handle, traverse), self.ctx, "fk_batch_run")
@@ -825,7 +836,7 @@ def tune_hemisphere(ctx, scene, coords, tidx, kind, spp, min_d, max_d, samples, 
     _check(ctx.lib.fk_tune_hemisphere(ctx.handle, scene.handle, coords.handle, tidx.handle, kind, ctypes.byref(p),
                                       samples.handle, offset, count, sample_rays, ctypes.byref(t),
                                       ctypes.byref(trav)), ctx, "fk_tune_hemisphere")
-    return {"refill": t.refill, "leaf_batch": t.leaf_batch, "speculate": t.speculate}, trav.value
+    return _tuning_dict(t), trav.value
 
 
 # ------------------------------------------------------------------ learned denoiser

@@ -20,14 +20,15 @@ bool fits(const fk_buf* b, uint64_t bytes) { return b && b->bytes >= bytes; }
 
 extern "C" {
 
-int fk_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, uint32_t offset, uint32_t count,
-               fk_buf* coords, fk_buf* tidx) {
+int fk_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, float max_dist, uint32_t offset,
+               uint32_t count, fk_buf* coords, fk_buf* tidx) {
   if (!ctx || !s || !m) return fk_fail(ctx, FK_ERR_INVALID, "fk_meshmap: null handle");
+  if (!(max_dist > 0.0f)) return fk_fail(ctx, FK_ERR_INVALID, "fk_meshmap: max_dist must be positive");
   if ((uint64_t)offset + count > m->count) return fk_fail(ctx, FK_ERR_INVALID, "fk_meshmap: texel range outside the map");
   uint64_t end = (uint64_t)offset + count;
   if (!fits(coords, 16 * end) || !fits(tidx, 4 * end))
     return fk_fail(ctx, FK_ERR_INVALID, "fk_meshmap: output buffers too small");
-  return fk::launch_meshmap(ctx, s, m, cull, offset, count, (float4*)coords->ptr, (uint32_t*)tidx->ptr);
+  return fk::launch_meshmap(ctx, s, m, cull, max_dist, offset, count, (float4*)coords->ptr, (uint32_t*)tidx->ptr);
 }
 
 int fk_hemisphere(fk_ctx* ctx, const fk_scene* s, const fk_buf* coords, const fk_buf* tidx, int kind,
@@ -290,7 +291,7 @@ int fk_meshmapping_run_step(fk_meshmapping* mm, int* done) {
   if (!mm->ready) return fk_fail(mm->ctx, FK_ERR_STATE, "fk_meshmapping_run_step: not initialised");
   uint32_t left = mm->count - mm->done;
   uint32_t n = (mm->per_step && mm->per_step < left) ? mm->per_step : left;
-  int rc = fk_meshmap(mm->ctx, mm->scene, mm->map, mm->cull, mm->done, n, mm->coords, mm->tidx);
+  int rc = fk_meshmap(mm->ctx, mm->scene, mm->map, mm->cull, FLT_MAX, mm->done, n, mm->coords, mm->tidx);
   if (rc != FK_OK) return rc;
   mm->done += n;
   if (done) *done = mm->done >= mm->count;

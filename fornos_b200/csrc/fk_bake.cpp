@@ -2,6 +2,7 @@
 // Scene and texel rows go up, mesh mapping and the enabled solvers run on the
 // context's stream, results come back.  Built only from the public entry
 // points of include/fornos_gpu.h.
+#include <cfloat>
 #include <cstring>
 #include <vector>
 
@@ -51,7 +52,8 @@ extern "C" int fk_bake(fk_ctx* ctx, const fk_bake_desc* d, fk_bake_out* out) {
   const size_t nn = n ? n : 1;
   fk_buf *coords, *tidx;
   if ((rc = s.alloc(16 * nn, &coords)) != FK_OK || (rc = s.alloc(4 * nn, &tidx)) != FK_OK) return rc;
-  if ((rc = fk_meshmap(ctx, s.scene, s.map, d->cull_backfaces, 0, n, coords, tidx)) != FK_OK) return rc;
+  if ((rc = fk_meshmap(ctx, s.scene, s.map, d->cull_backfaces,
+                       d->mapping_max_distance > 0.0f ? d->mapping_max_distance : FLT_MAX, 0, n, coords, tidx)) != FK_OK) return rc;
 
   auto gather = [&](int enabled, int kind, float* host, size_t width, int tangent) -> int {
     if (!enabled) return FK_OK;

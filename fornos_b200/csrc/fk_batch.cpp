@@ -41,7 +41,7 @@ struct fk_batch {
   bool ordered_ok = true;                 // every tree fits the 2-wide ordered traversal's stack
   bool ordered4_ok = true;                // every collapsed tree fits the 4-wide traversal's stack
   bool filter = true;
-  fk_tuning tuning = {8, 8, 0, 0};
+  fk_tuning tuning = {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -66,6 +66,7 @@ static int batch_run_chunks(fk_batch* b, int trav, bool filter, const fk_tuning&
     a.status = ctx->status;
     a.refill = tun.refill;
     a.leaf_batch = tun.leaf_batch;
+    a.ray_order = tun.ray_order;
     cudaError_t e = fk::launch_batch(a, b->kind, trav, filter, ctx->stream, ctx->sm_count, true);
     if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "batch launch");
     ctx->launches += 2;
@@ -97,6 +98,7 @@ static int batch_time(fk_batch* b, unsigned long long stride, int trav, bool fil
   a.status = ctx->status;
   a.refill = tun.refill;
   a.leaf_batch = tun.leaf_batch;
+  a.ray_order = FK_RAY_ORDER_SAMPLE;  // calibration samples every stride-th ray
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -242,13 +244,13 @@ int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int
   const bool ordered_ok = b->ordered_ok;
   for (uint32_t refill : {4u, 8u, 16u}) {
     if (ordered_ok)
-      for (uint32_t lb : {1u, 4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED, true, {refill, lb, 0, 0}});
+      for (uint32_t lb : {1u, 4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED, true, {refill, lb, 0, 0, 0, FK_L2_NONE, 256, 64}});
     if (b->ordered4_ok)
-      for (uint32_t lb : {4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED4, true, {refill, lb, 0, 0}});
-    cands.push_back({FK_TRAVERSE_SKIP, true, {refill, 8, 0, 0}});
+      for (uint32_t lb : {4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED4, true, {refill, lb, 0, 0, 0, FK_L2_NONE, 256, 64}});
+    cands.push_back({FK_TRAVERSE_SKIP, true, {refill, 8, 0, 0, 0, FK_L2_NONE, 256, 64}});
   }
-  if (ordered_ok) cands.push_back({FK_TRAVERSE_ORDERED, false, {8, 8, 0, 0}});
-  cands.push_back({FK_TRAVERSE_SKIP, false, {8, 8, 0, 0}});
+  if (ordered_ok) cands.push_back({FK_TRAVERSE_ORDERED, false, {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64}});
+  cands.push_back({FK_TRAVERSE_SKIP, false, {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64}});
   float best_ms = 1e30f;
   Cand best = cands[0];
   float warm = 0.0f;
@@ -263,6 +265,7 @@ int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int
     }
   }
   if (rc != FK_OK) return rc;
+  best.t.ray_order = ctx->tuning.ray_order;  // strided calibration cannot see the ray order: the context's
   b->traverse = best.trav;
   b->filter = best.filter;
   b->tuning = best.t;
@@ -327,45 +330,148 @@ int fk_batch_free(fk_batch* b) {
   return FK_OK;
 }
 
-// Tuner for a single fk_hemisphere call: a one-job batch over the same
-// arguments, calibrated on a strided sample of its rays.
+// Tuner for a single fk_hemisphere call.  It times the call's own trace
+// kernel on a sample that keeps the coherence of a whole-map pass: eight
+// windows of consecutive texels spread over [offset, offset + count), about
+// sample_rays rays in all, traced through the texel-list path (which traces
+// each listed texel exactly as the whole-map pass does).  The knobs are
+// searched one group at a time from the context's current tuning, each group
+// keeping its fastest value: traversal layout, refill x leaf batch,
+// speculation, ray order, block shape x stack depth, staged top records, L2
+// window.  The context's tuning is left as it was.
 int fk_tune_hemisphere(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
                        const fk_sample_params* params, const fk_buf* samples, uint32_t offset, uint32_t count,
                        uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse) {
   if (!ctx || !scene || !coords || !tidx || !params || !samples || !best_tuning || !best_traverse)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: null argument");
-  uint64_t end = (uint64_t)offset + count;
+  const uint64_t end = (uint64_t)offset + count;
   if (!fits(coords, 16 * end) || !fits(tidx, 4 * end))
     return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: mapping buffers too small");
-  if (count == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: no texels");
-  // views of the caller's buffers at `offset` (no copies), outputs to scratch
-  fk_buf c_view = *coords, t_view = *tidx;
-  c_view.ptr = (char*)coords->ptr + 16 * (size_t)offset;
-  c_view.bytes = 16 * (size_t)count;
-  t_view.ptr = (char*)tidx->ptr + 4 * (size_t)offset;
-  t_view.bytes = 4 * (size_t)count;
-  fk_buf *o0 = nullptr, *o1 = nullptr;
-  int rc = fk_buf_alloc(ctx, 12 * (size_t)count, &o0);
-  if (rc == FK_OK) rc = fk_buf_alloc(ctx, 12 * (size_t)count, &o1);
-  fk_batch* b = nullptr;
-  if (rc == FK_OK) {
-    fk_batch_job j;
-    std::memset(&j, 0, sizeof(j));
-    j.scene = scene;
-    j.coords = &c_view;
-    j.tidx = &t_view;
-    j.texel_count = count;
-    j.params = *params;
-    j.samples = samples;
-    j.out0 = o0;
-    j.out1 = o1;
-    rc = fk_batch_create(ctx, &j, 1, kind, &b);
+  if (count == 0 || params->sample_count == 0) return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: no work");
+  if (kind < FK_AO || kind > FK_AO_BN) return fk_fail(ctx, FK_ERR_INVALID, "fk_tune_hemisphere: unknown kind");
+  if (sample_rays == 0) sample_rays = 1ull << 24;
+  // the sample: eight windows of consecutive texels (or every texel)
+  const uint64_t want = std::max<uint64_t>(256, sample_rays / params->sample_count);
+  std::vector<uint32_t> ids;
+  if (want >= count) {
+    for (uint32_t t = 0; t < count; ++t) ids.push_back(offset + t);
+  } else {
+    const uint32_t per = (uint32_t)(want / 8), span = count - per;
+    for (uint32_t w = 0; w < 8; ++w) {
+      const uint32_t start = offset + (uint32_t)((uint64_t)span * w / 7);
+      for (uint32_t t = 0; t < per; ++t) ids.push_back(start + t);
+    }
   }
-  if (rc == FK_OK) rc = fk_batch_tune(b, sample_rays, best_tuning, best_traverse);
-  if (b) fk_batch_free(b);
+  fk_buf *idb = nullptr, *o0 = nullptr, *o1 = nullptr;
+  int rc = fk_buf_alloc(ctx, 4 * ids.size(), &idb);
+  if (rc == FK_OK) rc = fk_buf_upload(ctx, idb, 0, ids.data(), 4 * ids.size());
+  if (rc == FK_OK) rc = fk_buf_alloc(ctx, 12 * (size_t)end, &o0);
+  if (rc == FK_OK) rc = fk_buf_alloc(ctx, 12 * (size_t)end, &o1);
+  const fk_tuning saved = ctx->tuning;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (rc == FK_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+    rc = fk_fail(ctx, FK_ERR_CUDA, "fk_tune_hemisphere: events");
+  // one candidate: best of two timed launches
+  auto time_one = [&](const fk_tuning& t, int trav, float* ms) -> int {
+    ctx->tuning = t;
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaEventRecord(e0, ctx->stream);
+      int r = fk_hemisphere_texels(ctx, scene, coords, tidx, (uint32_t)end, kind, params, samples, idb, 0,
+                                   (uint32_t)ids.size(), trav | FK_SCHEDULE_DYNAMIC, o0, kind == FK_AO_BN ? o1 : nullptr,
+                                   nullptr, nullptr);
+      if (r != FK_OK) return r;
+      cudaEventRecord(e1, ctx->stream);
+      cudaError_t e = cudaEventSynchronize(e1);
+      if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "fk_tune_hemisphere: timing");
+      float x = 0.0f;
+      cudaEventElapsedTime(&x, e0, e1);
+      best = std::min(best, x);
+    }
+    *ms = best;
+    return FK_OK;
+  };
+  fk_tuning cur = saved;
+  int trav = scene->odepth <= fk::kMaxOrderedDepth ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
+  float cur_ms = 0.0f;
+  if (rc == FK_OK) rc = time_one(cur, trav, &cur_ms);  // warms code and caches
+  if (rc == FK_OK) rc = time_one(cur, trav, &cur_ms);
+  // tries `t` with traversal `tv`; keeps it when faster
+  auto consider = [&](const fk_tuning& t, int tv) {
+    float ms = 0.0f;
+    if (rc == FK_OK) rc = time_one(t, tv, &ms);
+    if (rc == FK_OK && ms < cur_ms) {
+      cur_ms = ms;
+      cur = t;
+      trav = tv;
+    }
+  };
+  if (rc == FK_OK) {
+    const fk_tuning base = cur;
+    const int base_trav = trav;
+    if (base_trav != FK_TRAVERSE_SKIP) consider(base, FK_TRAVERSE_SKIP);
+    // the 4-wide layout: built on first use; skipped when its tree is too deep
+    if (base_trav == FK_TRAVERSE_ORDERED && fk::ensure_wide4(ctx, const_cast<fk_scene*>(scene)) == FK_OK &&
+        scene->depth4 <= fk::kMaxOrdered4Depth)
+      consider(base, FK_TRAVERSE_ORDERED4);
+  }
+  if (rc == FK_OK && trav != FK_TRAVERSE_SKIP) {
+    const fk_tuning base = cur;
+    for (uint32_t refill : {8u, 16u, 24u, 32u})
+      for (uint32_t lb : {4u, 8u, 16u}) {
+        fk_tuning t = base;
+        t.refill = refill;
+        t.leaf_batch = lb;
+        if (t.refill != base.refill || t.leaf_batch != base.leaf_batch) consider(t, trav);
+      }
+    fk_tuning t = cur;
+    t.speculate = 1 - t.speculate;
+    consider(t, trav);
+  }
+  if (rc == FK_OK) {
+    fk_tuning t = cur;
+    t.ray_order = cur.ray_order == FK_RAY_ORDER_SECTOR ? FK_RAY_ORDER_SAMPLE : FK_RAY_ORDER_SECTOR;
+    consider(t, trav);
+  }
+  if (rc == FK_OK && trav == FK_TRAVERSE_ORDERED) {
+    const fk_tuning base = cur;
+    for (uint32_t block : {128u, 256u, 512u})
+      for (uint32_t stack : {32u, 64u}) {
+        if (stack == 32 && scene->odepth > 24) continue;
+        fk_tuning t = base;
+        t.block_threads = block;
+        t.stack_depth = stack;
+        if (block != base.block_threads || stack != base.stack_depth) consider(t, trav);
+      }
+    const fk_tuning base2 = cur;
+    for (uint32_t top : {0u, 64u, 256u}) {
+      fk_tuning t = base2;
+      t.top_records = top;
+      if (top != base2.top_records) consider(t, trav);
+    }
+  }
+  if (rc == FK_OK) {
+    const fk_tuning base = cur;
+    for (uint32_t l2 : {(uint32_t)FK_L2_NONE, (uint32_t)FK_L2_TREE, (uint32_t)FK_L2_TRIANGLES}) {
+      fk_tuning t = base;
+      t.l2_persist = l2;
+      if (l2 != base.l2_persist) consider(t, trav);
+    }
+  }
+  ctx->tuning = saved;
+  if (saved.l2_persist == FK_L2_NONE && ctx->l2_raised) {
+    cudaStreamSynchronize(ctx->stream);
+    fk::restore_l2(ctx);
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (idb) fk_buf_free(ctx, idb);
   if (o0) fk_buf_free(ctx, o0);
   if (o1) fk_buf_free(ctx, o1);
-  return rc;
+  if (rc != FK_OK) return rc;
+  *best_tuning = cur;
+  *best_traverse = trav | FK_SCHEDULE_DYNAMIC;
+  return FK_OK;
 }
 
 }  // extern "C"

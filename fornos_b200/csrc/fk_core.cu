@@ -66,6 +66,27 @@ void* fk_scratch(fk_ctx* ctx, size_t bytes) {
 namespace fk {
 // Builds the collapsed 4-wide layout of the scene's active inner tree on first
 // use (from the 2-wide records on the device) and points the scene at it.
+int raise_l2(fk_ctx* ctx, size_t bytes, float* hit_ratio) {
+  int max_persist = 0;
+  FK_CUDA(ctx, cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, ctx->device));
+  if (max_persist <= 0) return fk_fail(ctx, FK_ERR_UNSUPPORTED, "no persisting L2 on this device");
+  const size_t want = std::min(bytes, (size_t)max_persist);
+  if (!ctx->l2_raised) {
+    FK_CUDA(ctx, cudaDeviceGetLimit(&ctx->l2_prev_limit, cudaLimitPersistingL2CacheSize));
+    FK_CUDA(ctx, cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, (size_t)max_persist));
+    ctx->l2_raised = true;
+  }
+  *hit_ratio = bytes ? std::min(1.0f, (float)((double)want / (double)bytes)) : 0.0f;
+  return FK_OK;
+}
+
+void restore_l2(fk_ctx* ctx) {
+  if (!ctx->l2_raised) return;
+  cudaCtxResetPersistingL2Cache();
+  cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, ctx->l2_prev_limit);
+  ctx->l2_raised = false;
+}
+
 int ensure_wide4(fk_ctx* ctx, fk_scene* s) {
   const int t = s->tree;
   if (!s->tree_wide4[t] && s->tree_wide[t] && s->tree_count[t] > 0) {
@@ -149,6 +170,7 @@ int fk_ctx_destroy(fk_ctx* ctx) {
   for (fk_scene* s : std::set<fk_scene*>(ctx->scenes)) fk_scene_free(ctx, s);
   for (fk_texel_map* m : std::set<fk_texel_map*>(ctx->maps)) fk_texel_map_free(ctx, m);
   cudaStreamSynchronize(ctx->stream);
+  fk::restore_l2(ctx);
   cudaFree(ctx->counters);
   cudaFree(ctx->status);
   cudaFree(ctx->scratch);
@@ -188,8 +210,17 @@ uint64_t fk_launch_count(const fk_ctx* ctx) { return ctx ? ctx->launches : 0; }
 
 int fk_ctx_set_tuning(fk_ctx* ctx, const fk_tuning* t) {
   if (!ctx || !t) return FK_ERR_INVALID;
-  if (t->refill < 1 || t->refill > 32 || t->leaf_batch < 1 || t->leaf_batch > 32 || t->speculate > 1)
-    return fk_fail(ctx, FK_ERR_INVALID, "fk_ctx_set_tuning: refill and leaf_batch in 1..32, speculate 0 or 1");
+  if (t->refill < 1 || t->refill > 32 || t->leaf_batch < 1 || t->leaf_batch > 32 || t->speculate > 1 ||
+      t->ray_order > FK_RAY_ORDER_SECTOR || t->top_records > FK_MAX_TOP_RECORDS || t->l2_persist > FK_L2_TRIANGLES ||
+      (t->block_threads != 128 && t->block_threads != 256 && t->block_threads != 512) ||
+      (t->stack_depth != 32 && t->stack_depth != 64))
+    return fk_fail(ctx, FK_ERR_INVALID,
+                   "fk_ctx_set_tuning: refill and leaf_batch in 1..32, speculate 0 or 1, ray_order 0 or 1, "
+                   "top_records at most 1024, l2_persist 0..2, block_threads 128 / 256 / 512, stack_depth 32 / 64");
+  if (t->l2_persist == FK_L2_NONE && ctx->l2_raised) {
+    FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));  // windows already queued finish first
+    fk::restore_l2(ctx);
+  }
   ctx->tuning = *t;
   return FK_OK;
 }
@@ -525,8 +556,8 @@ int fk_scene_build(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint32_t
 int fk_scene_free(fk_ctx* ctx, fk_scene* s) {
   if (!ctx || !s || !ctx->scenes.count(s)) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_free: unknown scene");
   cudaStreamSynchronize(ctx->stream);
-  void* ps[] = {s->node_lo,      s->node_hi,      s->node_jump,     s->pos4,          s->nrm4,
-                s->tree_wide[0], s->tree_wide[1], s->tree_wide4[0], s->tree_wide4[1], s->tri_rec};
+  void* ps[] = {s->node_lo,         s->node_hi,         s->node_jump, s->pos4,    s->nrm4,  s->tree_wide[0],
+                s->tree_wide[1],   s->tree_wide4[0],   s->tree_wide4[1], s->tri_rec, s->top};
   for (void* p : ps) fk_dev_free(ctx, p);
   ctx->scenes.erase(s);
   delete s;

@@ -30,7 +30,12 @@ struct fk_ctx {
   // bakes reuse it instead of mapping and unmapping pages (fk_ctx_trim).
   cudaMemPool_t pool = nullptr;
   size_t scratch_bytes = 0;
-  fk_tuning tuning = {16, 8, 1, 0};  // dynamic-schedule knobs (fk_ctx_set_tuning)
+  fk_tuning tuning = {16, 8, 1, FK_RAY_ORDER_SECTOR, 0, FK_L2_NONE, 256, 64};  // fk_ctx_set_tuning
+  // Persisting L2 set-aside (fk_tuning.l2_persist): the device's limit before
+  // the context raised it, restored when the knob is turned off or the
+  // context is destroyed.
+  bool l2_raised = false;
+  size_t l2_prev_limit = 0;
   std::set<fk_buf*> bufs;
   std::set<fk_scene*> scenes;
   std::set<fk_texel_map*> maps;
@@ -67,6 +72,13 @@ struct fk_scene {
   float4* wide4 = nullptr;
   uint32_t wide4_count = 0, depth4 = 0;
   float4* tri_rec = nullptr;
+  // The first inner records of the active 2-wide tree in breadth-first order
+  // (fk_tuning.top_records), staged in shared memory by the ordered
+  // traversal; a child ref >= wide_count names staged record ref - wide_count.
+  // Built on first use for (top_tree, top_want).
+  float4* top = nullptr;
+  uint32_t top_count = 0, top_want = 0;
+  int top_tree = -1;
   uint32_t root_is_leaf = 0;
   uint32_t filter_ok = 0;        // every coordinate below 2^24 in magnitude
   size_t bytes = 0;
@@ -165,6 +177,13 @@ int build_sah_device(fk_ctx* ctx, const float4* node_lo, const float4* node_hi, 
                      float4** wide, uint32_t* depth);
 // The scene's 4-wide layout for its active tree, built on first use.
 int ensure_wide4(fk_ctx* ctx, fk_scene* s);
+// The scene's staged top records for `want` records of its active tree
+// (fk_scene::top), built on first use.
+int ensure_top(fk_ctx* ctx, fk_scene* s, uint32_t want);
+// Raises the device's persisting L2 set-aside for a window of `bytes` (once
+// per context) and gives the window's hit ratio; restore_l2 undoes it.
+int raise_l2(fk_ctx* ctx, size_t bytes, float* hit_ratio);
+void restore_l2(fk_ctx* ctx);
 
 // One job of a batched hemisphere launch (device-side job table entry).
 static constexpr uint32_t kMaxBatchJobs = 64;
@@ -193,11 +212,12 @@ struct BatchArgs {
   unsigned long long* queue;  // zeroed before the launch
   int* status;
   uint32_t refill, leaf_batch;
+  uint32_t ray_order;  // FK_RAY_ORDER_*, per job (stride 1 only)
 };
 cudaError_t launch_batch(const BatchArgs& a, int kind, int trav, bool filter, cudaStream_t stream, int sm_count,
                          bool reduce);
-int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, uint32_t offset, uint32_t count,
-                   float4* coords, uint32_t* tidx);
+int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, float max_d, uint32_t offset,
+                   uint32_t count, float4* coords, uint32_t* tidx);
 struct HemiLaunch {
   int kind;
   uint32_t spp, perms;

@@ -72,6 +72,28 @@ int launch_tri_records(fk_ctx* ctx, fk_scene* s) {
   return fk_after_launch(ctx, "tri_records_kernel");
 }
 
+#ifdef FK_BARY_FILTER
+// True only when the sampling test's barycentric check (y = ny / den,
+// z = nz / den, x = 1 - y - z; x, y, z >= 0 and y, z <= 1) certainly fails.
+// The quotients are estimated with the hardware reciprocal (rcp.approx: at
+// most 1 ulp, 2^-23 relative) and one rounded multiplication, so each
+// estimate is within 2^-21.4 relative of the divided value; a rejection is
+// taken only with a margin of 2^-19 on y and z (2^-18 on x, which adds two
+// roundings and both estimates' errors; y and z then lie in [-2^-19, 1 +
+// 2^-19]).  den must be a normal positive float below 2^100 (no flush, no
+// overflow); otherwise, and for NaN estimates, the exact division decides.
+__device__ __forceinline__ bool bary_certainly_outside(float ny, float nz, float den) {
+  if (!(den >= 1.17549435e-38f && den < 1.2676506e30f)) return false;
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(den));
+  const float y = __fmul_rn(ny, r), z = __fmul_rn(nz, r);
+  const float m = 1.9073486e-06f;  // 2^-19
+  if (y < -m || z < -m || y > __fadd_rn(1.0f, m) || z > __fadd_rn(1.0f, m)) return true;
+  const float x = __fsub_rn(__fsub_rn(1.0f, y), z);
+  return x < -3.8146973e-06f;  // 2^-18
+}
+#endif
+
 // ------------------------------------------------------------------ sampling test
 // Shaders/ao_step1.comp:71-92 followed by the range test of :100-105: returns
 // true and lowers `best` when the triangle is hit at t in [lo, best).  The
@@ -94,8 +116,13 @@ __device__ __forceinline__ void tri_sample(const float4* __restrict__ rec, uint3
   float d20 = dot(v2, xyz(C)), d21 = dot(v2, xyz(D));
   float d00 = C.w, d01 = B.w, d11 = D.w;
   float den = __fsub_rn(__fmul_rn(d00, d11), __fmul_rn(d01, d01));
-  float y = __fdiv_rn(__fsub_rn(__fmul_rn(d11, d20), __fmul_rn(d01, d21)), den);
-  float z = __fdiv_rn(__fsub_rn(__fmul_rn(d00, d21), __fmul_rn(d01, d20)), den);
+  const float ny = __fsub_rn(__fmul_rn(d11, d20), __fmul_rn(d01, d21));
+  const float nz = __fsub_rn(__fmul_rn(d00, d21), __fmul_rn(d01, d20));
+#ifdef FK_BARY_FILTER
+  if (bary_certainly_outside(ny, nz, den)) return;
+#endif
+  float y = __fdiv_rn(ny, den);
+  float z = __fdiv_rn(nz, den);
   float x = __fsub_rn(__fsub_rn(1.0f, y), z);
   if (x >= 0.0f && y >= 0.0f && y <= 1.0f && z >= 0.0f && z <= 1.0f) best = th;
 }
@@ -366,9 +393,26 @@ static int run_hemi(fk_ctx* ctx, const HemiArgs& a) {
   return fk_after_launch(ctx, "hemi_kernel");
 }
 
+// What a dynamic trace launch adds beyond its arguments: staged top records
+// and a persisting L2 window (fk_tuning.top_records / l2_persist).
+struct TraceExtras {
+  uint32_t odepth = 0;  // levels of the tree walked
+  const float4* top = nullptr;
+  uint32_t top_count = 0, top_base = 0xFFFFFFFFu;
+  const void* window = nullptr;
+  size_t window_bytes = 0;
+  float hit_ratio = 0.0f;
+};
+
 template <int KIND, int TRAV>
 static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter, uint32_t leaf_batch,
-                            uint32_t speculate);
+                            uint32_t speculate, const TraceExtras& x);
+
+// Sector groups of the ray order (fk_tuning.ray_order): spp / 32 when the
+// sector order applies, else 1 (sample order).
+static uint32_t ray_sectors(uint32_t ray_order, uint32_t spp) {
+  return ray_order == FK_RAY_ORDER_SECTOR && spp >= 64 && spp % 32 == 0 ? spp / 32 : 1;
+}
 
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   if ((h.traverse & FK_TRAVERSE_MASK) == FK_TRAVERSE_ORDERED4) {
@@ -412,15 +456,45 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
   const uint32_t leaf_batch = h.leaf_batch ? h.leaf_batch : ctx->tuning.leaf_batch;
   const uint32_t speculate = h.speculate ? h.speculate : ctx->tuning.speculate;
-#define FK_HEMI_CASE(K)                                                                                     \
-  case K:                                                                                                   \
-    if (sched == FK_SCHEDULE_DYNAMIC) {                                                                     \
-      if (trav == FK_TRAVERSE_ORDERED4)                                                                     \
-        return run_hemi_dynamic<K, FK_TRAVERSE_ORDERED4>(ctx, a, refill, filter, leaf_batch, speculate);  \
-      return trav == FK_TRAVERSE_ORDERED                                                                   \
-                 ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill, filter, leaf_batch, speculate)  \
-                 : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill, filter, leaf_batch, speculate);    \
-    }                                                                                                       \
+  TraceExtras x;
+  x.odepth = s->odepth;
+  if (sched == FK_SCHEDULE_DYNAMIC && trav == FK_TRAVERSE_ORDERED && ctx->tuning.top_records && !h.tally) {
+    fk_scene* ms = const_cast<fk_scene*>(s);
+    const int rc = ensure_top(ctx, ms, ctx->tuning.top_records);
+    if (rc != FK_OK) return rc;
+    if (ms->top) {
+      x.top = ms->top;
+      x.top_count = ms->top_count;
+      x.top_base = ms->wide_count;
+    }
+  }
+  if (sched == FK_SCHEDULE_DYNAMIC && ctx->tuning.l2_persist != FK_L2_NONE) {
+    if (ctx->tuning.l2_persist == FK_L2_TREE) {
+      x.window = trav == FK_TRAVERSE_ORDERED4 ? (const void*)s->wide4 : (const void*)s->wide;
+      x.window_bytes = trav == FK_TRAVERSE_ORDERED4 ? 128 * (size_t)s->wide4_count : 64 * (size_t)s->wide_count;
+      if (trav == FK_TRAVERSE_SKIP) x.window = s->node_lo, x.window_bytes = 16 * (size_t)s->node_count;
+    } else {
+      x.window = s->tri_rec;
+      x.window_bytes = 64 * (size_t)(s->corner_count / 3);
+    }
+    int max_window = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, ctx->device);
+    if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "cudaDevAttrMaxAccessPolicyWindowSize");
+    x.window_bytes = std::min(x.window_bytes, (size_t)max_window);
+    if (x.window && x.window_bytes) {
+      const int rc = raise_l2(ctx, x.window_bytes, &x.hit_ratio);
+      if (rc != FK_OK) return rc;
+    }
+  }
+#define FK_HEMI_CASE(K)                                                                                       \
+  case K:                                                                                                     \
+    if (sched == FK_SCHEDULE_DYNAMIC) {                                                                       \
+      if (trav == FK_TRAVERSE_ORDERED4)                                                                       \
+        return run_hemi_dynamic<K, FK_TRAVERSE_ORDERED4>(ctx, a, refill, filter, leaf_batch, speculate, x);  \
+      return trav == FK_TRAVERSE_ORDERED                                                                     \
+                 ? run_hemi_dynamic<K, FK_TRAVERSE_ORDERED>(ctx, a, refill, filter, leaf_batch, speculate, x)  \
+                 : run_hemi_dynamic<K, FK_TRAVERSE_SKIP>(ctx, a, refill, filter, leaf_batch, speculate, x);    \
+    }                                                                                                         \
     return trav == FK_TRAVERSE_ORDERED ? run_hemi<K, FK_TRAVERSE_ORDERED>(ctx, a)                           \
                                        : run_hemi<K, FK_TRAVERSE_SKIP>(ctx, a);
   switch (h.kind) {
@@ -452,13 +526,19 @@ struct DynArgs {
   uint32_t refill;
   uint32_t leaf_batch;  // postponed leaves that start a leaf phase early
   uint32_t speculate;   // lanes holding a leaf keep visiting inner records
+  uint32_t sectors;     // ray order: queue slot q of a texel traces sample
+                        // (q % 32) * sectors + q / 32 (1: sample order)
   float lo, hi;
-  float* __restrict__ scratch;  // one distance per ray
+  float* __restrict__ scratch;  // one distance per ray, in sample order
   uint32_t* queue;
   int* status;
   unsigned long long* tally;
   const uint32_t* __restrict__ ids;  // texel list, or null: ray texel g is ids[g]
   uint32_t texel_limit;
+  // Top records staged in shared memory (2-wide ordered traversal): a record
+  // ref >= top_base is staged record ref - top_base (top_base = ~0: none).
+  const float4* __restrict__ top;
+  uint32_t top_count, top_base;
 };
 
 // Texel of list position g: itself, or ids[g] for a texel list.  An id at or
@@ -519,8 +599,9 @@ struct OState {
 
 // Deferred entries are (ref, entry distance bits) pairs: one 8-byte access
 // per push or pop.
+template <int STACK = kStack>
 __device__ __forceinline__ bool push(int2* stk, int& sp, int32_t ref, float dist, int* status) {
-  if (sp >= kStack) {
+  if (sp >= STACK) {
     atomicOr(status, 1);
     return false;
   }
@@ -531,6 +612,7 @@ __device__ __forceinline__ bool push(int2* stk, int& sp, int32_t ref, float dist
 
 // A child that passed its box test: the first leaf becomes the postponed
 // leaf, the first inner record the next one to visit, the rest are deferred.
+template <int STACK = kStack>
 __device__ __forceinline__ bool place(OState& st, int32_t& next, int2* stk, int32_t ref, float dist, int* status) {
   if (ref < 0) {
     if (st.pend < 0) {
@@ -538,22 +620,29 @@ __device__ __forceinline__ bool place(OState& st, int32_t& next, int2* stk, int3
       st.pend_dist = dist;
       return true;
     }
-    return push(stk, st.sp, ref, dist, status);
+    return push<STACK>(stk, st.sp, ref, dist, status);
   }
   if (next < 0) {
     next = ref;
     return true;
   }
-  return push(stk, st.sp, ref, dist, status);
+  return push<STACK>(stk, st.sp, ref, dist, status);
 }
 
 // Inner phase: tests both children of record `cur` against `thr` and takes
 // them nearer entry first (straight-line selects: no per-lane arrays).
-template <bool COUNT, bool FILTER>
+template <bool COUNT, bool FILTER, int STACK = kStack>
 __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
-                                            int* status, Tally& tally) {
-  const float4* w = s.wide + 4 * (size_t)st.cur;
-  float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
+                                            int* status, Tally& tally, const float4* top = nullptr,
+                                            uint32_t top_base = 0xFFFFFFFFu) {
+  float4 w0, w1, w2, w3;
+  if ((uint32_t)st.cur >= top_base) {  // staged in shared memory
+    const float4* w = top + 4 * ((uint32_t)st.cur - top_base);
+    w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+  } else {
+    const float4* w = s.wide + 4 * (size_t)st.cur;
+    w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
+  }
   float d0, d1;
   const bool h0 = child_maybe<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
   const bool h1 = child_maybe<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
@@ -563,8 +652,8 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   const float dn = swap ? d1 : d0, df = swap ? d0 : d1;
   const int32_t rn = __float_as_int(swap ? w3.y : w3.x), rf = __float_as_int(swap ? w3.x : w3.y);
   int32_t next = -1;
-  if (hn && !place(st, next, stk, rn, dn, status)) return false;
-  if (hf && !place(st, next, stk, rf, df, status)) return false;
+  if (hn && !place<STACK>(st, next, stk, rn, dn, status)) return false;
+  if (hf && !place<STACK>(st, next, stk, rf, df, status)) return false;
   st.cur = next;
   return true;
 }
@@ -585,7 +674,7 @@ __device__ __forceinline__ void cex(float& ka, int32_t& ra, float& kb, int32_t& 
 // (a 5-comparator sorting network), keeps the nearest inner child as the next
 // node and the nearest leaf as the postponed leaf when none is held, and
 // defers the rest farthest first, so that the nearest is popped next.
-template <bool COUNT, bool FILTER>
+template <bool COUNT, bool FILTER, int STACK = kStack>
 __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
                                              int* status, Tally& tally) {
   const float4* w = s.wide4 + 8 * (size_t)st.cur;
@@ -616,10 +705,10 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   const int ni = n0 ? 0 : (n1 ? 1 : (n2 ? 2 : (n3 ? 3 : 4)));
   const int nl = (l0 ? 0 : (l1 ? 1 : (l2 ? 2 : (l3 ? 3 : 4))));
   const int keep = st.pend < 0 ? nl : 4;  // the leaf that becomes the postponed leaf, if any
-  if (v3 && ni != 3 && keep != 3 && !push(stk, st.sp, r3, k3, status)) return false;
-  if (v2 && ni != 2 && keep != 2 && !push(stk, st.sp, r2, k2, status)) return false;
-  if (v1 && ni != 1 && keep != 1 && !push(stk, st.sp, r1, k1, status)) return false;
-  if (v0 && ni != 0 && keep != 0 && !push(stk, st.sp, r0, k0, status)) return false;
+  if (v3 && ni != 3 && keep != 3 && !push<STACK>(stk, st.sp, r3, k3, status)) return false;
+  if (v2 && ni != 2 && keep != 2 && !push<STACK>(stk, st.sp, r2, k2, status)) return false;
+  if (v1 && ni != 1 && keep != 1 && !push<STACK>(stk, st.sp, r1, k1, status)) return false;
+  if (v0 && ni != 0 && keep != 0 && !push<STACK>(stk, st.sp, r0, k0, status)) return false;
   if (keep < 4) {
     const int32_t r = keep == 0 ? r0 : (keep == 1 ? r1 : (keep == 2 ? r2 : r3));
     st.pend = -r - 1;
@@ -629,11 +718,12 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   return true;
 }
 
-template <int TRAV, bool COUNT, bool FILTER>
+template <int TRAV, bool COUNT, bool FILTER, int STACK = kStack>
 __device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
-                                            int* status, Tally& tally) {
-  if (TRAV == FK_TRAVERSE_ORDERED4) return inner_visit4<COUNT, FILTER>(s, rp, thr, st, stk, status, tally);
-  return inner_visit<COUNT, FILTER>(s, rp, thr, st, stk, status, tally);
+                                            int* status, Tally& tally, const float4* top = nullptr,
+                                            uint32_t top_base = 0xFFFFFFFFu) {
+  if (TRAV == FK_TRAVERSE_ORDERED4) return inner_visit4<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally);
+  return inner_visit<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally, top, top_base);
 }
 
 // Order-preserving key of a non-negative distance (total order, -0 below +0)
@@ -719,6 +809,64 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
   return mine;
 }
 
+#ifdef FK_LEAF_SMEM
+// The leaf phase with the owners' rays read from shared memory: each lane
+// publishes (origin, distance) and (direction, first triangle - first item)
+// once per phase (`sray`, 64 float4 for this warp), and a lane testing item j
+// reads its owner's two float4 instead of shuffling seven words per round.
+template <bool COUNT, bool FILTER>
+__device__ __forceinline__ bool leaf_phase_smem(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
+                                                OState& st, bool active, uint32_t* skey, float4* sray, Tally& tally) {
+  const unsigned full = 0xFFFFFFFFu;
+  const int lane = threadIdx.x & 31;
+  uint32_t first = 0, cnt = 0;
+  const bool mine = active && st.pend >= 0;
+  if (mine) {
+    const float4 L = __ldg(s.node_lo + st.pend), H = __ldg(s.node_hi + st.pend);
+    float entry;
+    if (COUNT) tally.box++;
+    if (child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry)) {
+      first = as_u32(L.w) / 3;
+      cnt = (as_u32(H.w) - as_u32(L.w)) / 3;
+      if (COUNT) tally.tri += cnt;
+    }
+    st.pend = -1;
+  }
+  uint32_t incl = cnt;
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t v = __shfl_up_sync(full, incl, d);
+    if (lane >= d) incl += v;
+  }
+  const uint32_t total = __shfl_sync(full, incl, 31);
+  if (total == 0) return mine;
+  const uint32_t excl = incl - cnt;
+  skey[lane] = dist_key(best);
+  if (cnt > 0) {
+    sray[2 * lane] = make_float4(rp.o.x, rp.o.y, rp.o.z, best);
+    sray[2 * lane + 1] = make_float4(rp.d.x, rp.d.y, rp.d.z, __uint_as_float(first - excl));
+  }
+  __syncwarp();
+  for (uint32_t base = 0; base < total; base += 32) {
+    const uint32_t j = base + lane;
+    int o = 0;
+    for (int step = 16; step > 0; step >>= 1) {
+      const uint32_t v = __shfl_sync(full, incl, o + step - 1);
+      if (v <= j) o += step;
+    }
+    if (j < total) {
+      const float4 A = sray[2 * o], B = sray[2 * o + 1];
+      float b = A.w;
+      tri_sample(s.rec, __float_as_uint(B.w) + j, xyz(A), xyz(B), lo, b);
+      if (b < A.w) atomicMin(skey + o, dist_key(b));
+    }
+  }
+  __syncwarp();
+  if (cnt > 0) best = dist_unkey(skey[lane]);
+  __syncwarp();  // the words are rewritten by the next leaf phase
+  return mine;
+}
+#endif
+
 // Takes the nearest still-open deferred entry; false when none is left.
 template <bool FILTER>
 __device__ __forceinline__ bool pop(OState& st, const int2* stk, float thr) {
@@ -759,18 +907,31 @@ __device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, f
   return i >= s.node_count;
 }
 
-template <int KIND, int TRAV, bool COUNT, bool FILTER>
-__global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
+// BLOCK: threads per block; STACK: deferred entries per lane (the ordered
+// traversals accept trees of depth below STACK, the 4-wide one of depth up
+// to (STACK - 1) / 3).
+template <int KIND, int TRAV, bool COUNT, bool FILTER, int BLOCK = 256, int STACK = kStack>
+__global__ void __launch_bounds__(BLOCK) hemi_trace_kernel(DynArgs p) {
   constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
-  int2 stk[is_ordered(TRAV) ? kStack : 1];  // deferred (ref, entry) pairs
-  __shared__ uint32_t leaf_keys[256 / 32][32];  // leaf-phase distance minimum, per warp
+  int2 stk[is_ordered(TRAV) ? STACK : 1];  // deferred (ref, entry) pairs
+  __shared__ uint32_t leaf_keys[BLOCK / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
+  extern __shared__ float4 top_smem[];  // p.top_count staged records (TRAV == ORDERED)
+  if (TRAV == FK_TRAVERSE_ORDERED && p.top_count) {
+    for (uint32_t i = threadIdx.x; i < 4 * p.top_count; i += blockDim.x) top_smem[i] = __ldg(p.top + i);
+    __syncthreads();
+  }
+  const uint32_t top_base = TRAV == FK_TRAVERSE_ORDERED && p.top_count ? p.top_base : 0xFFFFFFFFu;
+#ifdef FK_LEAF_SMEM
+  __shared__ float4 leaf_rays[BLOCK / 32][64];
+  float4* sray = leaf_rays[threadIdx.x >> 5];
+#endif
   Tally tally;
   bool active = false, exhausted = false;
-  uint32_t r = 0;
+  uint32_t slot = 0;  // scratch slot of the lane's ray: its texel's row, its sample
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX;
   int32_t cur = 0;  // skip walk: node index
@@ -789,9 +950,12 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
       base = __shfl_sync(full, base, leader);
       if (base + n_idle >= p.total) exhausted = true;
       if (!active) {
-        r = base + __popc(idle & lower);
+        const uint32_t r = base + __popc(idle & lower);
         if (r < p.total) {
-          const uint32_t k = r % p.spp;
+          // queue slot q of the texel -> sample k (a bijection of 0..spp-1)
+          const uint32_t q = r % p.spp;
+          const uint32_t k = p.sectors > 1 ? (q & 31u) * p.sectors + (q >> 5) : q;
+          slot = r - q + k;
           const uint32_t g = list_texel(p.ids, p.texel_limit, p.texel0 + r / p.spp, p.status);
           const uint32_t id = g == kMiss ? kMiss : __ldg(p.tidx + g);
           best = FLT_MAX;
@@ -810,7 +974,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
               if (COUNT) tally.box++;
               if (a < p.hi) {
                 st.sp = 0;
-                st.cur = p.s.root_is_leaf ? -1 : 0;
+                st.cur = p.s.root_is_leaf ? -1 : (top_base != 0xFFFFFFFFu ? (int32_t)top_base : 0);
                 st.pend = p.s.root_is_leaf ? 0 : -1;
                 st.pend_dist = a;
                 done = false;
@@ -822,7 +986,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
           } else if (id != kMiss) {
             atomicOr(p.status, 2);
           }
-          if (done) p.scratch[r] = best;
+          if (done) p.scratch[slot] = best;
           else active = true;
         }
       }
@@ -835,7 +999,7 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
     }
     if (is_ordered(TRAV)) {
       // phase choice, uniform across the warp
-      const bool spec_ok = st.sp < kStack - 4;
+      const bool spec_ok = st.sp < STACK - 4;
       const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
       const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
@@ -843,25 +1007,31 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
         wc[1] += leaf_phase;
         wc[leaf_phase ? 3 : 2] += __popc(leaf_phase ? leaves : need);
       }
+#ifdef FK_LEAF_SMEM
+      const bool visited =
+          leaf_phase && leaf_phase_smem<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, active, skey, sray, tally);
+#else
       const bool visited =
           leaf_phase && leaf_phase_warp<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, active, skey, tally);
+#endif
       if (active) {
         bool fin = false;
         if (leaf_phase) {
           if (visited) fin = settled<STOP>(best, p.hi);
         } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
-          if (!visit_inner<TRAV, COUNT, FILTER>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally))
+          if (!visit_inner<TRAV, COUNT, FILTER, STACK>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally, top_smem,
+                                                top_base))
             fin = true;
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, p.hi));
         if (fin) {
-          p.scratch[r] = best;
+          p.scratch[slot] = best;
           active = false;
         }
       }
     } else if (active) {
       if (skip_step<STOP, COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, cur, tally)) {
-        p.scratch[r] = best;
+        p.scratch[slot] = best;
         active = false;
       }
     }
@@ -878,6 +1048,104 @@ __global__ void __launch_bounds__(256) hemi_trace_kernel(DynArgs p) {
       for (int k = 0; k < 6; ++k) atomicAdd(p.tally + 2 + k, wc[k]);
     }
   }
+}
+
+// ------------------------------------------------------------------ staged top records
+// The first k inner records of a 2-wide tree in breadth-first order (its top
+// levels), one level per pass: record i of `top` copies a tree record, and
+// those of its inner children that are staged as well are referred to as
+// base + their staged index (base = the tree's record count), so a traversal
+// tells staged records by ref >= base.  Leaf refs and unstaged children are
+// kept.  One block of 1024 threads; k <= 1024 (a level then has at most 1024
+// records).
+__global__ void __launch_bounds__(1024) top_records_kernel(const float4* __restrict__ wide, uint32_t base,
+                                                           uint32_t k, float4* __restrict__ top) {
+  __shared__ int32_t ids[2][1024];
+  __shared__ uint32_t warp_sum[32];
+  __shared__ uint32_t level_total;
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) ids[0][0] = 0;
+  __syncthreads();
+  uint32_t first = 0, n = 1;  // staged index of the level's first record; the level's size
+  int cur = 0;
+  while (n > 0) {
+    float4 w0 = {}, w1 = {}, w2 = {}, w3 = {};
+    int32_t r0 = -1, r1 = -1;
+    uint32_t c = 0;
+    if (t < n) {
+      const float4* w = wide + 4 * (size_t)ids[cur][t];
+      w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
+      r0 = __float_as_int(w3.x);
+      r1 = __float_as_int(w3.y);
+      c = (r0 >= 0) + (r1 >= 0);
+    }
+    // exclusive scan of the inner-child counts over the block
+    uint32_t incl = c;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+      if (lane >= (uint32_t)d) incl += v;
+    }
+    if (lane == 31) warp_sum[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+      uint32_t v = warp_sum[lane], x = v;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= (uint32_t)d) x += y;
+      }
+      warp_sum[lane] = x - v;  // exclusive prefix of the warp totals
+    }
+    __syncthreads();
+    const uint32_t excl = warp_sum[warp] + incl - c;
+    const uint32_t next = first + n;  // staged index of the next level's first record
+    if (t < n) {
+      uint32_t q = excl;
+      if (r0 >= 0) {
+        if (next + q < k) {
+          ids[cur ^ 1][q] = r0;
+          r0 = (int32_t)(base + next + q);
+        }
+        ++q;
+      }
+      if (r1 >= 0) {
+        if (next + q < k) {
+          ids[cur ^ 1][q] = r1;
+          r1 = (int32_t)(base + next + q);
+        }
+        ++q;
+      }
+      w3.x = __int_as_float(r0);
+      w3.y = __int_as_float(r1);
+      float4* o = top + 4 * (size_t)(first + t);
+      o[0] = w0, o[1] = w1, o[2] = w2, o[3] = w3;
+    }
+    if (t == 1023) level_total = excl + c;
+    __syncthreads();
+    n = next < k ? min(level_total, k - next) : 0;
+    first = next;
+    cur ^= 1;
+    __syncthreads();  // ids[cur] of this level and level_total are rewritten by the next pass
+  }
+}
+
+int ensure_top(fk_ctx* ctx, fk_scene* s, uint32_t want) {
+  if (want == 0 || !s->wide || s->root_is_leaf) return FK_OK;
+  if (s->top && s->top_want == want && s->top_tree == s->tree) return FK_OK;
+  const uint32_t k = std::min(want, s->wide_count);
+  if (s->top) {
+    fk_dev_free(ctx, s->top);
+    s->top = nullptr;
+    s->top_count = 0;
+  }
+  int rc = fk_dev_alloc(ctx, (void**)&s->top, 4 * sizeof(float4) * (size_t)k);
+  if (rc != FK_OK) return rc;
+  top_records_kernel<<<1, 1024, 0, ctx->stream>>>(s->wide, s->wide_count, k, s->top);
+  rc = fk_after_launch(ctx, "top_records_kernel");
+  if (rc != FK_OK) return rc;
+  s->top_count = k;
+  s->top_want = want;
+  s->top_tree = s->tree;
+  return FK_OK;
 }
 
 // Folds each texel's per-sample distances in sample order (the *_step2
@@ -960,13 +1228,49 @@ __global__ void __launch_bounds__(256) hemi_reduce_kernel(HemiArgs p, const floa
   }
 }
 
+// The trace kernel for a launch: the counting and unfiltered variants at 256
+// threads and a 64-entry stack; the production variant (filtered box tests)
+// of the 2-wide ordered traversal in every block shape and stack depth.
+template <int KIND, int TRAV>
+static void (*pick_trace(bool count, bool filter, uint32_t block, uint32_t stack))(DynArgs) {
+  if (count) return filter ? hemi_trace_kernel<KIND, TRAV, true, true> : hemi_trace_kernel<KIND, TRAV, true, false>;
+  if (!filter) return hemi_trace_kernel<KIND, TRAV, false, false>;
+  if (TRAV == FK_TRAVERSE_ORDERED) {
+    if (stack == 32) {
+      if (block == 128) return hemi_trace_kernel<KIND, TRAV, false, true, 128, 32>;
+      if (block == 512) return hemi_trace_kernel<KIND, TRAV, false, true, 512, 32>;
+      return hemi_trace_kernel<KIND, TRAV, false, true, 256, 32>;
+    }
+    if (block == 128) return hemi_trace_kernel<KIND, TRAV, false, true, 128, kStack>;
+    if (block == 512) return hemi_trace_kernel<KIND, TRAV, false, true, 512, kStack>;
+  }
+  return hemi_trace_kernel<KIND, TRAV, false, true>;
+}
+
+// Block shape and stack depth a launch uses: the tuning's where the
+// production variant applies and the tree fits the stack, else 256 / 64.
+static void trace_shape(const fk_tuning& t, const HemiArgs& a, int trav, bool filter, uint32_t odepth,
+                        uint32_t* block, uint32_t* stack) {
+  *block = 256;
+  *stack = kStack;
+  if (a.tally || !filter || trav != FK_TRAVERSE_ORDERED) return;
+  *block = t.block_threads;
+  if (t.stack_depth == 32 && odepth <= 24) *stack = 32;
+}
+
 template <int KIND, int TRAV>
 static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter, uint32_t leaf_batch,
-                            uint32_t speculate) {
-  auto trace = a.tally ? (filter ? hemi_trace_kernel<KIND, TRAV, true, true> : hemi_trace_kernel<KIND, TRAV, true, false>)
-                       : (filter ? hemi_trace_kernel<KIND, TRAV, false, true> : hemi_trace_kernel<KIND, TRAV, false, false>);
+                            uint32_t speculate, const TraceExtras& x) {
+  uint32_t block = 256, stack = kStack;
+  trace_shape(ctx->tuning, a, TRAV, filter, x.odepth, &block, &stack);
+  auto trace = pick_trace<KIND, TRAV>(a.tally != nullptr, filter, block, stack);
+  const size_t smem = 64 * (size_t)x.top_count;
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(trace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "cudaFuncSetAttribute");
+  }
   int per_sm = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace, 256, 0);
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace, (int)block, smem);
   if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "occupancy");
   if (per_sm < 1) per_sm = 1;
   // Scratch: one float per ray, texels processed in chunks that fit it.
@@ -988,6 +1292,7 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
     d.refill = refill;
     d.leaf_batch = leaf_batch;
     d.speculate = speculate;
+    d.sectors = ray_sectors(ctx->tuning.ray_order, a.spp);
     d.lo = a.lo;
     d.hi = a.hi;
     d.scratch = scratch;
@@ -996,10 +1301,33 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
     d.tally = a.tally;
     d.ids = a.ids;
     d.texel_limit = a.texel_limit;
+    d.top = x.top;
+    d.top_count = x.top_count;
+    d.top_base = x.top_base;
     uint32_t blocks = (uint32_t)ctx->sm_count * (uint32_t)per_sm;
-    uint32_t need = (d.total + 255) / 256;
+    uint32_t need = (d.total + block - 1) / block;
     if (blocks > need) blocks = need;
-    trace<<<blocks, 256, 0, ctx->stream>>>(d);
+    if (x.window_bytes) {
+      // the window rides on this launch only: the stream's attributes stay as the caller set them
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3(blocks);
+      cfg.blockDim = dim3(block);
+      cfg.dynamicSmemBytes = smem;
+      cfg.stream = ctx->stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeAccessPolicyWindow;
+      at[0].val.accessPolicyWindow.base_ptr = const_cast<void*>(x.window);
+      at[0].val.accessPolicyWindow.num_bytes = x.window_bytes;
+      at[0].val.accessPolicyWindow.hitRatio = x.hit_ratio;
+      at[0].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+      at[0].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      e = cudaLaunchKernelEx(&cfg, trace, d);
+      if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "hemi_trace_kernel launch");
+    } else {
+      trace<<<blocks, block, smem, ctx->stream>>>(d);
+    }
     int rc = fk_after_launch(ctx, "hemi_trace_kernel");
     if (rc != FK_OK) return rc;
     HemiArgs r = a;
@@ -1036,7 +1364,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   Tally tally;
   bool active = false, exhausted = false;
-  uint32_t q = 0;
+  uint32_t slot = 0;  // scratch slot of the lane's ray (its sample's, in sample order)
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX, lo = 0.0f, hi = 0.0f;
   int32_t cur = 0;
@@ -1055,7 +1383,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
       base = __shfl_sync(full, base, leader);
       if ((unsigned long long)base + n_idle >= total) exhausted = true;
       if (!active) {
-        q = base + __popc(idle & lower);
+        const uint32_t q = base + __popc(idle & lower);
         if (q < total) {
           const unsigned long long r = p.r0 + (unsigned long long)q * p.stride;
           int a = 0, b = (int)p.njobs - 1;  // last job whose ray_base <= r
@@ -1066,7 +1394,15 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
           const BatchJobDev& J = jobs[a];
           sc = J.s;
           const unsigned long long local = r - J.ray_base;
-          const uint32_t g = (uint32_t)(local / J.spp), k = (uint32_t)(local % J.spp);
+          const uint32_t g = (uint32_t)(local / J.spp);
+          uint32_t k = (uint32_t)(local % J.spp);
+          slot = q;
+          if (p.ray_order == FK_RAY_ORDER_SECTOR && p.stride == 1 && J.spp >= 64 && (J.spp & 31u) == 0) {
+            // queue slot k of the texel traces sample (k % 32) * (spp / 32) + k / 32
+            const uint32_t ks = (k & 31u) * (J.spp >> 5) + (k >> 5);
+            slot = q - k + ks;
+            k = ks;
+          }
           const uint32_t id = __ldg(J.tidx + g);
           best = FLT_MAX;
           lo = J.lo;
@@ -1098,7 +1434,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
           } else if (id != kMiss) {
             atomicOr(p.status, 2);
           }
-          if (done) p.scratch[q] = best;
+          if (done) p.scratch[slot] = best;
           else active = true;
         }
       }
@@ -1122,13 +1458,13 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, hi));
         if (fin) {
-          p.scratch[q] = best;
+          p.scratch[slot] = best;
           active = false;
         }
       }
     } else if (active) {
       if (skip_step<STOP, false, FILTER>(s, rp, lo, hi, best, cur, tally) || (uint32_t)cur >= end) {
-        p.scratch[q] = best;
+        p.scratch[slot] = best;
         active = false;
       }
     }
@@ -1287,6 +1623,7 @@ static cudaError_t run_hemi_external(const HemiArgs& a, cudaStream_t stream, int
   d.refill = tun.refill;
   d.leaf_batch = tun.leaf_batch;
   d.speculate = tun.speculate;
+  d.sectors = ray_sectors(tun.ray_order, a.spp);
   d.lo = a.lo;
   d.hi = a.hi;
   d.scratch = dist;
@@ -1295,6 +1632,9 @@ static cudaError_t run_hemi_external(const HemiArgs& a, cudaStream_t stream, int
   d.tally = nullptr;
   d.ids = nullptr;
   d.texel_limit = 0;
+  d.top = nullptr;
+  d.top_count = 0;
+  d.top_base = 0xFFFFFFFFu;
   uint32_t blocks = (uint32_t)sm_count * (uint32_t)per_sm;
   uint32_t need = (d.total + 255) / 256;
   if (blocks > need) blocks = need;
@@ -1443,9 +1783,11 @@ __device__ float walk_twoside(const SceneDev& s, f3 o, f3 d, float mint, uint32_
   return mint;
 }
 
+// max_d: the walks' initial closest distance (FLT_MAX in the shaders); a
+// miss writes t = FLT_MAX whatever it is.
 template <int CULL>
-__global__ void __launch_bounds__(128) meshmap_kernel(SceneDev s, const float4* __restrict__ pix, uint32_t offset,
-                                                      uint32_t count, float4* __restrict__ coords,
+__global__ void __launch_bounds__(128) meshmap_kernel(SceneDev s, const float4* __restrict__ pix, float max_d,
+                                                      uint32_t offset, uint32_t count, float4* __restrict__ coords,
                                                       uint32_t* __restrict__ tidx) {
   uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= count) return;
@@ -1453,7 +1795,7 @@ __global__ void __launch_bounds__(128) meshmap_kernel(SceneDev s, const float4* 
   f3 p = xyz(__ldg(pix + 2 * (size_t)g)), d = xyz(__ldg(pix + 2 * (size_t)g + 1));
   uint32_t id = kMiss;
   f3 w = mk3(0.0f, 0.0f, 0.0f);
-  float t = FLT_MAX;
+  float t = max_d;
   if (CULL) {
     walk_oneside<+1>(s, p, d, t, id, w);
     walk_oneside<-1>(s, p, neg(d), t, id, w);
@@ -1461,16 +1803,17 @@ __global__ void __launch_bounds__(128) meshmap_kernel(SceneDev s, const float4* 
     t = fminf(t, walk_twoside(s, p, d, t, id, w));
     t = fminf(t, walk_twoside(s, p, neg(d), t, id, w));
   }
+  if (id == kMiss) t = FLT_MAX;
   coords[g] = make_float4(t, w.x, w.y, w.z);
   tidx[g] = id;
 }
 
-int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, uint32_t offset, uint32_t count,
-                   float4* coords, uint32_t* tidx) {
+int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, float max_d, uint32_t offset,
+                   uint32_t count, float4* coords, uint32_t* tidx) {
   if (count == 0) return FK_OK;
   uint32_t blocks = (count + 127) / 128;
-  if (cull) meshmap_kernel<1><<<blocks, 128, 0, ctx->stream>>>(dev_of(s), m->pix, offset, count, coords, tidx);
-  else meshmap_kernel<0><<<blocks, 128, 0, ctx->stream>>>(dev_of(s), m->pix, offset, count, coords, tidx);
+  if (cull) meshmap_kernel<1><<<blocks, 128, 0, ctx->stream>>>(dev_of(s), m->pix, max_d, offset, count, coords, tidx);
+  else meshmap_kernel<0><<<blocks, 128, 0, ctx->stream>>>(dev_of(s), m->pix, max_d, offset, count, coords, tidx);
   return fk_after_launch(ctx, "meshmap_kernel");
 }
 

@@ -13,11 +13,16 @@
 // Host code cannot pass the array's name to a kernel: on the host that name is
 // only a stand-in, not a device address.  The device address is obtained once
 // per device with cudaGetSymbolAddress, with that device current, on the first
-// call made on that device.  All calls share the one array, which keeps whatever the last
-// call left in it: the queue and status words are cleared at the start of each
-// call (the distance slots are always written before they are read), and calls
-// whose work overlaps on the GPU (different streams, or threads on one device
-// without ordering) race on it and must be serialised by the caller.
+// call made on that device, and kept for the life of the process (a device
+// reset after that call is not supported: it also ends the context the scene
+// belongs to).  All calls share the one array, which keeps whatever the last
+// call left in it: the queue word is cleared at the start of each call (the
+// distance slots are always written before they are read), and calls whose
+// work overlaps on the GPU (different streams, or threads on one device
+// without ordering) race on it and must be serialised by the caller.  Device
+// errors (a traversal that overflowed its stack, a texel naming a triangle
+// outside the scene) go to the context's own status word, which already
+// exists, so fk_ctx_check reports them as it does for fk_hemisphere.
 #include <mutex>
 #include <string>
 
@@ -26,7 +31,7 @@
 namespace {
 
 constexpr uint32_t kMaxRays = FK_NOALLOC_MAX_RAYS;
-constexpr size_t kWords = 64;  // control area after the distances: queue word, status word, padding
+constexpr size_t kWords = 64;  // control area after the distances: queue word, padding
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) float g_noalloc_scratch[kMaxRays + kWords];
@@ -81,7 +86,7 @@ extern "C" int fk_hemisphere_noalloc(const fk_scene* scene, const float* coords4
   if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "cudaGetSymbolAddress");
   uint32_t* words = (uint32_t*)(scratch + kMaxRays);
   cudaStream_t st = (cudaStream_t)stream;
-  e = cudaMemsetAsync(words, 0, 2 * sizeof(uint32_t), st);  // queue and status start at zero
+  e = cudaMemsetAsync(words, 0, sizeof(uint32_t), st);  // the queue starts at zero
   if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "cudaMemsetAsync");
   fk::HemiLaunch h;
   h.kind = kind;
@@ -100,8 +105,8 @@ extern "C" int fk_hemisphere_noalloc(const fk_scene* scene, const float* coords4
   h.hits0 = hits0;
   h.hits1 = kind == FK_AO_BN ? hits1 : nullptr;
   std::string err;
-  int rc = fk::launch_hemisphere_external(scene, h, st, ctx->sm_count, ctx->tuning, scratch, words,
-                                          (int*)(words + 1), err);
+  int rc = fk::launch_hemisphere_external(scene, h, st, ctx->sm_count, ctx->tuning, scratch, words, ctx->status,
+                                          err);
   if (rc != FK_OK) return fk_fail(ctx, rc, "fk_hemisphere_noalloc: " + err);
   return FK_OK;
 }

@@ -16,6 +16,7 @@
 // Sample tables come from `seed` (the reference draws them from
 // std::random_device); AO and bent normals with equal sample parameters
 // share one traversal.
+#include <cfloat>
 #include <cstring>
 #include <future>
 #include <string>
@@ -137,7 +138,7 @@ int fk_run(fk_ctx* ctx, const fk_run_params* p) {
   const size_t nn = n ? n : 1;
   fk_buf *coords, *tidx;
   if ((rc = o.alloc(16 * nn, &coords)) != FK_OK || (rc = o.alloc(4 * nn, &tidx)) != FK_OK) return rc;
-  if ((rc = fk_meshmap(ctx, o.scene, o.map, p->ignore_backfaces, 0, n, coords, tidx)) != FK_OK) return rc;
+  if ((rc = fk_meshmap(ctx, o.scene, o.map, p->ignore_backfaces, FLT_MAX, 0, n, coords, tidx)) != FK_OK) return rc;
 
   // exports: one device image buffer, reused; each downloaded image is encoded
   // and written on a thread of its own while the device runs the next

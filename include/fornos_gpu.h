@@ -76,14 +76,36 @@ int fk_ctx_trim(fk_ctx* ctx);
 uint64_t fk_launch_count(const fk_ctx* ctx);
 
 /* Knobs of the dynamically scheduled hemisphere traversal (defaults 16, 8,
- * 1, 0, from a full-size sweep of the plane workload); fk_tune_hemisphere
- * picks them by measurement. */
+ * 1, FK_RAY_ORDER_SECTOR, from full-size sweeps of the plane workload);
+ * fk_tune_hemisphere picks them by measurement.  No knob changes a result:
+ * each ray still writes the slot of its own sample, and the per-texel sums
+ * run in sample order. */
+#define FK_RAY_ORDER_SAMPLE 0 /* a texel's rays are taken in sample order */
+#define FK_RAY_ORDER_SECTOR 1 /* sample k = (q % 32) * (spp / 32) + q / 32 for queue slot q: the 32
+                                 rays a warp takes share one azimuth sector of the sample table
+                                 (Src/math.h:339-382 puts the low bits of k into the azimuth's high
+                                 bits); spp a multiple of 32, else sample order */
 typedef struct fk_tuning {
   uint32_t refill;      /* idle lanes of a warp that trigger a batch fetch (1..32) */
   uint32_t leaf_batch;  /* lanes holding a postponed leaf that start a leaf phase (1..32) */
   uint32_t speculate;   /* lanes holding a leaf keep visiting inner records (0 / 1) */
-  uint32_t reserved;
+  uint32_t ray_order;   /* FK_RAY_ORDER_* */
+  uint32_t top_records; /* 2-wide ordered traversal: the first top_records inner records of the tree in
+                           breadth-first order (its top levels) are staged in each block's shared
+                           memory (0 = none, at most FK_MAX_TOP_RECORDS; 64 bytes each) */
+  uint32_t l2_persist;  /* FK_L2_*: records read through a persisting L2 access-policy window.  The
+                           window is a launch attribute of the trace kernel (the stream's attributes
+                           are untouched); the context sets the device's persisting L2 set-aside
+                           while a window is in use and restores it when the knob is turned off or
+                           the context is destroyed */
+  uint32_t block_threads; /* threads per block of the trace kernel: 128, 256 or 512 */
+  uint32_t stack_depth;   /* deferred entries per lane of the ordered traversals: 32 or 64; 32 serves
+                             trees of at most 24 levels (4-wide: 10), deeper trees use 64 */
 } fk_tuning;
+#define FK_MAX_TOP_RECORDS 1024
+#define FK_L2_NONE 0
+#define FK_L2_TREE 1      /* the inner records of the tree being walked */
+#define FK_L2_TRIANGLES 2 /* the triangle records (hit ratio: set-aside / their size) */
 int fk_ctx_set_tuning(fk_ctx* ctx, const fk_tuning* tuning);
 int fk_ctx_get_tuning(const fk_ctx* ctx, fk_tuning* tuning);
 
@@ -234,9 +256,13 @@ int fk_samples_cosine(uint32_t spp, uint32_t perms, uint32_t seed, float* out4);
  * Mesh mapping, Shaders/meshmapping_nobackfaces.comp (cull_backfaces = 1,
  * the default of Src/fornos.h:48) or Shaders/meshmapping.comp, over texels
  * [offset, offset + count) of `map`.  coords: float4 (t, b0, b1, b2) per
- * texel; tidx: u32 per texel, 0xFFFFFFFF on a miss. */
-int fk_meshmap(fk_ctx* ctx, const fk_scene* scene, const fk_texel_map* map, int cull_backfaces, uint32_t offset,
-               uint32_t count, fk_buf* coords, fk_buf* tidx);
+ * texel; tidx: u32 per texel, 0xFFFFFFFF on a miss.  max_dist is the walks'
+ * initial closest distance (curdist / mint of the shaders, FLT_MAX there):
+ * only hits at t < max_dist are taken, and boxes are pruned against it.
+ * FLT_MAX gives the reference's mapping; a miss writes t = FLT_MAX either
+ * way.  Must be positive (FK_ERR_INVALID otherwise). */
+int fk_meshmap(fk_ctx* ctx, const fk_scene* scene, const fk_texel_map* map, int cull_backfaces, float max_dist,
+               uint32_t offset, uint32_t count, fk_buf* coords, fk_buf* tidx);
 
 /* ShaderParams of Src/solver_ao.h:67-73. */
 typedef struct fk_sample_params {
@@ -319,8 +345,14 @@ int fk_gather(fk_ctx* ctx, const fk_scene* scene, int kind, const fk_buf* coords
  * samples4 as fk_samples_cosine fills them, outputs as fk_hemisphere writes
  * them); `stream` is a cudaStream_t (NULL = default stream).  The scene's
  * device must be current.  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress).  Every call reuses the same array: calls whose work may overlap on the GPU
- * race on it and must be serialised by the caller. */
+ * device address (cudaGetSymbolAddress) and keeps it for the process, so make
+ * that first call before any stream capture, and do not reset the device
+ * after it.  Every call reuses the same array: calls whose work may overlap on
+ * the GPU race on it and must be serialised by the caller.  Device errors (a
+ * traversal that overflowed its stack, a texel naming a triangle outside the
+ * scene) are recorded in the context's status word, as fk_hemisphere records
+ * them: synchronise `stream`, then call fk_ctx_check, which reports them as
+ * FK_ERR_DEVICE. */
 #define FK_NOALLOC_MAX_RAYS (1u << 22)
 int fk_hemisphere_noalloc(const fk_scene* scene, const float* coords4, const uint32_t* tidx, int kind,
                           const fk_sample_params* params, const float* samples4, uint32_t offset, uint32_t count,
@@ -411,8 +443,10 @@ int fk_batch_info(const fk_batch* batch, uint64_t* rays, uint32_t* texels, uint3
 /* Autotuner: times a strided sample of about sample_rays rays of every job
  * (0 = 4M) under each candidate schedule (ordered over the 2-wide or the
  * collapsed 4-wide layout vs the skip-pointer walk, filtered vs divided box
- * tests, refill threshold, postponed-leaf batch) and
- * keeps the fastest for later runs; reports it. */
+ * tests, refill threshold, postponed-leaf batch) and keeps the fastest for
+ * later runs; reports it.  The ray order is the context's (a strided sample
+ * has no per-texel order to time); the batch kernel runs 256-thread blocks
+ * with 64-entry stacks. */
 int fk_batch_tune(fk_batch* batch, uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse);
 /* One run on the context's stream; traverse 0 = the tuned schedule. */
 int fk_batch_run(fk_batch* batch, int traverse);
@@ -421,8 +455,17 @@ int fk_batch_capture(fk_batch* batch, int traverse);
 int fk_batch_replay(fk_batch* batch);
 int fk_batch_free(fk_batch* batch);
 
-/* The autotuner for one fk_hemisphere call (same arguments); apply the result
- * with fk_ctx_set_tuning and the returned traverse flags. */
+/* The autotuner for one fk_hemisphere call (same arguments; sample_rays 0 =
+ * 16M).  It times the call's own trace kernel on eight windows of consecutive
+ * texels spread over the range (about sample_rays rays, traced as the whole
+ * pass traces them) and searches the knobs one group at a time from the
+ * context's tuning, keeping each group's fastest: traversal layout (2-wide,
+ * 4-wide, skip walk), refill x leaf batch, speculation, ray order, block
+ * shape x stack depth, staged top records, L2 window.  Rays per lane follow
+ * from the persistent schedule: a lane takes its next ray as soon as it
+ * finishes one, and `refill` sets how many lanes a warp refills at once.
+ * Apply the result with fk_ctx_set_tuning and the returned traverse flags;
+ * the context's tuning is left unchanged. */
 int fk_tune_hemisphere(fk_ctx* ctx, const fk_scene* scene, const fk_buf* coords, const fk_buf* tidx, int kind,
                        const fk_sample_params* params, const fk_buf* samples4, uint32_t offset, uint32_t count,
                        uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse);
@@ -461,6 +504,7 @@ typedef struct fk_bake_desc {
   fk_bake_sampler bent_normals;
   fk_bake_sampler thickness;
   int traverse;             /* FK_TRAVERSE_* */
+  float mapping_max_distance; /* fk_meshmap's max_dist; 0 = no limit (the reference's mapping) */
 } fk_bake_desc;
 
 /* Host outputs, texel_count rows each; NULL skips the copy. */

@@ -1,7 +1,8 @@
 """Build recipe for oracle/_ref: the reference's own code, compiled on the host.
 
 Test infrastructure only.  Compiles, from the files where they lie in the
-reference tree (default /root/reference, override with FORNOS_REF_ROOT):
+reference tree (the first argument; else FORNOS_REF_ROOT; else a checkout
+named `reference` beside this repository):
 
   * Src/bvh.cpp, Src/compute.cpp          verbatim, with a force-included shim
                                            (ref_shim.h) for the MSVC-only
@@ -46,7 +47,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
 OBJ = os.path.join(OUT, "obj")
-REF = os.environ.get("FORNOS_REF_ROOT", "/root/reference")
+REPO = os.path.dirname(HERE)
+REF = (sys.argv[1] if len(sys.argv) > 1 else
+       os.environ.get("FORNOS_REF_ROOT", os.path.join(os.path.dirname(REPO), "reference")))
 
 CXX = ["g++", "-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-fopenmp", "-w"]
 

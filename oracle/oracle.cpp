@@ -626,10 +626,14 @@ static float walk_twoside(const SceneView& s, F3 o, F3 d, float mint, uint32_t& 
 }
 
 // One texel of the mesh-mapping pass: outputs vec4(t, bary) and the hit index.
-static void map_texel(const SceneView& s, F3 p, F3 d, int cull, float* coord, uint32_t* tidx, Counters* ctr) {
+// max_d is the walks' initial closest distance (FLT_MAX in the shaders:
+// meshmapping_nobackfaces.comp:193, meshmapping.comp:150); a miss writes
+// t = FLT_MAX whatever it is.
+static void map_texel(const SceneView& s, F3 p, F3 d, int cull, float max_d, float* coord, uint32_t* tidx,
+                      Counters* ctr) {
   uint32_t id = kMiss;
   F3 w = mk(0, 0, 0);
-  float t = FLT_MAX;
+  float t = max_d;
   if (cull) {
     walk_oneside(s, p, d, +1, t, id, w, ctr);
     walk_oneside(s, p, -d, -1, t, id, w, ctr);
@@ -637,6 +641,7 @@ static void map_texel(const SceneView& s, F3 p, F3 d, int cull, float* coord, ui
     t = std::fmin(t, walk_twoside(s, p, d, t, id, w, ctr));
     t = std::fmin(t, walk_twoside(s, p, -d, t, id, w, ctr));
   }
+  if (id == kMiss) t = FLT_MAX;
   coord[0] = t; coord[1] = w.x; coord[2] = w.y; coord[3] = w.z;
   *tidx = id;
 }
@@ -866,14 +871,14 @@ static SceneView sview(const void* nodes, uint32_t count, const float* pos4, con
 // d.xyz, pad) = Pix_GPUData (Src/meshmapping.h:15-20).  counters (optional):
 // total box / triangle tests.
 int orc_meshmap(const void* nodes, uint32_t nnodes, const float* pos4, const float* pix8, uint32_t count, int cull,
-                float* coords, uint32_t* tidx, uint64_t* counters) {
+                float max_d, float* coords, uint32_t* tidx, uint64_t* counters) {
   SceneView s = sview(nodes, nnodes, pos4, nullptr);
   uint64_t tb = 0, tt = 0;
 #pragma omp parallel for schedule(dynamic, 64) reduction(+ : tb, tt)
   for (int64_t i = 0; i < (int64_t)count; ++i) {
     Counters c = {0, 0};
     const float* px = pix8 + 8 * (size_t)i;
-    map_texel(s, ld3(px), ld3(px + 4), cull, coords + 4 * (size_t)i, tidx + i, counters ? &c : nullptr);
+    map_texel(s, ld3(px), ld3(px + 4), cull, max_d, coords + 4 * (size_t)i, tidx + i, counters ? &c : nullptr);
     tb += c.box;
     tt += c.tri;
   }

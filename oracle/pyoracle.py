@@ -25,6 +25,7 @@ _int = ctypes.c_int
 NODE_DTYPE = np.dtype([("lo", np.float32, 3), ("hi", np.float32, 3), ("start", np.uint32), ("end", np.uint32),
                        ("jump", np.uint32)])
 assert NODE_DTYPE.itemsize == 36
+FLT_MAX = float(np.finfo(np.float32).max)
 
 
 def build_oracle(force=False):
@@ -147,13 +148,15 @@ class Oracle:
         return out
 
     # ---- shaders
-    def meshmap(self, nodes, pos4, pix8, cull=True, counters=False):
+    def meshmap(self, nodes, pos4, pix8, cull=True, counters=False, max_dist=FLT_MAX):
+        """max_dist: the walks' initial closest distance (FLT_MAX in the
+        shaders)."""
         n = pix8.shape[0]
         coords = np.zeros((n, 4), np.float32)
         tidx = np.zeros(n, np.uint32)
         ctr = np.zeros(2, np.uint64) if counters else None
         self.lib.orc_meshmap(nodes.ctypes.data_as(_vp), _u32(len(nodes)), ptr(pos4), ptr(pix8), _u32(n), _int(int(cull)),
-                             ptr(coords), ptr(tidx, _u32p), ptr(ctr, _u64p))
+                             ctypes.c_float(max_dist), ptr(coords), ptr(tidx, _u32p), ptr(ctr, _u64p))
         return (coords, tidx, ctr) if counters else (coords, tidx)
 
     def hemisphere(self, kind, nodes, pos4, nrm4, coords, tidx, samples4, spp, min_d, max_d, texels=None,

@@ -108,4 +108,4 @@ def test_autotuner_choice_gives_same_results(ctx, setup):
                                     j["max_distance"], j["samples"], 0, j["texel_count"], sample_rays=1 << 15)
     ctx.set_tuning(**tun)
     assert trav & api.SCHEDULE_DYNAMIC
-    ctx.set_tuning(8, 8, 0)
+    ctx.set_tuning(refill=8, leaf_batch=8, speculate=0)
