@@ -72,28 +72,6 @@ int launch_tri_records(fk_ctx* ctx, fk_scene* s) {
   return fk_after_launch(ctx, "tri_records_kernel");
 }
 
-#ifdef FK_BARY_FILTER
-// True only when the sampling test's barycentric check (y = ny / den,
-// z = nz / den, x = 1 - y - z; x, y, z >= 0 and y, z <= 1) certainly fails.
-// The quotients are estimated with the hardware reciprocal (rcp.approx: at
-// most 1 ulp, 2^-23 relative) and one rounded multiplication, so each
-// estimate is within 2^-21.4 relative of the divided value; a rejection is
-// taken only with a margin of 2^-19 on y and z (2^-18 on x, which adds two
-// roundings and both estimates' errors; y and z then lie in [-2^-19, 1 +
-// 2^-19]).  den must be a normal positive float below 2^100 (no flush, no
-// overflow); otherwise, and for NaN estimates, the exact division decides.
-__device__ __forceinline__ bool bary_certainly_outside(float ny, float nz, float den) {
-  if (!(den >= 1.17549435e-38f && den < 1.2676506e30f)) return false;
-  float r;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(den));
-  const float y = __fmul_rn(ny, r), z = __fmul_rn(nz, r);
-  const float m = 1.9073486e-06f;  // 2^-19
-  if (y < -m || z < -m || y > __fadd_rn(1.0f, m) || z > __fadd_rn(1.0f, m)) return true;
-  const float x = __fsub_rn(__fsub_rn(1.0f, y), z);
-  return x < -3.8146973e-06f;  // 2^-18
-}
-#endif
-
 // ------------------------------------------------------------------ sampling test
 // Shaders/ao_step1.comp:71-92 followed by the range test of :100-105: returns
 // true and lowers `best` when the triangle is hit at t in [lo, best).  The
@@ -118,9 +96,6 @@ __device__ __forceinline__ void tri_sample(const float4* __restrict__ rec, uint3
   float den = __fsub_rn(__fmul_rn(d00, d11), __fmul_rn(d01, d01));
   const float ny = __fsub_rn(__fmul_rn(d11, d20), __fmul_rn(d01, d21));
   const float nz = __fsub_rn(__fmul_rn(d00, d21), __fmul_rn(d01, d20));
-#ifdef FK_BARY_FILTER
-  if (bary_certainly_outside(ny, nz, den)) return;
-#endif
   float y = __fdiv_rn(ny, den);
   float z = __fdiv_rn(nz, den);
   float x = __fsub_rn(__fsub_rn(1.0f, y), z);
@@ -658,6 +633,69 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   return true;
 }
 
+#ifdef FK_EXP_LEAN
+// Inner-phase box test without the exact-only branch: for the rare ray with a
+// direction component in (0, 2^-100) every inner box is accepted (inner boxes
+// only prune; the leaf boxes are still tested exactly), with an entry of
+// -FLT_MAX so deferred culling keeps it.
+__device__ __forceinline__ bool box_maybe_lean(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
+  f3 n1 = sub(lo, r.o), n2 = sub(hi, r.o);
+  f3 t1 = mk3(__fmul_rn(n1.x, r.inv.x), __fmul_rn(n1.y, r.inv.y), __fmul_rn(n1.z, r.inv.z));
+  f3 t2 = mk3(__fmul_rn(n2.x, r.inv.x), __fmul_rn(n2.y, r.inv.y), __fmul_rn(n2.z, r.inv.z));
+  f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
+  float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
+  float b = fminf(tx.x, fminf(tx.y, tx.z));
+  const float inf = __int_as_float(0x7f800000);
+  const float a_lo = below(a), b_hi = above(b);
+  const bool reject = !(a < inf) || !(b > -inf) || b_hi < 0.0f || a_lo > b_hi || a_lo >= thr;
+  entry = r.exact_only ? -FLT_MAX : a;
+  return r.exact_only || !reject;
+}
+
+// Inner visit with straight-line placement: both children's roles (postponed
+// leaf, next record, deferred entries near first) are decided by selects and
+// the deferred entries written by predicated stores; one overflow check per
+// visit.  Same visit order and stack contents as inner_visit.
+template <bool COUNT, bool FILTER, int STACK = kStack>
+__device__ __forceinline__ bool inner_visit_lean(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
+                                                 int* status, Tally& tally) {
+  const float4* w = s.wide + 4 * (size_t)st.cur;
+  const float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
+  float d0, d1;
+  bool h0, h1;
+  if (FILTER) {
+    h0 = box_maybe_lean(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
+    h1 = box_maybe_lean(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
+  } else {
+    h0 = child_maybe<false>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
+    h1 = child_maybe<false>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
+  }
+  if (COUNT) tally.box += 2;
+  const bool swap = d1 < d0;
+  const bool hn = swap ? h1 : h0, hf = swap ? h0 : h1;
+  const float dn = swap ? d1 : d0, df = swap ? d0 : d1;
+  const int32_t rn = __float_as_int(swap ? w3.y : w3.x), rf = __float_as_int(swap ? w3.x : w3.y);
+  const bool nl = hn && rn < 0, ni = hn && rn >= 0, fl = hf && rf < 0, fi = hf && rf >= 0;
+  const bool take_nl = nl && st.pend < 0;
+  const bool take_fl = fl && st.pend < 0 && !take_nl;
+  const bool push_n = nl && !take_nl;
+  const bool push_f = (fl && !take_fl) || (fi && ni);
+  int sp = st.sp;
+  if (push_n && sp < STACK) stk[sp] = make_int2(rn, __float_as_int(dn));
+  sp += push_n;
+  if (push_f && sp < STACK) stk[sp] = make_int2(rf, __float_as_int(df));
+  sp += push_f;
+  st.pend = take_nl ? -rn - 1 : (take_fl ? -rf - 1 : st.pend);
+  st.cur = ni ? rn : (fi ? rf : -1);
+  st.sp = sp;
+  if (sp > STACK) {
+    atomicOr(status, 1);
+    return false;
+  }
+  return true;
+}
+#endif
+
 // Compare-exchange of (key, ref) pairs: ascending keys.
 __device__ __forceinline__ void cex(float& ka, int32_t& ra, float& kb, int32_t& rb) {
   const bool sw = kb < ka;
@@ -723,7 +761,11 @@ __device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp,
                                             int* status, Tally& tally, const float4* top = nullptr,
                                             uint32_t top_base = 0xFFFFFFFFu) {
   if (TRAV == FK_TRAVERSE_ORDERED4) return inner_visit4<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally);
+#ifdef FK_EXP_LEAN
+  return inner_visit_lean<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally);
+#else
   return inner_visit<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally, top, top_base);
+#endif
 }
 
 // Order-preserving key of a non-negative distance (total order, -0 below +0)
@@ -809,64 +851,6 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
   return mine;
 }
 
-#ifdef FK_LEAF_SMEM
-// The leaf phase with the owners' rays read from shared memory: each lane
-// publishes (origin, distance) and (direction, first triangle - first item)
-// once per phase (`sray`, 64 float4 for this warp), and a lane testing item j
-// reads its owner's two float4 instead of shuffling seven words per round.
-template <bool COUNT, bool FILTER>
-__device__ __forceinline__ bool leaf_phase_smem(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
-                                                OState& st, bool active, uint32_t* skey, float4* sray, Tally& tally) {
-  const unsigned full = 0xFFFFFFFFu;
-  const int lane = threadIdx.x & 31;
-  uint32_t first = 0, cnt = 0;
-  const bool mine = active && st.pend >= 0;
-  if (mine) {
-    const float4 L = __ldg(s.node_lo + st.pend), H = __ldg(s.node_hi + st.pend);
-    float entry;
-    if (COUNT) tally.box++;
-    if (child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry)) {
-      first = as_u32(L.w) / 3;
-      cnt = (as_u32(H.w) - as_u32(L.w)) / 3;
-      if (COUNT) tally.tri += cnt;
-    }
-    st.pend = -1;
-  }
-  uint32_t incl = cnt;
-  for (int d = 1; d < 32; d <<= 1) {
-    const uint32_t v = __shfl_up_sync(full, incl, d);
-    if (lane >= d) incl += v;
-  }
-  const uint32_t total = __shfl_sync(full, incl, 31);
-  if (total == 0) return mine;
-  const uint32_t excl = incl - cnt;
-  skey[lane] = dist_key(best);
-  if (cnt > 0) {
-    sray[2 * lane] = make_float4(rp.o.x, rp.o.y, rp.o.z, best);
-    sray[2 * lane + 1] = make_float4(rp.d.x, rp.d.y, rp.d.z, __uint_as_float(first - excl));
-  }
-  __syncwarp();
-  for (uint32_t base = 0; base < total; base += 32) {
-    const uint32_t j = base + lane;
-    int o = 0;
-    for (int step = 16; step > 0; step >>= 1) {
-      const uint32_t v = __shfl_sync(full, incl, o + step - 1);
-      if (v <= j) o += step;
-    }
-    if (j < total) {
-      const float4 A = sray[2 * o], B = sray[2 * o + 1];
-      float b = A.w;
-      tri_sample(s.rec, __float_as_uint(B.w) + j, xyz(A), xyz(B), lo, b);
-      if (b < A.w) atomicMin(skey + o, dist_key(b));
-    }
-  }
-  __syncwarp();
-  if (cnt > 0) best = dist_unkey(skey[lane]);
-  __syncwarp();  // the words are rewritten by the next leaf phase
-  return mine;
-}
-#endif
-
 // Takes the nearest still-open deferred entry; false when none is left.
 template <bool FILTER>
 __device__ __forceinline__ bool pop(OState& st, const int2* stk, float thr) {
@@ -910,8 +894,11 @@ __device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, f
 // BLOCK: threads per block; STACK: deferred entries per lane (the ordered
 // traversals accept trees of depth below STACK, the 4-wide one of depth up
 // to (STACK - 1) / 3).
+#ifndef FK_EXP_MINB
+#define FK_EXP_MINB 1
+#endif
 template <int KIND, int TRAV, bool COUNT, bool FILTER, int BLOCK = 256, int STACK = kStack>
-__global__ void __launch_bounds__(BLOCK) hemi_trace_kernel(DynArgs p) {
+__global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? FK_EXP_MINB : 1) hemi_trace_kernel(DynArgs p) {
   constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
@@ -925,10 +912,6 @@ __global__ void __launch_bounds__(BLOCK) hemi_trace_kernel(DynArgs p) {
     __syncthreads();
   }
   const uint32_t top_base = TRAV == FK_TRAVERSE_ORDERED && p.top_count ? p.top_base : 0xFFFFFFFFu;
-#ifdef FK_LEAF_SMEM
-  __shared__ float4 leaf_rays[BLOCK / 32][64];
-  float4* sray = leaf_rays[threadIdx.x >> 5];
-#endif
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t slot = 0;  // scratch slot of the lane's ray: its texel's row, its sample
@@ -970,9 +953,9 @@ __global__ void __launch_bounds__(BLOCK) hemi_trace_kernel(DynArgs p) {
             if (!p.s.filter_ok) rp.exact_only = true;
             if (is_ordered(TRAV)) {
               float4 L = __ldg(p.s.node_lo), H = __ldg(p.s.node_hi);
-              float a = ray_box(o, dir, xyz(L), xyz(H));
+              float a;
               if (COUNT) tally.box++;
-              if (a < p.hi) {
+              if (child_hit<FILTER>(rp, xyz(L), xyz(H), p.hi, a)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
                 st.cur = p.s.root_is_leaf ? -1 : (top_base != 0xFFFFFFFFu ? (int32_t)top_base : 0);
                 st.pend = p.s.root_is_leaf ? 0 : -1;
@@ -1007,13 +990,8 @@ __global__ void __launch_bounds__(BLOCK) hemi_trace_kernel(DynArgs p) {
         wc[1] += leaf_phase;
         wc[leaf_phase ? 3 : 2] += __popc(leaf_phase ? leaves : need);
       }
-#ifdef FK_LEAF_SMEM
-      const bool visited =
-          leaf_phase && leaf_phase_smem<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, active, skey, sray, tally);
-#else
       const bool visited =
           leaf_phase && leaf_phase_warp<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, active, skey, tally);
-#endif
       if (active) {
         bool fin = false;
         if (leaf_phase) {
@@ -1022,6 +1000,19 @@ __global__ void __launch_bounds__(BLOCK) hemi_trace_kernel(DynArgs p) {
           if (!visit_inner<TRAV, COUNT, FILTER, STACK>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally, top_smem,
                                                 top_base))
             fin = true;
+#if defined(FK_INNER_VISITS) && FK_INNER_VISITS > 1
+          // further visits in the same iteration, continuing from the stack
+          for (int v = 1; v < FK_INNER_VISITS && !fin; ++v) {
+            if (st.cur < 0 && st.pend < 0 && !pop<FILTER>(st, stk, fminf(best, p.hi))) {
+              fin = true;
+              break;
+            }
+            if (!(st.cur >= 0 && (st.pend < 0 || (p.speculate && st.sp < STACK - 4)))) break;
+            if (!visit_inner<TRAV, COUNT, FILTER, STACK>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally,
+                                                         top_smem, top_base))
+              fin = true;
+          }
+#endif
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, p.hi));
         if (fin) {
@@ -1418,8 +1409,8 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
             if (!J.s.filter_ok) rp.exact_only = true;
             if (is_ordered(TRAV)) {
               float4 L = __ldg(J.s.node_lo), H = __ldg(J.s.node_hi);
-              float aa = ray_box(o, dir, xyz(L), xyz(H));
-              if (aa < hi) {
+              float aa;
+              if (child_hit<FILTER>(rp, xyz(L), xyz(H), hi, aa)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
                 st.cur = J.s.root_is_leaf ? -1 : 0;
                 st.pend = J.s.root_is_leaf ? 0 : -1;

@@ -88,7 +88,9 @@ def test_meshmap_max_distance_matches_oracle(ctx, oracle, name, cull, max_dist):
     full_t = mm.results()[1][:n]
     hit = ot != api.MISS
     assert (oc[hit, 0] < np.float32(max_dist)).all() and (oc[~hit, 0] == api.FLT_MAX).all()
-    assert hit.sum() < (full_t != api.MISS).sum()
+    assert hit.sum() <= (full_t != api.MISS).sum()
+    if max_dist < 0.05:  # every case has mapping distances beyond 0.02
+        assert hit.sum() < (full_t != api.MISS).sum()
     # a hit under the limit is the unlimited walk's hit (grazing hits on box faces aside)
     assert (ot[hit] == full_t[hit]).mean() >= 0.999
 
