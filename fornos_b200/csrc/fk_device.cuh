@@ -118,23 +118,23 @@ __device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr
 // Conservative form for boxes that only prune (inner nodes): false only when
 // ray_box(o, d, lo, hi) < thr certainly fails, true when it holds or is
 // uncertain.  An infinite entry or a minus-infinite exit is a certain miss of
-// the exact test as well.  `entry` is the filtered entry distance.
+// the exact test as well.  `entry` is the filtered entry distance.  For the
+// rare ray whose direction has a component in (0, 2^-100) (exact_only) every
+// box is accepted, with entry -FLT_MAX so that deferred culling keeps it: the
+// leaf boxes are still tested exactly, so results are unchanged, and the test
+// stays free of branches.
 __device__ __forceinline__ bool box_maybe(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
-  if (r.exact_only) {
-    entry = ray_box(r.o, r.d, lo, hi);
-    return entry < thr;
-  }
   f3 n1 = sub(lo, r.o), n2 = sub(hi, r.o);
   f3 t1 = mk3(__fmul_rn(n1.x, r.inv.x), __fmul_rn(n1.y, r.inv.y), __fmul_rn(n1.z, r.inv.z));
   f3 t2 = mk3(__fmul_rn(n2.x, r.inv.x), __fmul_rn(n2.y, r.inv.y), __fmul_rn(n2.z, r.inv.z));
   f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
   float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
   float b = fminf(tx.x, fminf(tx.y, tx.z));
-  entry = a;
   const float inf = __int_as_float(0x7f800000);
-  if (!(a < inf) || !(b > -inf)) return false;
   const float a_lo = below(a), b_hi = above(b);
-  return !(b_hi < 0.0f || a_lo > b_hi || a_lo >= thr);
+  const bool reject = !(a < inf) || !(b > -inf) || b_hi < 0.0f || a_lo > b_hi || a_lo >= thr;
+  entry = r.exact_only ? -FLT_MAX : a;
+  return r.exact_only || !reject;
 }
 
 // Binary64 barycentric of Shaders/meshmapping_nobackfaces.comp:48-62.

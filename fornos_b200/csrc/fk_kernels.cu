@@ -585,33 +585,20 @@ __device__ __forceinline__ bool push(int2* stk, int& sp, int32_t ref, float dist
   return true;
 }
 
-// A child that passed its box test: the first leaf becomes the postponed
-// leaf, the first inner record the next one to visit, the rest are deferred.
-template <int STACK = kStack>
-__device__ __forceinline__ bool place(OState& st, int32_t& next, int2* stk, int32_t ref, float dist, int* status) {
-  if (ref < 0) {
-    if (st.pend < 0) {
-      st.pend = -ref - 1;
-      st.pend_dist = dist;
-      return true;
-    }
-    return push<STACK>(stk, st.sp, ref, dist, status);
-  }
-  if (next < 0) {
-    next = ref;
-    return true;
-  }
-  return push<STACK>(stk, st.sp, ref, dist, status);
-}
-
 // Inner phase: tests both children of record `cur` against `thr` and takes
-// them nearer entry first (straight-line selects: no per-lane arrays).
-template <bool COUNT, bool FILTER, int STACK = kStack>
+// them nearer entry first.  Their roles are decided by selects, in the order
+// near child, far child: the first leaf becomes the postponed leaf when none
+// is held, the first inner record the next one to visit, and the rest are
+// deferred by predicated stores (near first, so the far one is popped first),
+// with one overflow check per visit.  Straight-line code keeps the visit free
+// of divergent branches.  TOP: records ref >= top_base are read from the
+// staged copies in shared memory.
+template <bool COUNT, bool FILTER, int STACK = kStack, bool TOP = false>
 __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
                                             int* status, Tally& tally, const float4* top = nullptr,
                                             uint32_t top_base = 0xFFFFFFFFu) {
   float4 w0, w1, w2, w3;
-  if ((uint32_t)st.cur >= top_base) {  // staged in shared memory
+  if (TOP && (uint32_t)st.cur >= top_base) {
     const float4* w = top + 4 * ((uint32_t)st.cur - top_base);
     w0 = w[0], w1 = w[1], w2 = w[2], w3 = w[3];
   } else {
@@ -621,55 +608,6 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   float d0, d1;
   const bool h0 = child_maybe<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
   const bool h1 = child_maybe<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
-  if (COUNT) tally.box += 2;
-  const bool swap = d1 < d0;
-  const bool hn = swap ? h1 : h0, hf = swap ? h0 : h1;
-  const float dn = swap ? d1 : d0, df = swap ? d0 : d1;
-  const int32_t rn = __float_as_int(swap ? w3.y : w3.x), rf = __float_as_int(swap ? w3.x : w3.y);
-  int32_t next = -1;
-  if (hn && !place<STACK>(st, next, stk, rn, dn, status)) return false;
-  if (hf && !place<STACK>(st, next, stk, rf, df, status)) return false;
-  st.cur = next;
-  return true;
-}
-
-#ifdef FK_EXP_LEAN
-// Inner-phase box test without the exact-only branch: for the rare ray with a
-// direction component in (0, 2^-100) every inner box is accepted (inner boxes
-// only prune; the leaf boxes are still tested exactly), with an entry of
-// -FLT_MAX so deferred culling keeps it.
-__device__ __forceinline__ bool box_maybe_lean(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
-  f3 n1 = sub(lo, r.o), n2 = sub(hi, r.o);
-  f3 t1 = mk3(__fmul_rn(n1.x, r.inv.x), __fmul_rn(n1.y, r.inv.y), __fmul_rn(n1.z, r.inv.z));
-  f3 t2 = mk3(__fmul_rn(n2.x, r.inv.x), __fmul_rn(n2.y, r.inv.y), __fmul_rn(n2.z, r.inv.z));
-  f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
-  float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
-  float b = fminf(tx.x, fminf(tx.y, tx.z));
-  const float inf = __int_as_float(0x7f800000);
-  const float a_lo = below(a), b_hi = above(b);
-  const bool reject = !(a < inf) || !(b > -inf) || b_hi < 0.0f || a_lo > b_hi || a_lo >= thr;
-  entry = r.exact_only ? -FLT_MAX : a;
-  return r.exact_only || !reject;
-}
-
-// Inner visit with straight-line placement: both children's roles (postponed
-// leaf, next record, deferred entries near first) are decided by selects and
-// the deferred entries written by predicated stores; one overflow check per
-// visit.  Same visit order and stack contents as inner_visit.
-template <bool COUNT, bool FILTER, int STACK = kStack>
-__device__ __forceinline__ bool inner_visit_lean(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
-                                                 int* status, Tally& tally) {
-  const float4* w = s.wide + 4 * (size_t)st.cur;
-  const float4 w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
-  float d0, d1;
-  bool h0, h1;
-  if (FILTER) {
-    h0 = box_maybe_lean(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
-    h1 = box_maybe_lean(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
-  } else {
-    h0 = child_maybe<false>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
-    h1 = child_maybe<false>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
-  }
   if (COUNT) tally.box += 2;
   const bool swap = d1 < d0;
   const bool hn = swap ? h1 : h0, hf = swap ? h0 : h1;
@@ -694,7 +632,6 @@ __device__ __forceinline__ bool inner_visit_lean(const SceneDev& s, const RayPre
   }
   return true;
 }
-#endif
 
 // Compare-exchange of (key, ref) pairs: ascending keys.
 __device__ __forceinline__ void cex(float& ka, int32_t& ra, float& kb, int32_t& rb) {
@@ -756,16 +693,12 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   return true;
 }
 
-template <int TRAV, bool COUNT, bool FILTER, int STACK = kStack>
+template <int TRAV, bool COUNT, bool FILTER, int STACK = kStack, bool TOP = false>
 __device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
                                             int* status, Tally& tally, const float4* top = nullptr,
                                             uint32_t top_base = 0xFFFFFFFFu) {
   if (TRAV == FK_TRAVERSE_ORDERED4) return inner_visit4<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally);
-#ifdef FK_EXP_LEAN
-  return inner_visit_lean<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally);
-#else
-  return inner_visit<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally, top, top_base);
-#endif
+  return inner_visit<COUNT, FILTER, STACK, TOP>(s, rp, thr, st, stk, status, tally, top, top_base);
 }
 
 // Order-preserving key of a non-negative distance (total order, -0 below +0)
@@ -891,14 +824,21 @@ __device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, f
   return i >= s.node_count;
 }
 
+// Inner visits a lane makes per iteration of the trace loop before the warp
+// decides its next phase again (the phase ballots and the refill check are
+// paid once per kInnerVisits visits).
+#ifndef FK_INNER_VISITS
+#define FK_INNER_VISITS 2
+#endif
+constexpr int kInnerVisits = FK_INNER_VISITS;
+
 // BLOCK: threads per block; STACK: deferred entries per lane (the ordered
 // traversals accept trees of depth below STACK, the 4-wide one of depth up
-// to (STACK - 1) / 3).
-#ifndef FK_EXP_MINB
-#define FK_EXP_MINB 1
-#endif
-template <int KIND, int TRAV, bool COUNT, bool FILTER, int BLOCK = 256, int STACK = kStack>
-__global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? FK_EXP_MINB : 1) hemi_trace_kernel(DynArgs p) {
+// to (STACK - 1) / 3); TOP: staged top records in shared memory (the 2-wide
+// ordered traversal).  The launch bounds ask for 40 resident warps per SM
+// (at most 51 registers a thread at 256 threads).
+template <int KIND, int TRAV, bool COUNT, bool FILTER, int BLOCK = 256, int STACK = kStack, bool TOP = false>
+__global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_trace_kernel(DynArgs p) {
   constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
@@ -906,12 +846,12 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? FK_EXP_MINB : 1) hemi_tr
   int2 stk[is_ordered(TRAV) ? STACK : 1];  // deferred (ref, entry) pairs
   __shared__ uint32_t leaf_keys[BLOCK / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
-  extern __shared__ float4 top_smem[];  // p.top_count staged records (TRAV == ORDERED)
-  if (TRAV == FK_TRAVERSE_ORDERED && p.top_count) {
+  extern __shared__ float4 top_smem[];  // p.top_count staged records (TOP)
+  if (TOP) {
     for (uint32_t i = threadIdx.x; i < 4 * p.top_count; i += blockDim.x) top_smem[i] = __ldg(p.top + i);
     __syncthreads();
   }
-  const uint32_t top_base = TRAV == FK_TRAVERSE_ORDERED && p.top_count ? p.top_base : 0xFFFFFFFFu;
+  const uint32_t top_base = TOP ? p.top_base : 0xFFFFFFFFu;
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t slot = 0;  // scratch slot of the lane's ray: its texel's row, its sample
@@ -957,7 +897,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? FK_EXP_MINB : 1) hemi_tr
               if (COUNT) tally.box++;
               if (child_hit<FILTER>(rp, xyz(L), xyz(H), p.hi, a)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
-                st.cur = p.s.root_is_leaf ? -1 : (top_base != 0xFFFFFFFFu ? (int32_t)top_base : 0);
+                st.cur = p.s.root_is_leaf ? -1 : (TOP ? (int32_t)top_base : 0);
                 st.pend = p.s.root_is_leaf ? 0 : -1;
                 st.pend_dist = a;
                 done = false;
@@ -997,22 +937,20 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? FK_EXP_MINB : 1) hemi_tr
         if (leaf_phase) {
           if (visited) fin = settled<STOP>(best, p.hi);
         } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
-          if (!visit_inner<TRAV, COUNT, FILTER, STACK>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally, top_smem,
-                                                top_base))
+          if (!visit_inner<TRAV, COUNT, FILTER, STACK, TOP>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally,
+                                                             top_smem, top_base))
             fin = true;
-#if defined(FK_INNER_VISITS) && FK_INNER_VISITS > 1
           // further visits in the same iteration, continuing from the stack
-          for (int v = 1; v < FK_INNER_VISITS && !fin; ++v) {
+          for (int v = 1; v < kInnerVisits && !fin; ++v) {
             if (st.cur < 0 && st.pend < 0 && !pop<FILTER>(st, stk, fminf(best, p.hi))) {
               fin = true;
               break;
             }
             if (!(st.cur >= 0 && (st.pend < 0 || (p.speculate && st.sp < STACK - 4)))) break;
-            if (!visit_inner<TRAV, COUNT, FILTER, STACK>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally,
-                                                         top_smem, top_base))
+            if (!visit_inner<TRAV, COUNT, FILTER, STACK, TOP>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally,
+                                                               top_smem, top_base))
               fin = true;
           }
-#endif
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, p.hi));
         if (fin) {
@@ -1223,9 +1161,10 @@ __global__ void __launch_bounds__(256) hemi_reduce_kernel(HemiArgs p, const floa
 // threads and a 64-entry stack; the production variant (filtered box tests)
 // of the 2-wide ordered traversal in every block shape and stack depth.
 template <int KIND, int TRAV>
-static void (*pick_trace(bool count, bool filter, uint32_t block, uint32_t stack))(DynArgs) {
+static void (*pick_trace(bool count, bool filter, uint32_t block, uint32_t stack, bool top))(DynArgs) {
   if (count) return filter ? hemi_trace_kernel<KIND, TRAV, true, true> : hemi_trace_kernel<KIND, TRAV, true, false>;
   if (!filter) return hemi_trace_kernel<KIND, TRAV, false, false>;
+  if (TRAV == FK_TRAVERSE_ORDERED && top) return hemi_trace_kernel<KIND, TRAV, false, true, 256, kStack, true>;
   if (TRAV == FK_TRAVERSE_ORDERED) {
     if (stack == 32) {
       if (block == 128) return hemi_trace_kernel<KIND, TRAV, false, true, 128, 32>;
@@ -1240,11 +1179,11 @@ static void (*pick_trace(bool count, bool filter, uint32_t block, uint32_t stack
 
 // Block shape and stack depth a launch uses: the tuning's where the
 // production variant applies and the tree fits the stack, else 256 / 64.
-static void trace_shape(const fk_tuning& t, const HemiArgs& a, int trav, bool filter, uint32_t odepth,
+static void trace_shape(const fk_tuning& t, const HemiArgs& a, int trav, bool filter, uint32_t odepth, bool top,
                         uint32_t* block, uint32_t* stack) {
   *block = 256;
   *stack = kStack;
-  if (a.tally || !filter || trav != FK_TRAVERSE_ORDERED) return;
+  if (a.tally || !filter || trav != FK_TRAVERSE_ORDERED || top) return;
   *block = t.block_threads;
   if (t.stack_depth == 32 && odepth <= 24) *stack = 32;
 }
@@ -1253,8 +1192,8 @@ template <int KIND, int TRAV>
 static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, bool filter, uint32_t leaf_batch,
                             uint32_t speculate, const TraceExtras& x) {
   uint32_t block = 256, stack = kStack;
-  trace_shape(ctx->tuning, a, TRAV, filter, x.odepth, &block, &stack);
-  auto trace = pick_trace<KIND, TRAV>(a.tally != nullptr, filter, block, stack);
+  trace_shape(ctx->tuning, a, TRAV, filter, x.odepth, x.top_count > 0, &block, &stack);
+  auto trace = pick_trace<KIND, TRAV>(a.tally != nullptr, filter, block, stack, x.top_count > 0);
   const size_t smem = 64 * (size_t)x.top_count;
   if (smem > 48 * 1024) {
     cudaError_t e = cudaFuncSetAttribute(trace, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -1446,6 +1385,14 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
         } else if (st.cur >= 0 && st.pend < 0) {
           if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally))
             fin = true;
+          for (int v = 1; v < kInnerVisits && !fin; ++v) {  // as in hemi_trace_kernel
+            if (st.cur < 0 && st.pend < 0 && !pop<FILTER>(st, stk, fminf(best, hi))) {
+              fin = true;
+              break;
+            }
+            if (!(st.cur >= 0 && st.pend < 0)) break;
+            if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally)) fin = true;
+          }
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, hi));
         if (fin) {
