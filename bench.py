@@ -84,6 +84,15 @@ def rays_per_texel(wl):
     return 2 + spp * sum(k in wl["bakers"] for k in ("ao", "bn", "thick"))
 
 
+def parse_tuning(text):
+    """'refill=8,top_records=64' -> fk_tuning fields (fk_ctx_set_tuning)."""
+    out = {}
+    for item in filter(None, text.split(",")):
+        k, v = item.split("=")
+        out[k.strip()] = int(v)
+    return out
+
+
 def traversals_per_texel(wl):
     """Rays actually traced per texel: AO and bent normals share one traversal."""
     b = wl["bakers"]
@@ -273,6 +282,8 @@ def run_fornos(args, wl, rank, world):
     stream = torch.cuda.Stream()
     ctx = api.Context(dev)
     ctx.set_stream(stream.cuda_stream)
+    if args.tuning:
+        ctx.set_tuning(**parse_tuning(args.tuning))
     trav = TRAVERSE[args.traverse] | SCHEDULE[args.schedule]
     prep = Prepared(wl, replica_seed(args.seed, rank))
     tex, spp, lo_d, hi_d = wl["tex"], wl["spp"], wl["min_d"], wl["max_d"]
@@ -437,6 +448,7 @@ def run_fornos(args, wl, rank, world):
         "config": {"workload": args.workload, "desc": wl["desc"], "texels": n, "texture": tex, "spp": spp,
                    "high_poly_triangles": prep.triangles, "bvh_nodes": info["node_count"],
                    "bvh_depth": info["depth"], "traverse": args.traverse, "schedule": args.schedule, "tree": args.tree,
+                   "tuning": ctx.get_tuning(),
                    "rays_per_texel": rays_per_texel(wl), "traversals_per_texel": traversals_per_texel(wl),
                    "rays_counted": "2 mapping + spp each for AO, bent normals, thickness, as the reference traces "
                                    "them; AO and bent normals share one traversal here, so the rays traced are "
@@ -1008,6 +1020,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-denoise", action="store_true", help="skip the denoised-vs-plain comparison")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-bake comparison of the default line")
+    ap.add_argument("--tuning", default="",
+                    help="fk_tuning knobs for the bake, e.g. refill=8,top_records=64 (default: the context's)")
     ap.add_argument("--side", default="sphere512",
                     help="other workloads measured in the default line (comma-separated; empty: none)")
     ap.add_argument("--line-batch-jobs", type=int, default=16,

@@ -67,6 +67,7 @@ static int batch_run_chunks(fk_batch* b, int trav, bool filter, const fk_tuning&
     a.refill = tun.refill;
     a.leaf_batch = tun.leaf_batch;
     a.ray_order = tun.ray_order;
+    a.speculate = tun.speculate;
     cudaError_t e = fk::launch_batch(a, b->kind, trav, filter, ctx->stream, ctx->sm_count, true);
     if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "batch launch");
     ctx->launches += 2;
@@ -99,6 +100,7 @@ static int batch_time(fk_batch* b, unsigned long long stride, int trav, bool fil
   a.refill = tun.refill;
   a.leaf_batch = tun.leaf_batch;
   a.ray_order = FK_RAY_ORDER_SAMPLE;  // calibration samples every stride-th ray
+  a.speculate = tun.speculate;
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -242,15 +244,28 @@ int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int
   };
   std::vector<Cand> cands;
   const bool ordered_ok = b->ordered_ok;
-  for (uint32_t refill : {4u, 8u, 16u}) {
+  const fk_tuning ct = ctx->tuning;  // the context's ray order, block and stack carry over
+  auto knobs = [&](uint32_t refill, uint32_t lb, uint32_t spec) {
+    fk_tuning t = ct;
+    t.refill = refill;
+    t.leaf_batch = lb;
+    t.speculate = spec;
+    t.top_records = 0;
+    t.l2_persist = FK_L2_NONE;
+    return t;
+  };
+  for (uint32_t refill : {8u, 16u, 24u}) {
     if (ordered_ok)
-      for (uint32_t lb : {1u, 4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED, true, {refill, lb, 0, 0, 0, FK_L2_NONE, 256, 64}});
+      for (uint32_t lb : {4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED, true, knobs(refill, lb, 1)});
     if (b->ordered4_ok)
-      for (uint32_t lb : {4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED4, true, {refill, lb, 0, 0, 0, FK_L2_NONE, 256, 64}});
-    cands.push_back({FK_TRAVERSE_SKIP, true, {refill, 8, 0, 0, 0, FK_L2_NONE, 256, 64}});
+      for (uint32_t lb : {4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED4, true, knobs(refill, lb, 1)});
+    cands.push_back({FK_TRAVERSE_SKIP, true, knobs(refill, 8, 0)});
   }
-  if (ordered_ok) cands.push_back({FK_TRAVERSE_ORDERED, false, {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64}});
-  cands.push_back({FK_TRAVERSE_SKIP, false, {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64}});
+  if (ordered_ok) {
+    cands.push_back({FK_TRAVERSE_ORDERED, true, knobs(16, 8, 0)});
+    cands.push_back({FK_TRAVERSE_ORDERED, false, knobs(16, 8, 1)});
+  }
+  cands.push_back({FK_TRAVERSE_SKIP, false, knobs(16, 8, 0)});
   float best_ms = 1e30f;
   Cand best = cands[0];
   float warm = 0.0f;
@@ -265,7 +280,6 @@ int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int
     }
   }
   if (rc != FK_OK) return rc;
-  best.t.ray_order = ctx->tuning.ray_order;  // strided calibration cannot see the ray order: the context's
   b->traverse = best.trav;
   b->filter = best.filter;
   b->tuning = best.t;

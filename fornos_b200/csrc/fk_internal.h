@@ -213,6 +213,7 @@ struct BatchArgs {
   int* status;
   uint32_t refill, leaf_batch;
   uint32_t ray_order;  // FK_RAY_ORDER_*, per job (stride 1 only)
+  uint32_t speculate;  // lanes holding a leaf keep visiting inner records
 };
 cudaError_t launch_batch(const BatchArgs& a, int kind, int trav, bool filter, cudaStream_t stream, int sm_count,
                          bool reduce);

@@ -1278,7 +1278,7 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
 // that job's scene in place.  `stride` > 1 traces every stride-th ray only
 // (the autotuner's calibration sample).
 template <int KIND, int TRAV, bool FILTER>
-__global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
+__global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
   constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
   __shared__ BatchJobDev jobs[kMaxBatchJobs];
   for (uint32_t i = threadIdx.x; i < p.njobs * (uint32_t)(sizeof(BatchJobDev) / 4); i += blockDim.x)
@@ -1300,9 +1300,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
   int32_t cur = 0;
   uint32_t end = 0;  // skip walk: one past the job's last node
   OState st = {-1, -1, 0.0f, 0};
-  // the lane's job scene, copied from the table when the lane starts a ray so
-  // that node visits read its arrays' addresses from registers
-  SceneDev sc = {};
+  uint32_t job = 0;  // the lane's job: its scene's arrays are read from the table in shared memory
   for (;;) {
     unsigned idle = __ballot_sync(full, !active);
     if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
@@ -1322,7 +1320,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
             if (jobs[m].ray_base <= r) a = m; else b = m - 1;
           }
           const BatchJobDev& J = jobs[a];
-          sc = J.s;
+          job = (uint32_t)a;
           const unsigned long long local = r - J.ray_base;
           const uint32_t g = (uint32_t)(local / J.spp);
           uint32_t k = (uint32_t)(local % J.spp);
@@ -1371,8 +1369,9 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
       idle = __ballot_sync(full, !active);
     }
     if (exhausted && idle == full) break;
-    const SceneDev& s = sc;
+    const SceneDev& s = jobs[job].s;
     if (is_ordered(TRAV)) {
+      const bool spec_ok = st.sp < kStack - 4;
       const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
       const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
@@ -1382,7 +1381,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
         bool fin = false;
         if (leaf_phase) {
           if (visited) fin = settled<STOP>(best, hi);
-        } else if (st.cur >= 0 && st.pend < 0) {
+        } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
           if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally))
             fin = true;
           for (int v = 1; v < kInnerVisits && !fin; ++v) {  // as in hemi_trace_kernel
@@ -1390,7 +1389,7 @@ __global__ void __launch_bounds__(256) batch_trace_kernel(BatchArgs p) {
               fin = true;
               break;
             }
-            if (!(st.cur >= 0 && st.pend < 0)) break;
+            if (!(st.cur >= 0 && (st.pend < 0 || (p.speculate && st.sp < kStack - 4)))) break;
             if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally)) fin = true;
           }
         }

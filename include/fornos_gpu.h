@@ -443,10 +443,10 @@ int fk_batch_info(const fk_batch* batch, uint64_t* rays, uint32_t* texels, uint3
 /* Autotuner: times a strided sample of about sample_rays rays of every job
  * (0 = 4M) under each candidate schedule (ordered over the 2-wide or the
  * collapsed 4-wide layout vs the skip-pointer walk, filtered vs divided box
- * tests, refill threshold, postponed-leaf batch) and keeps the fastest for
- * later runs; reports it.  The ray order is the context's (a strided sample
- * has no per-texel order to time); the batch kernel runs 256-thread blocks
- * with 64-entry stacks. */
+ * tests, refill threshold, postponed-leaf batch, speculation) and keeps the
+ * fastest for later runs; reports it.  The ray order is the context's (a
+ * strided sample has no per-texel order to time); the batch kernel runs
+ * 256-thread blocks with 64-entry stacks. */
 int fk_batch_tune(fk_batch* batch, uint64_t sample_rays, fk_tuning* best_tuning, int* best_traverse);
 /* One run on the context's stream; traverse 0 = the tuned schedule. */
 int fk_batch_run(fk_batch* batch, int traverse);
