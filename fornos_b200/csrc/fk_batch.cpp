@@ -42,6 +42,9 @@ struct fk_batch {
   bool ordered4_ok = true;                // every collapsed tree fits the 4-wide traversal's stack
   bool filter = true;
   fk_tuning tuning = {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64};
+  // the jobs' scenes laid end to end (fk::BatchArgs::cat) and its allocations
+  fk::SceneDev cat = {};
+  void* cat_mem[7] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -54,6 +57,7 @@ static int batch_run_chunks(fk_batch* b, int trav, bool filter, const fk_tuning&
     const Chunk& ch = b->chunks[c];
     FK_CUDA(ctx, cudaMemsetAsync(b->queues + c, 0, sizeof(unsigned long long), ctx->stream));
     fk::BatchArgs a;
+    a.cat = b->cat;
     a.jobs = b->jobs;
     a.njobs = b->njobs;
     a.r0 = ch.r0;
@@ -88,6 +92,7 @@ static int batch_time(fk_batch* b, unsigned long long stride, int trav, bool fil
   fk_ctx* ctx = b->ctx;
   unsigned long long* q = b->queues + b->chunks.size();
   fk::BatchArgs a;
+  a.cat = b->cat;
   a.jobs = b->jobs;
   a.njobs = b->njobs;
   a.r0 = 0;
@@ -132,7 +137,7 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   if (kind < FK_AO || kind > FK_AO_BN) return fk_fail(ctx, FK_ERR_INVALID, "fk_batch_create: unknown kind");
   std::vector<fk::BatchJobDev> table(njobs);
   unsigned long long rays = 0;
-  uint64_t texels = 0;
+  uint64_t texels = 0, nodes = 0, corners = 0, recs2 = 0, recs4 = 0;
   for (uint32_t i = 0; i < njobs; ++i) {
     const fk_batch_job& J = jobs[i];
     const uint64_t n = J.texel_count;
@@ -168,6 +173,16 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
     d.perms = J.params.perm_count;
     d.lo = J.params.min_distance;
     d.hi = J.params.max_distance;
+    d.node_base = (uint32_t)nodes;
+    d.corner_base = (uint32_t)corners;
+    d.root2 = J.scene->wide_count ? (int32_t)recs2 : -1;
+    d.root4 = J.scene->wide4_count ? (int32_t)recs4 : -1;
+    nodes += J.scene->node_count;
+    corners += J.scene->corner_count;
+    recs2 += J.scene->wide_count;
+    recs4 += J.scene->wide4_count;
+    if (nodes > 0x7FFFFFFFull || corners > 0xFFFFFFFFull || recs2 > 0x7FFFFFFFull || recs4 > 0x7FFFFFFFull)
+      return fk_fail(ctx, FK_ERR_INVALID, "fk_batch_create: the jobs' scenes exceed 2^31 nodes or records");
     rays += n * J.params.sample_count;
     texels += n;
     if (texels > 0xFFFFFFFFull) return fk_fail(ctx, FK_ERR_INVALID, "fk_batch_create: more than 2^32 texels");
@@ -200,6 +215,28 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   if (cur.t1 > cur.t0) b->chunks.push_back(cur);
   b->scratch_rays = std::min<unsigned long long>(std::max<unsigned long long>(rays, 1), kMaxChunkRays);
   int rc = fk_dev_alloc(ctx, (void**)&b->jobs, sizeof(fk::BatchJobDev) * njobs);
+  // the concatenated scene: nodes (lo, hi, jump), corners (positions, normals), triangle records, both layouts
+  const size_t cat_bytes[7] = {16 * (size_t)nodes, 16 * (size_t)nodes, 4 * (size_t)nodes, 16 * (size_t)corners,
+                               16 * (size_t)corners, 64 * (size_t)(corners / 3), 64 * (size_t)recs2};
+  for (int k = 0; k < 7 && rc == FK_OK; ++k) rc = fk_dev_alloc(ctx, &b->cat_mem[k], std::max<size_t>(cat_bytes[k], 16));
+  if (rc == FK_OK && recs4) rc = fk_dev_alloc(ctx, (void**)&b->cat.wide4, 128 * (size_t)recs4);
+  if (rc == FK_OK) {
+    b->cat.node_lo = (const float4*)b->cat_mem[0];
+    b->cat.node_hi = (const float4*)b->cat_mem[1];
+    b->cat.node_jump = (const uint32_t*)b->cat_mem[2];
+    b->cat.pos4 = (const float4*)b->cat_mem[3];
+    b->cat.nrm4 = (const float4*)b->cat_mem[4];
+    b->cat.rec = (const float4*)b->cat_mem[5];
+    b->cat.wide = (const float4*)b->cat_mem[6];
+    b->cat.node_count = (uint32_t)nodes;
+    b->cat.corner_count = (uint32_t)corners;
+    b->cat.filter_ok = 1;
+    for (uint32_t i = 0; i < njobs && rc == FK_OK; ++i)
+      if (fk::concat_batch_scene(ctx->stream, jobs[i].scene, table[i].node_base, table[i].corner_base,
+                                 table[i].root2 < 0 ? 0 : (uint32_t)table[i].root2,
+                                 table[i].root4 < 0 ? 0 : (uint32_t)table[i].root4, b->cat) != FK_OK)
+        rc = fk_fail(ctx, FK_ERR_CUDA, "fk_batch_create: scene concatenation");
+  }
   if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->queues, sizeof(unsigned long long) * (b->chunks.size() + 1));
   if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->scratch, sizeof(float) * b->scratch_rays);
   if (rc == FK_OK) {
@@ -340,6 +377,8 @@ int fk_batch_free(fk_batch* b) {
   fk_dev_free(b->ctx, b->jobs);
   fk_dev_free(b->ctx, b->queues);
   fk_dev_free(b->ctx, b->scratch);
+  for (void* p : b->cat_mem) fk_dev_free(b->ctx, p);
+  fk_dev_free(b->ctx, const_cast<float4*>(b->cat.wide4));
   delete b;
   return FK_OK;
 }

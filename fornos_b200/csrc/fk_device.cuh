@@ -117,11 +117,14 @@ __device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr
 
 // Conservative form for boxes that only prune (inner nodes): false only when
 // ray_box(o, d, lo, hi) < thr certainly fails, true when it holds or is
-// uncertain.  An infinite entry or a minus-infinite exit is a certain miss of
-// the exact test as well.  `entry` is the filtered entry distance.  For the
-// rare ray whose direction has a component in (0, 2^-100) (exact_only) every
-// box is accepted, with entry -FLT_MAX so that deferred culling keeps it: the
-// leaf boxes are still tested exactly, so results are unchanged, and the test
+// uncertain.  `entry` is the filtered entry distance.  An infinite entry or a
+// minus-infinite exit (a direction component of exactly 0 with the origin
+// outside that slab) is a certain miss of the exact test as well; rejecting it
+// here matters for speed, since its margins are NaN and the box would
+// otherwise be accepted, and with it every box below.  For the rare ray whose
+// direction has a component in (0, 2^-100) (exact_only) every box is
+// accepted, with entry -FLT_MAX so that deferred culling keeps it: its leaf
+// boxes are still tested exactly, so results are unchanged, and the test
 // stays free of branches.
 __device__ __forceinline__ bool box_maybe(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
   f3 n1 = sub(lo, r.o), n2 = sub(hi, r.o);

@@ -200,9 +200,17 @@ struct BatchJobDev {
   uint32_t texel_base;          // first texel of the job in the batch's texel space
   uint32_t texels, spp, perms;
   float lo, hi;
+  // the job's place in the batch's concatenated scene arrays (BatchArgs::cat)
+  uint32_t node_base, corner_base;  // flattened nodes; corners (a multiple of 3)
+  int32_t root2, root4;             // root records of the 2-wide and 4-wide layouts
   uint32_t pad[2];
 };
 struct BatchArgs {
+  // Every job's scene laid end to end: node, corner and triangle-record
+  // arrays, and both inner layouts, with the jobs' child refs, leaf refs,
+  // triangle ranges and skip pointers offset to the concatenated arrays, so a
+  // traversal needs no per-job pointers.
+  SceneDev cat;
   const BatchJobDev* jobs;
   uint32_t njobs;
   unsigned long long r0, r1;  // rays of this launch
@@ -217,6 +225,10 @@ struct BatchArgs {
 };
 cudaError_t launch_batch(const BatchArgs& a, int kind, int trav, bool filter, cudaStream_t stream, int sm_count,
                          bool reduce);
+// Copies scene `s` into the concatenated arrays of `cat` at the given bases
+// (nodes, corners, 2-wide and 4-wide records), offsetting its refs.
+int concat_batch_scene(cudaStream_t st, const fk_scene* s, uint32_t node_base, uint32_t corner_base, uint32_t rec2,
+                       uint32_t rec4, const SceneDev& cat);
 int launch_meshmap(fk_ctx* ctx, const fk_scene* s, const fk_texel_map* m, int cull, float max_d, uint32_t offset,
                    uint32_t count, float4* coords, uint32_t* tidx);
 struct HemiLaunch {

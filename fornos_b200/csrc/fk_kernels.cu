@@ -574,16 +574,6 @@ struct OState {
 
 // Deferred entries are (ref, entry distance bits) pairs: one 8-byte access
 // per push or pop.
-template <int STACK = kStack>
-__device__ __forceinline__ bool push(int2* stk, int& sp, int32_t ref, float dist, int* status) {
-  if (sp >= STACK) {
-    atomicOr(status, 1);
-    return false;
-  }
-  stk[sp] = make_int2(ref, __float_as_int(dist));
-  ++sp;
-  return true;
-}
 
 // Inner phase: tests both children of record `cur` against `thr` and takes
 // them nearer entry first.  Their roles are decided by selects, in the order
@@ -680,16 +670,26 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   const int ni = n0 ? 0 : (n1 ? 1 : (n2 ? 2 : (n3 ? 3 : 4)));
   const int nl = (l0 ? 0 : (l1 ? 1 : (l2 ? 2 : (l3 ? 3 : 4))));
   const int keep = st.pend < 0 ? nl : 4;  // the leaf that becomes the postponed leaf, if any
-  if (v3 && ni != 3 && keep != 3 && !push<STACK>(stk, st.sp, r3, k3, status)) return false;
-  if (v2 && ni != 2 && keep != 2 && !push<STACK>(stk, st.sp, r2, k2, status)) return false;
-  if (v1 && ni != 1 && keep != 1 && !push<STACK>(stk, st.sp, r1, k1, status)) return false;
-  if (v0 && ni != 0 && keep != 0 && !push<STACK>(stk, st.sp, r0, k0, status)) return false;
-  if (keep < 4) {
-    const int32_t r = keep == 0 ? r0 : (keep == 1 ? r1 : (keep == 2 ? r2 : r3));
-    st.pend = -r - 1;
-    st.pend_dist = keep == 0 ? k0 : (keep == 1 ? k1 : (keep == 2 ? k2 : k3));
-  }
+  // deferred entries farthest first, by predicated stores; one overflow check
+  const bool p3 = v3 && ni != 3 && keep != 3, p2 = v2 && ni != 2 && keep != 2;
+  const bool p1 = v1 && ni != 1 && keep != 1, p0 = v0 && ni != 0 && keep != 0;
+  int sp = st.sp;
+  if (p3 && sp < STACK) stk[sp] = make_int2(r3, __float_as_int(k3));
+  sp += p3;
+  if (p2 && sp < STACK) stk[sp] = make_int2(r2, __float_as_int(k2));
+  sp += p2;
+  if (p1 && sp < STACK) stk[sp] = make_int2(r1, __float_as_int(k1));
+  sp += p1;
+  if (p0 && sp < STACK) stk[sp] = make_int2(r0, __float_as_int(k0));
+  sp += p0;
+  st.sp = sp;
+  const int32_t rk = keep == 0 ? r0 : (keep == 1 ? r1 : (keep == 2 ? r2 : r3));
+  st.pend = keep < 4 ? -rk - 1 : st.pend;
   st.cur = ni == 0 ? r0 : (ni == 1 ? r1 : (ni == 2 ? r2 : (ni == 3 ? r3 : -1)));
+  if (sp > STACK) {
+    atomicOr(status, 1);
+    return false;
+  }
   return true;
 }
 
@@ -721,9 +721,9 @@ __device__ __forceinline__ float dist_unkey(uint32_t k) {
 // minimum over the hits in [lo, best), so neither the order of the tests nor
 // the owner's distance at the start of the phase (which only admits more
 // candidates) changes it.  All lanes of the warp call this; returns whether
-// this lane visited a leaf.  MULTI: lanes may trace different scenes and
-// distance ranges (batched jobs), so the owner's triangle records and minimum
-// distance travel with its ray.
+// this lane visited a leaf.  MULTI: lanes may trace different jobs of a
+// batch, whose scenes lie in one concatenated array but whose distance
+// ranges differ, so the owner's minimum distance travels with its ray.
 template <bool COUNT, bool FILTER, bool MULTI = false>
 __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
                                                 OState& st, bool active, uint32_t* skey, Tally& tally) {
@@ -767,11 +767,7 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
     const uint32_t tri = __shfl_sync(full, first, o) + (j - __shfl_sync(full, excl, o));
     const float4* rec = s.rec;
     float olo = lo;
-    if (MULTI) {
-      const unsigned long long a = __shfl_sync(full, (unsigned long long)(uintptr_t)s.rec, o);
-      rec = reinterpret_cast<const float4*>((uintptr_t)a);
-      olo = __shfl_sync(full, lo, o);
-    }
+    if (MULTI) olo = __shfl_sync(full, lo, o);
     if (j < total) {
       float b = ob;
       tri_sample(rec, tri, ro, rd, olo, b);
@@ -828,7 +824,7 @@ __device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, f
 // decides its next phase again (the phase ballots and the refill check are
 // paid once per kInnerVisits visits).
 #ifndef FK_INNER_VISITS
-#define FK_INNER_VISITS 2
+#define FK_INNER_VISITS 3
 #endif
 constexpr int kInnerVisits = FK_INNER_VISITS;
 
@@ -1280,10 +1276,20 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
 template <int KIND, int TRAV, bool FILTER>
 __global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
   constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
-  __shared__ BatchJobDev jobs[kMaxBatchJobs];
-  for (uint32_t i = threadIdx.x; i < p.njobs * (uint32_t)(sizeof(BatchJobDev) / 4); i += blockDim.x)
-    ((uint32_t*)jobs)[i] = ((const uint32_t*)p.jobs)[i];
-  __syncthreads();
+  // the job table is read at ray set-up only (through the cache): node visits
+  // need nothing per job, since the scenes are concatenated
+  const BatchJobDev* __restrict__ jobs = p.jobs;
+  // The lane's job: found once for the launch's first ray by binary search,
+  // then advanced, since a lane's rays come from the queue in increasing order
+  // (usually no step, so ray set-up adds no chain of dependent loads).
+  int job = 0;
+  {
+    int b = (int)p.njobs - 1;  // last job whose ray_base <= r0
+    while (job < b) {
+      const int m = (job + b + 1) >> 1;
+      if (jobs[m].ray_base <= p.r0) job = m; else b = m - 1;
+    }
+  }
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
@@ -1300,7 +1306,7 @@ __global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
   int32_t cur = 0;
   uint32_t end = 0;  // skip walk: one past the job's last node
   OState st = {-1, -1, 0.0f, 0};
-  uint32_t job = 0;  // the lane's job: its scene's arrays are read from the table in shared memory
+  const SceneDev& s = p.cat;  // every job's scene, concatenated
   for (;;) {
     unsigned idle = __ballot_sync(full, !active);
     if (!exhausted && (uint32_t)__popc(idle) >= p.refill) {
@@ -1314,13 +1320,8 @@ __global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
         const uint32_t q = base + __popc(idle & lower);
         if (q < total) {
           const unsigned long long r = p.r0 + (unsigned long long)q * p.stride;
-          int a = 0, b = (int)p.njobs - 1;  // last job whose ray_base <= r
-          while (a < b) {
-            int m = (a + b + 1) >> 1;
-            if (jobs[m].ray_base <= r) a = m; else b = m - 1;
-          }
-          const BatchJobDev& J = jobs[a];
-          job = (uint32_t)a;
+          while (job + 1 < (int)p.njobs && jobs[job + 1].ray_base <= r) ++job;
+          const BatchJobDev& J = jobs[job];
           const unsigned long long local = r - J.ray_base;
           const uint32_t g = (uint32_t)(local / J.spp);
           uint32_t k = (uint32_t)(local % J.spp);
@@ -1338,25 +1339,25 @@ __global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
           bool done = true;
           if (id != kMiss && valid_hit(id, J.s.corner_count)) {
             f3 o, d, tx, ty;
-            texel_frame(J.s, __ldg(J.coords + g), id, o, d, tx, ty);
+            texel_frame(s, __ldg(J.coords + g), id + J.corner_base, o, d, tx, ty);
             if (KIND == FK_THICK) d = neg(d);
             float4 rs = __ldg(J.samples + (size_t)(g % J.perms) * J.spp + k);
             f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
             rp = ray_pre(o, dir);
             if (!J.s.filter_ok) rp.exact_only = true;
             if (is_ordered(TRAV)) {
-              float4 L = __ldg(J.s.node_lo), H = __ldg(J.s.node_hi);
+              float4 L = __ldg(s.node_lo + J.node_base), H = __ldg(s.node_hi + J.node_base);
               float aa;
               if (child_hit<FILTER>(rp, xyz(L), xyz(H), hi, aa)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
-                st.cur = J.s.root_is_leaf ? -1 : 0;
-                st.pend = J.s.root_is_leaf ? 0 : -1;
+                st.cur = J.s.root_is_leaf ? -1 : (TRAV == FK_TRAVERSE_ORDERED4 ? J.root4 : J.root2);
+                st.pend = J.s.root_is_leaf ? (int32_t)J.node_base : -1;
                 st.pend_dist = aa;
                 done = false;
               }
             } else {
-              cur = 0;
-              end = J.s.node_count;
+              cur = (int32_t)J.node_base;
+              end = J.node_base + J.s.node_count;
               done = false;
             }
           } else if (id != kMiss) {
@@ -1369,7 +1370,6 @@ __global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
       idle = __ballot_sync(full, !active);
     }
     if (exhausted && idle == full) break;
-    const SceneDev& s = jobs[job].s;
     if (is_ordered(TRAV)) {
       const bool spec_ok = st.sp < kStack - 4;
       const unsigned need = __ballot_sync(full, active && st.cur >= 0 && st.pend < 0);
@@ -1406,6 +1406,82 @@ __global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
       }
     }
   }
+}
+
+// ------------------------------------------------------------------ batch scene concatenation
+// One job's scene copied into the batch's concatenated arrays: triangle ranges
+// (corner indices in the .w bits) and skip pointers offset by the job's corner
+// and node bases, inner-record refs by its record base, leaf refs
+// -(flat + 1) by its node base.
+__device__ __forceinline__ float cat_ref(float r, uint32_t rec_base, uint32_t node_base) {
+  const int32_t v = __float_as_int(r);
+  return __int_as_float(v >= 0 ? v + (int32_t)rec_base : v - (int32_t)node_base);
+}
+
+__global__ void cat_nodes_kernel(const float4* __restrict__ lo, const float4* __restrict__ hi,
+                                 const uint32_t* __restrict__ jump, uint32_t n, uint32_t node_base,
+                                 uint32_t corner_base, float4* clo, float4* chi, uint32_t* cjump) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 L = lo[i], H = hi[i];
+  L.w = __uint_as_float(__float_as_uint(L.w) + corner_base);
+  H.w = __uint_as_float(__float_as_uint(H.w) + corner_base);
+  clo[node_base + i] = L;
+  chi[node_base + i] = H;
+  cjump[node_base + i] = jump[i] + node_base;
+}
+
+// `width` float4 per record; the refs are float4 `ref_at` of a record, its
+// first `refs` components.
+__global__ void cat_records_kernel(const float4* __restrict__ rec, uint32_t n, uint32_t width, uint32_t ref_at,
+                                   uint32_t refs, uint32_t rec_base, uint32_t node_base, float4* crec) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n * width) return;
+  float4 v = rec[i];
+  if (i % width == ref_at) {
+    v.x = cat_ref(v.x, rec_base, node_base);
+    v.y = cat_ref(v.y, rec_base, node_base);
+    if (refs > 2) {
+      v.z = cat_ref(v.z, rec_base, node_base);
+      v.w = cat_ref(v.w, rec_base, node_base);
+    }
+  }
+  crec[(size_t)rec_base * width + i] = v;
+}
+
+int concat_batch_scene(cudaStream_t st, const fk_scene* s, uint32_t node_base, uint32_t corner_base, uint32_t rec2,
+                       uint32_t rec4, const SceneDev& cat) {
+  const uint32_t nn = s->node_count;
+  if (nn) {
+    cat_nodes_kernel<<<(nn + 255) / 256, 256, 0, st>>>(s->node_lo, s->node_hi, s->node_jump, nn, node_base,
+                                                       corner_base, const_cast<float4*>(cat.node_lo),
+                                                       const_cast<float4*>(cat.node_hi),
+                                                       const_cast<uint32_t*>(cat.node_jump));
+    if (cudaGetLastError() != cudaSuccess) return FK_ERR_CUDA;
+  }
+  if (s->wide && s->wide_count) {
+    const uint32_t n = s->wide_count;
+    cat_records_kernel<<<(4 * n + 255) / 256, 256, 0, st>>>(s->wide, n, 4, 3, 2, rec2, node_base,
+                                                            const_cast<float4*>(cat.wide));
+    if (cudaGetLastError() != cudaSuccess) return FK_ERR_CUDA;
+  }
+  if (s->wide4 && s->wide4_count) {
+    const uint32_t n = s->wide4_count;
+    cat_records_kernel<<<(8 * n + 255) / 256, 256, 0, st>>>(s->wide4, n, 8, 6, 4, rec4, node_base,
+                                                            const_cast<float4*>(cat.wide4));
+    if (cudaGetLastError() != cudaSuccess) return FK_ERR_CUDA;
+  }
+  const size_t nc = s->corner_count;
+  if (nc) {
+    if (cudaMemcpyAsync(const_cast<float4*>(cat.pos4) + corner_base, s->pos4, 16 * nc, cudaMemcpyDeviceToDevice,
+                        st) != cudaSuccess ||
+        cudaMemcpyAsync(const_cast<float4*>(cat.nrm4) + corner_base, s->nrm4, 16 * nc, cudaMemcpyDeviceToDevice,
+                        st) != cudaSuccess ||
+        cudaMemcpyAsync(const_cast<float4*>(cat.rec) + 4 * (size_t)(corner_base / 3), s->tri_rec, 64 * (nc / 3),
+                        cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return FK_ERR_CUDA;
+  }
+  return FK_OK;
 }
 
 // Per-texel folds for a batch chunk: global texels [t0, t1), one warp each.
