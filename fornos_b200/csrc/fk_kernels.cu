@@ -1273,8 +1273,11 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
 // over the job table, which every block keeps in shared memory, and traverses
 // that job's scene in place.  `stride` > 1 traces every stride-th ray only
 // (the autotuner's calibration sample).
+#ifndef FK_BATCH_MIN_BLOCKS
+#define FK_BATCH_MIN_BLOCKS 5
+#endif
 template <int KIND, int TRAV, bool FILTER>
-__global__ void __launch_bounds__(256, 5) batch_trace_kernel(BatchArgs p) {
+__global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(BatchArgs p) {
   constexpr int STOP = KIND == FK_THICK ? kClosest : (KIND == FK_BN ? kAnyHit : kUnderMax);
   // the job table is read at ray set-up only (through the cache): node visits
   // need nothing per job, since the scenes are concatenated
