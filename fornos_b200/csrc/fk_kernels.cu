@@ -872,10 +872,11 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
         const uint32_t r = base + __popc(idle & lower);
         if (r < p.total) {
           // queue slot q of the texel -> sample k (a bijection of 0..spp-1)
-          const uint32_t q = r % p.spp;
+          const uint32_t tq = r / p.spp;  // texel of the ray within the launch
+          const uint32_t q = r - tq * p.spp;
           const uint32_t k = p.sectors > 1 ? (q & 31u) * p.sectors + (q >> 5) : q;
           slot = r - q + k;
-          const uint32_t g = list_texel(p.ids, p.texel_limit, p.texel0 + r / p.spp, p.status);
+          const uint32_t g = list_texel(p.ids, p.texel_limit, p.texel0 + tq, p.status);
           const uint32_t id = g == kMiss ? kMiss : __ldg(p.tidx + g);
           best = FLT_MAX;
           bool done = true;
@@ -1326,8 +1327,16 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
           while (job + 1 < (int)p.njobs && jobs[job + 1].ray_base <= r) ++job;
           const BatchJobDev& J = jobs[job];
           const unsigned long long local = r - J.ray_base;
-          const uint32_t g = (uint32_t)(local / J.spp);
-          uint32_t k = (uint32_t)(local % J.spp);
+          // texel and sample of the ray within its job: 32-bit division when the
+          // job's ray index fits (a 64-bit one is a long subroutine)
+          uint32_t g, k;
+          if (local < 0x100000000ull) {
+            g = (uint32_t)local / J.spp;
+            k = (uint32_t)local - g * J.spp;
+          } else {
+            g = (uint32_t)(local / J.spp);
+            k = (uint32_t)(local - (unsigned long long)g * J.spp);
+          }
           slot = q;
           if (p.ray_order == FK_RAY_ORDER_SECTOR && p.stride == 1 && J.spp >= 64 && (J.spp & 31u) == 0) {
             // queue slot k of the texel traces sample (k % 32) * (spp / 32) + k / 32
