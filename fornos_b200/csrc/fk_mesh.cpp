@@ -3,9 +3,11 @@
 // table (Src/math.h:314-382).  Arithmetic is binary32 in the reference's
 // evaluation order (the library is built with -ffp-contract=off), so the
 // results are the reference's bit for bit.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
+#include <thread>
 #include <unordered_map>
 
 #include "fk_internal.h"
@@ -223,11 +225,19 @@ int fk_mesh_compute_tangent_space(fk_mesh* m) {
 // the reference, seeded with `seed` instead of std::random_device.
 int fk_samples_cosine(uint32_t spp, uint32_t perms, uint32_t seed, float* out4) {
   if (!out4 || spp == 0 || perms == 0) return FK_ERR_INVALID;
+  // The rows' random words are drawn in order from one engine; the rows are
+  // then independent and are filled on several threads (the same operations
+  // per sample, so the table does not depend on the thread count).
   std::mt19937 eng(seed);
   std::uniform_int_distribution<uint32_t> dist;
-  const float two_pi = (float)(2.0 * 3.14159265);
+  std::vector<uint32_t> words(2 * (size_t)perms);
   for (uint32_t row = 0; row < perms; ++row) {
-    uint32_t rx = dist(eng), ry = dist(eng);
+    words[2 * (size_t)row] = dist(eng);
+    words[2 * (size_t)row + 1] = dist(eng);
+  }
+  const float two_pi = (float)(2.0 * 3.14159265);
+  auto fill = [&](uint32_t row) {
+    const uint32_t rx = words[2 * (size_t)row], ry = words[2 * (size_t)row + 1];
     float xoff = float(rx & 0xffffu) / float(1 << 16);
     for (uint32_t i = 0; i < spp; ++i) {
       uint32_t rev = i;
@@ -247,7 +257,19 @@ int fk_samples_cosine(uint32_t spp, uint32_t perms, uint32_t seed, float* out4) 
       o[2] = std::sqrt(1.0f - u);
       o[3] = 0.0f;
     }
+  };
+  const uint64_t work = (uint64_t)spp * perms;
+  const unsigned threads = work < (1u << 16) ? 1u : std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  if (threads == 1) {
+    for (uint32_t row = 0; row < perms; ++row) fill(row);
+    return FK_OK;
   }
+  std::vector<std::thread> pool;
+  for (unsigned t = 0; t < threads; ++t)
+    pool.emplace_back([&, t] {
+      for (uint32_t row = t; row < perms; row += threads) fill(row);
+    });
+  for (auto& th : pool) th.join();
   return FK_OK;
 }
 
