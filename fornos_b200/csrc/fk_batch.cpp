@@ -41,6 +41,7 @@ struct fk_batch {
   bool ordered_ok = true;                 // every tree fits the 2-wide ordered traversal's stack
   bool ordered4_ok = true;                // every collapsed tree fits the 4-wide traversal's stack
   bool filter = true;
+  bool filter_ok = true;                  // every scene's coordinates admit the filtered box tests
   fk_tuning tuning = {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64};
   // the jobs' scenes laid end to end (fk::BatchArgs::cat) and its allocations
   fk::SceneDev cat = {};
@@ -72,7 +73,7 @@ static int batch_run_chunks(fk_batch* b, int trav, bool filter, const fk_tuning&
     a.leaf_batch = tun.leaf_batch;
     a.ray_order = tun.ray_order;
     a.speculate = tun.speculate;
-    cudaError_t e = fk::launch_batch(a, b->kind, trav, filter, ctx->stream, ctx->sm_count, true);
+    cudaError_t e = fk::launch_batch(a, b->kind, trav, filter && b->filter_ok, ctx->stream, ctx->sm_count, true);
     if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "batch launch");
     ctx->launches += 2;
   }
@@ -114,7 +115,7 @@ static int batch_time(fk_batch* b, unsigned long long stride, int trav, bool fil
   for (int rep = 0; rep < 2 && rc == FK_OK; ++rep) {
     cudaMemsetAsync(q, 0, sizeof(unsigned long long), ctx->stream);
     cudaEventRecord(e0, ctx->stream);
-    cudaError_t e = fk::launch_batch(a, b->kind, trav, filter, ctx->stream, ctx->sm_count, false);
+    cudaError_t e = fk::launch_batch(a, b->kind, trav, filter && b->filter_ok, ctx->stream, ctx->sm_count, false);
     cudaEventRecord(e1, ctx->stream);
     if (e != cudaSuccess) rc = fk_cuda_fail(ctx, e, "batch calibration");
     else if ((e = cudaEventSynchronize(e1)) != cudaSuccess) rc = fk_cuda_fail(ctx, e, "batch calibration sync");
@@ -253,6 +254,7 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   for (uint32_t i = 0; i < njobs; ++i) {
     if (jobs[i].scene->odepth > fk::kMaxOrderedDepth) b->ordered_ok = false;
     if (jobs[i].scene->depth4 > fk::kMaxOrdered4Depth) b->ordered4_ok = false;
+    if (!jobs[i].scene->filter_ok) b->filter_ok = false;
   }
   b->traverse = b->ordered_ok ? FK_TRAVERSE_ORDERED : FK_TRAVERSE_SKIP;
   b->tuning = ctx->tuning;

@@ -378,14 +378,16 @@ static int scene_create(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, cons
   s->wide4_count = 0;  // the 4-wide layout is built on first use (fk::ensure_wide4)
   s->depth4 = 0;
   s->root_is_leaf = nodes[0].jump == 1;
-  // The filtered box test assumes |box - origin| < 2^26; ray origins lie on
+  // The filtered box tests assume |box - origin| < 2^26; ray origins lie on
   // the scene's triangles, so box and corner coordinates below 2^24 suffice.
+  // The conservative inner test also takes each box's faces in order.
   {
     const float lim = 16777216.0f;
     bool ok = true;
     for (uint32_t i = 0; i < nn && ok; ++i)
       for (int a = 0; a < 3; ++a)
-        ok = ok && std::fabs(nodes[i].aabb_min[a]) < lim && std::fabs(nodes[i].aabb_max[a]) < lim;
+        ok = ok && std::fabs(nodes[i].aabb_min[a]) < lim && std::fabs(nodes[i].aabb_max[a]) < lim &&
+             nodes[i].aabb_min[a] <= nodes[i].aabb_max[a];
     if (!dev) {
       // the corners are checked on the device once uploaded (below)
     } else if (ok) {

@@ -62,7 +62,8 @@ __device__ __forceinline__ float ray_box(f3 o, f3 d, f3 lo, f3 hi) {
 // The outcome is therefore always that of ray_box(o, d, lo, hi) < thr.
 struct RayPre {
   f3 o, d, inv;
-  bool exact_only;  // some |d| is nonzero but below 2^-100: always divide
+  f3 ol, oh;        // box_near: per-axis offsets of the near and far faces
+  bool exact_only;  // the filtered decision's premises fail: always divide
 };
 
 __device__ __forceinline__ RayPre ray_pre(f3 o, f3 d) {
@@ -73,6 +74,51 @@ __device__ __forceinline__ RayPre ray_pre(f3 o, f3 d) {
   const float tiny = 7.8886091e-31f;  // 2^-100
   r.exact_only = (d.x != 0.0f && fabsf(d.x) < tiny) || (d.y != 0.0f && fabsf(d.y) < tiny) ||
                  (d.z != 0.0f && fabsf(d.z) < tiny);
+  r.ol = mk3(FLT_MAX, FLT_MAX, FLT_MAX);
+  r.oh = mk3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+  return r;
+}
+
+// Terms of box_near on one axis, for origin o, direction d and a scene whose
+// boxes lie within [lo, hi] on this axis (the root box).  Let M bound |o| and
+// every face coordinate f, and inv = fl(1 / d).  The slab value box_near
+// computes, fl(f * inv - fl(fl(o * inv) +- m)), and the reference's,
+// fl(fl(f - o) / d), both lie within 2 |Q| u + |o inv| u (+ subnormal terms)
+// of the real Q = (f - o) / d, with |Q| <= 2 M |inv| (1 + u) and u = 2^-24;
+// their difference is therefore below 10.02 u M |inv| + 2^-149, and so is
+// the rounding of ol / oh themselves.  The margin m = 2^-20 M |inv| +
+// 2^-126 (16 u per unit, rounded) covers that, so the near face's value,
+// shifted by -m, is at most the reference's, and the far face's, shifted by
+// +m, at least.  The products stay below 2^124 when M |inv| < 2^120.  An axis
+// where that fails, or where |d| < 2^-100 (including d = 0), is left
+// unconstrained (slab values -FLT_MAX / +FLT_MAX: the box's other axes
+// decide), and the ray then takes the exact quotients in box_hit.  M below
+// 2^24 is box_hit's premise (|f - o| < 2^26) as well.
+__device__ __forceinline__ void near_far_axis(float o, float d, float lo, float hi, float& inv, float& ol, float& oh,
+                                              bool& exact) {
+  const float rc = __frcp_rn(d);
+  const float M = fmaxf(fmaxf(fabsf(lo), fabsf(hi)), fabsf(o));
+  const float span = __fmul_rn(M, fabsf(rc));
+  const bool ok = fabsf(d) >= 7.8886091e-31f && M < 16777216.0f && span < 1.32922800e36f;  // 2^-100, 2^24, 2^120
+  const float m = __fmaf_rn(span, 9.53674316e-07f, 1.17549435e-38f);                         // 2^-20, 2^-126
+  const float oi = __fmul_rn(o, rc);
+  const float sm = rc < 0.0f ? -m : m;
+  inv = ok ? rc : 0.0f;
+  ol = ok ? __fadd_rn(oi, sm) : FLT_MAX;
+  oh = ok ? __fsub_rn(oi, sm) : -FLT_MAX;
+  exact = exact || !ok;
+}
+
+// Ray terms for both box tests (box_hit, box_near) over a scene with root box
+// [L, H] whose coordinates are all below 2^24 in magnitude.
+__device__ __forceinline__ RayPre ray_pre_bounded(f3 o, f3 d, f3 L, f3 H) {
+  RayPre r;
+  r.o = o;
+  r.d = d;
+  r.exact_only = false;
+  near_far_axis(o.x, d.x, L.x, H.x, r.inv.x, r.ol.x, r.oh.x, r.exact_only);
+  near_far_axis(o.y, d.y, L.y, H.y, r.inv.y, r.ol.y, r.oh.y, r.exact_only);
+  near_far_axis(o.z, d.z, L.z, H.z, r.inv.z, r.ol.z, r.oh.z, r.exact_only);
   return r;
 }
 
@@ -115,29 +161,23 @@ __device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr
   return ((b >= 0.0f && a <= b) ? a : FLT_MAX) < thr;
 }
 
-// Conservative form for boxes that only prune (inner nodes): false only when
-// ray_box(o, d, lo, hi) < thr certainly fails, true when it holds or is
-// uncertain.  `entry` is the filtered entry distance.  An infinite entry or a
-// minus-infinite exit (a direction component of exactly 0 with the origin
-// outside that slab) is a certain miss of the exact test as well; rejecting it
-// here matters for speed, since its margins are NaN and the box would
-// otherwise be accepted, and with it every box below.  For the rare ray whose
-// direction has a component in (0, 2^-100) (exact_only) every box is
-// accepted, with entry -FLT_MAX so that deferred culling keeps it: its leaf
-// boxes are still tested exactly, so results are unchanged, and the test
-// stays free of branches.
-__device__ __forceinline__ bool box_maybe(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
-  f3 n1 = sub(lo, r.o), n2 = sub(hi, r.o);
-  f3 t1 = mk3(__fmul_rn(n1.x, r.inv.x), __fmul_rn(n1.y, r.inv.y), __fmul_rn(n1.z, r.inv.z));
-  f3 t2 = mk3(__fmul_rn(n2.x, r.inv.x), __fmul_rn(n2.y, r.inv.y), __fmul_rn(n2.z, r.inv.z));
-  f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
-  float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
-  float b = fminf(tx.x, fminf(tx.y, tx.z));
-  const float inf = __int_as_float(0x7f800000);
-  const float a_lo = below(a), b_hi = above(b);
-  const bool reject = !(a < inf) || !(b > -inf) || b_hi < 0.0f || a_lo > b_hi || a_lo >= thr;
-  entry = r.exact_only ? -FLT_MAX : a;
-  return r.exact_only || !reject;
+// Conservative test for boxes that only prune (inner records), on the terms
+// of ray_pre_bounded: one fused multiply-add per slab value, margins folded
+// into the offsets.  The near value of each axis is at most the reference's
+// and the far value at least (near_far_axis), min / max keep those bounds,
+// so a <= the reference's entry and b >= its exit: whenever
+// ray_box(o, d, lo, hi) < thr holds (exit >= 0, entry <= exit, entry < thr)
+// this holds too.  `entry` = a is a lower bound of the reference's entry
+// distance, for ordering and for culling deferred records (entry < thr).  The
+// box must lie within the root box the terms were made for.
+__device__ __forceinline__ bool box_near(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
+  const float t1x = __fmaf_rn(lo.x, r.inv.x, -r.ol.x), t2x = __fmaf_rn(hi.x, r.inv.x, -r.oh.x);
+  const float t1y = __fmaf_rn(lo.y, r.inv.y, -r.ol.y), t2y = __fmaf_rn(hi.y, r.inv.y, -r.oh.y);
+  const float t1z = __fmaf_rn(lo.z, r.inv.z, -r.ol.z), t2z = __fmaf_rn(hi.z, r.inv.z, -r.oh.z);
+  const float a = fmaxf(fmaxf(fminf(t1x, t2x), fminf(t1y, t2y)), fminf(t1z, t2z));
+  const float b = fminf(fminf(fmaxf(t1x, t2x), fmaxf(t1y, t2y)), fmaxf(t1z, t2z));
+  entry = a;
+  return fmaxf(a, 0.0f) <= b && a < thr;
 }
 
 // Binary64 barycentric of Shaders/meshmapping_nobackfaces.comp:48-62.

@@ -80,7 +80,7 @@ struct fk_scene {
   uint32_t top_count = 0, top_want = 0;
   int top_tree = -1;
   uint32_t root_is_leaf = 0;
-  uint32_t filter_ok = 0;        // every coordinate below 2^24 in magnitude
+  uint32_t filter_ok = 0;        // every coordinate below 2^24 in magnitude, box faces in order
   size_t bytes = 0;
 };
 

@@ -428,7 +428,8 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   if (trav == FK_TRAVERSE_ORDERED4 && sched != FK_SCHEDULE_DYNAMIC)
     return fk_fail(ctx, FK_ERR_UNSUPPORTED, "the 4-wide traversal runs on the dynamic schedule only");
   const uint32_t refill = h.refill ? h.refill : ctx->tuning.refill;
-  const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
+  // the filtered box tests need every scene coordinate below 2^24 (fk_scene::filter_ok)
+  const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS) && s->filter_ok;
   const uint32_t leaf_batch = h.leaf_batch ? h.leaf_batch : ctx->tuning.leaf_batch;
   const uint32_t speculate = h.speculate ? h.speculate : ctx->tuning.speculate;
   TraceExtras x;
@@ -539,22 +540,22 @@ __device__ __forceinline__ bool child_hit(const RayPre& r, f3 lo, f3 hi, float t
 }
 
 // Inner-phase child test of the ordered traversals.  The filtered form is
-// conservative: a box there only prunes (the exact slab test is monotone, so a
-// box inside one the ray misses is missed too), and every leaf's box is
-// tested exactly when the leaf is visited, so accepting an uncertain box only
-// adds work.  That keeps the divisions out of the inner phase.
+// conservative (fk_device.cuh: box_near): a box there only prunes (the exact
+// slab test is monotone, so a box inside one the ray misses is missed too),
+// and every leaf's box is tested exactly when the leaf is visited, so
+// accepting a box the exact test would reject only adds work.  That keeps the
+// divisions out of the inner phase.  Its entry distance is a lower bound of
+// the exact one, so deferred records compare it directly (still_open).
 template <bool FILTER>
 __device__ __forceinline__ bool child_maybe(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
-  if (FILTER) return box_maybe(r, lo, hi, thr, entry);
+  if (FILTER) return box_near(r, lo, hi, thr, entry);
   entry = ray_box(r.o, r.d, lo, hi);
   return entry < thr;
 }
 
-// Deferred node still worth visiting: exact distances compare directly;
-// filtered ones only cull when certainly at or beyond the threshold.
+// Deferred node still worth visiting.
 template <bool FILTER>
 __device__ __forceinline__ bool still_open(float entry, float thr) {
-  if (FILTER) return below(entry) < thr;
   return entry < thr;
 }
 
@@ -568,7 +569,6 @@ __device__ __forceinline__ bool still_open(float entry, float thr) {
 // triangles run, so the leaf set is that of the ordered traversal.
 struct OState {
   int32_t cur, pend;
-  float pend_dist;
   int sp;
 };
 
@@ -789,7 +789,6 @@ __device__ __forceinline__ bool pop(OState& st, const int2* stk, float thr) {
     if (!still_open<FILTER>(dist, thr)) continue;
     if (e.x < 0) {
       st.pend = -e.x - 1;
-      st.pend_dist = dist;
     } else {
       st.cur = e.x;
     }
@@ -854,7 +853,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX;
   int32_t cur = 0;  // skip walk: node index
-  OState st = {-1, -1, 0.0f, 0};
+  OState st = {-1, -1, 0};
   // counting variant, per warp: iterations, leaf-phase iterations, lanes at
   // work in inner / leaf phases, lanes holding a ray, refills
   unsigned long long wc[6] = {0, 0, 0, 0, 0, 0};
@@ -886,20 +885,21 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
             if (KIND == FK_THICK) d = neg(d);
             float4 rs = __ldg(p.samples + (size_t)(g % p.perms) * p.spp + k);
             f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
-            rp = ray_pre(o, dir);
-            if (!p.s.filter_ok) rp.exact_only = true;
             if (is_ordered(TRAV)) {
-              float4 L = __ldg(p.s.node_lo), H = __ldg(p.s.node_hi);
+              const float4 L = __ldg(p.s.node_lo), H = __ldg(p.s.node_hi);
+              rp = ray_pre_bounded(o, dir, xyz(L), xyz(H));
+              if (!p.s.filter_ok) rp.exact_only = true;
               float a;
               if (COUNT) tally.box++;
               if (child_hit<FILTER>(rp, xyz(L), xyz(H), p.hi, a)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
                 st.cur = p.s.root_is_leaf ? -1 : (TOP ? (int32_t)top_base : 0);
                 st.pend = p.s.root_is_leaf ? 0 : -1;
-                st.pend_dist = a;
                 done = false;
               }
             } else {
+              rp = ray_pre(o, dir);
+              if (!p.s.filter_ok) rp.exact_only = true;
               cur = 0;
               done = false;
             }
@@ -1309,7 +1309,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
   float best = FLT_MAX, lo = 0.0f, hi = 0.0f;
   int32_t cur = 0;
   uint32_t end = 0;  // skip walk: one past the job's last node
-  OState st = {-1, -1, 0.0f, 0};
+  OState st = {-1, -1, 0};
   const SceneDev& s = p.cat;  // every job's scene, concatenated
   for (;;) {
     unsigned idle = __ballot_sync(full, !active);
@@ -1355,19 +1355,20 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
             if (KIND == FK_THICK) d = neg(d);
             float4 rs = __ldg(J.samples + (size_t)(g % J.perms) * J.spp + k);
             f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
-            rp = ray_pre(o, dir);
-            if (!J.s.filter_ok) rp.exact_only = true;
             if (is_ordered(TRAV)) {
-              float4 L = __ldg(s.node_lo + J.node_base), H = __ldg(s.node_hi + J.node_base);
+              const float4 L = __ldg(s.node_lo + J.node_base), H = __ldg(s.node_hi + J.node_base);
+              rp = ray_pre_bounded(o, dir, xyz(L), xyz(H));
+              if (!J.s.filter_ok) rp.exact_only = true;
               float aa;
               if (child_hit<FILTER>(rp, xyz(L), xyz(H), hi, aa)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
                 st.cur = J.s.root_is_leaf ? -1 : (TRAV == FK_TRAVERSE_ORDERED4 ? J.root4 : J.root2);
                 st.pend = J.s.root_is_leaf ? (int32_t)J.node_base : -1;
-                st.pend_dist = aa;
                 done = false;
               }
             } else {
+              rp = ray_pre(o, dir);
+              if (!J.s.filter_ok) rp.exact_only = true;
               cur = (int32_t)J.node_base;
               end = J.node_base + J.s.node_count;
               done = false;
@@ -1702,7 +1703,7 @@ int launch_hemisphere_external(const fk_scene* s, const HemiLaunch& h, cudaStrea
     err = "4-wide traversal needs a 4-wide depth <= 21; use FK_TRAVERSE_ORDERED";
     return FK_ERR_INVALID;
   }
-  const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS);
+  const bool filter = !(h.traverse & FK_EXACT_BOX_TESTS) && s->filter_ok;
   cudaError_t e = cudaSuccess;
 #define FK_EXT_CASE(K)                                                                                     \
   case K:                                                                                                  \
