@@ -16,6 +16,8 @@ struct Scoped {
   fk_scene* scene = nullptr;
   fk_texel_map* map = nullptr;
   ~Scoped() {
+    // result copies on the copy stream read these buffers: they finish first
+    if (ctx->copy_stream) cudaStreamSynchronize(ctx->copy_stream);
     for (fk_buf* b : bufs) fk_buf_release(ctx, b);  // used on the context's stream only
     if (scene) fk_scene_free(ctx, scene);
     if (map) fk_texel_map_free(ctx, map);
@@ -32,9 +34,18 @@ bool same_params(const fk_bake_sampler& a, const fk_bake_sampler& b) {
          a.seed == b.seed;
 }
 
+// Copies a finished result to the host on the copy stream, once the work
+// queued so far on the context's stream is done, so that the copy overlaps
+// the passes queued after it.
 int download(fk_ctx* ctx, const fk_buf* b, void* dst, size_t bytes) {
   if (!dst || !bytes) return FK_OK;
-  FK_CUDA(ctx, cudaMemcpyAsync(dst, b->ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  cudaEvent_t ev;
+  FK_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+  cudaError_t e = cudaEventRecord(ev, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_stream, ev, 0);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dst, b->ptr, bytes, cudaMemcpyDeviceToHost, ctx->copy_stream);
+  cudaEventDestroy(ev);
+  if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "fk_bake: result copy");
   return FK_OK;
 }
 
@@ -43,10 +54,17 @@ int download(fk_ctx* ctx, const fk_buf* b, void* dst, size_t bytes) {
 extern "C" int fk_bake(fk_ctx* ctx, const fk_bake_desc* d, fk_bake_out* out) {
   if (!ctx || !d || !out) return fk_fail(ctx, FK_ERR_INVALID, "fk_bake: null argument");
   const uint32_t perms = 4096;
+  if (!ctx->copy_stream && cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    ctx->copy_stream = nullptr;
+    return fk_fail(ctx, FK_ERR_CUDA, "fk_bake: copy stream");
+  }
   Scoped s{ctx};
-  int rc = fk_scene_upload(ctx, d->nodes, d->node_count, d->positions4, d->normals4, d->corner_count, &s.scene);
+  // the texel rows go up while the host checks and lays out the scene (the
+  // scene upload waits for the stream before it returns)
+  int rc = fk::texel_map_upload_async(ctx, d->width, d->height, d->texel_count, d->pix8, d->pixt12, d->indices,
+                                      &s.map);
   if (rc != FK_OK) return rc;
-  rc = fk_texel_map_from_host(ctx, d->width, d->height, d->texel_count, d->pix8, d->pixt12, d->indices, &s.map);
+  rc = fk_scene_upload(ctx, d->nodes, d->node_count, d->positions4, d->normals4, d->corner_count, &s.scene);
   if (rc != FK_OK) return rc;
   const uint32_t n = d->texel_count;
   const size_t nn = n ? n : 1;
@@ -54,6 +72,8 @@ extern "C" int fk_bake(fk_ctx* ctx, const fk_bake_desc* d, fk_bake_out* out) {
   if ((rc = s.alloc(16 * nn, &coords)) != FK_OK || (rc = s.alloc(4 * nn, &tidx)) != FK_OK) return rc;
   if ((rc = fk_meshmap(ctx, s.scene, s.map, d->cull_backfaces,
                        d->mapping_max_distance > 0.0f ? d->mapping_max_distance : FLT_MAX, 0, n, coords, tidx)) != FK_OK) return rc;
+  if ((rc = download(ctx, coords, out->coords4, 16 * (size_t)n)) != FK_OK) return rc;
+  if ((rc = download(ctx, tidx, out->tidx, 4 * (size_t)n)) != FK_OK) return rc;
 
   auto gather = [&](int enabled, int kind, float* host, size_t width, int tangent) -> int {
     if (!enabled) return FK_OK;
@@ -126,9 +146,8 @@ extern "C" int fk_bake(fk_ctx* ctx, const fk_bake_desc* d, fk_bake_out* out) {
       return rc;
     if ((rc = download(ctx, th_out, out->thickness, 4 * (size_t)n)) != FK_OK) return rc;
   }
-  if ((rc = download(ctx, coords, out->coords4, 16 * (size_t)n)) != FK_OK) return rc;
-  if ((rc = download(ctx, tidx, out->tidx, 4 * (size_t)n)) != FK_OK) return rc;
   FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  FK_CUDA(ctx, cudaStreamSynchronize(ctx->copy_stream));
   int st = 0;
   FK_CUDA(ctx, cudaMemcpy(&st, ctx->status, sizeof(int), cudaMemcpyDeviceToHost));
   if (st) {

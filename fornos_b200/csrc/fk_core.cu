@@ -175,6 +175,7 @@ int fk_ctx_destroy(fk_ctx* ctx) {
   cudaFree(ctx->status);
   cudaFree(ctx->scratch);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+  if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return FK_OK;
@@ -618,6 +619,27 @@ int fk_scene_get_info(const fk_scene* s, fk_scene_info* o) {
 // ------------------------------------------------------------------ texel map
 int fk_texel_map_from_host(fk_ctx* ctx, uint32_t w, uint32_t h, uint32_t count, const float* pix8,
                            const float* pixt12, const uint32_t* idx, fk_texel_map** out) {
+  int rc = fk::texel_map_upload_async(ctx, w, h, count, pix8, pixt12, idx, out);
+  if (rc == FK_OK && count) {
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+      fk_texel_map_free(ctx, *out);
+      *out = nullptr;
+      return fk_cuda_fail(ctx, e, "fk_texel_map_from_host");
+    }
+  }
+  return rc;
+}
+
+}  // extern "C"
+
+namespace fk {
+
+// fk_texel_map_from_host without the final wait: the copies are queued on the
+// context's stream, so the host rows must stay unchanged until that stream
+// has passed them.
+int texel_map_upload_async(fk_ctx* ctx, uint32_t w, uint32_t h, uint32_t count, const float* pix8,
+                           const float* pixt12, const uint32_t* idx, fk_texel_map** out) {
   if (!ctx || !out || (count && (!pix8 || !pixt12 || !idx)) || (uint64_t)count > (uint64_t)w * h)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_texel_map_from_host: bad arguments");
   fk_texel_map* m = new (std::nothrow) fk_texel_map();
@@ -638,11 +660,14 @@ int fk_texel_map_from_host(fk_ctx* ctx, uint32_t w, uint32_t h, uint32_t count, 
     FK_CUDA(ctx, cudaMemcpyAsync(m->pix, pix8, 32 * (size_t)count, cudaMemcpyHostToDevice, ctx->stream));
     FK_CUDA(ctx, cudaMemcpyAsync(m->pixt, pixt12, 48 * (size_t)count, cudaMemcpyHostToDevice, ctx->stream));
     FK_CUDA(ctx, cudaMemcpyAsync(m->indices, idx, 4 * (size_t)count, cudaMemcpyHostToDevice, ctx->stream));
-    FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   }
   *out = m;
   return FK_OK;
 }
+
+}  // namespace fk
+
+extern "C" {
 
 int fk_texel_map_info(const fk_texel_map* m, uint32_t* w, uint32_t* h, uint32_t* count) {
   if (!m) return FK_ERR_INVALID;

@@ -18,6 +18,7 @@ struct fk_ctx {
   int sm_count = 0;
   cudaStream_t own_stream = nullptr;
   cudaStream_t stream = nullptr;
+  cudaStream_t copy_stream = nullptr;  // fk_bake's result copies, beside the stream's work (made on first use)
   std::string err;
   uint64_t launches = 0;
   uint32_t* counters = nullptr;   // device work-queue counters for persistent kernels
@@ -30,7 +31,7 @@ struct fk_ctx {
   // bakes reuse it instead of mapping and unmapping pages (fk_ctx_trim).
   cudaMemPool_t pool = nullptr;
   size_t scratch_bytes = 0;
-  fk_tuning tuning = {16, 8, 1, FK_RAY_ORDER_SECTOR, 0, FK_L2_NONE, 256, 64};  // fk_ctx_set_tuning
+  fk_tuning tuning = {20, 8, 1, FK_RAY_ORDER_SECTOR, 0, FK_L2_NONE, 256, 64};  // fk_ctx_set_tuning
   // Persisting L2 set-aside (fk_tuning.l2_persist): the device's limit before
   // the context raised it, restored when the knob is turned off or the
   // context is destroyed.
@@ -91,6 +92,11 @@ struct fk_texel_map {
   float4* pixt = nullptr;    // 3 float4 per texel: n, t, b
   uint32_t* indices = nullptr;
 };
+
+namespace fk {
+int texel_map_upload_async(fk_ctx* ctx, uint32_t w, uint32_t h, uint32_t count, const float* pix8,
+                           const float* pixt12, const uint32_t* idx, fk_texel_map** out);
+}
 
 // ------------------------------------------------------------------ helpers
 int fk_fail(fk_ctx* ctx, int code, const std::string& msg);

@@ -823,7 +823,7 @@ __device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, f
 // decides its next phase again (the phase ballots and the refill check are
 // paid once per kInnerVisits visits).
 #ifndef FK_INNER_VISITS
-#define FK_INNER_VISITS 3
+#define FK_INNER_VISITS 4
 #endif
 constexpr int kInnerVisits = FK_INNER_VISITS;
 

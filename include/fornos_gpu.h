@@ -75,7 +75,7 @@ int fk_ctx_trim(fk_ctx* ctx);
 /* Kernel launches issued by this context so far. */
 uint64_t fk_launch_count(const fk_ctx* ctx);
 
-/* Knobs of the dynamically scheduled hemisphere traversal (defaults 16, 8,
+/* Knobs of the dynamically scheduled hemisphere traversal (defaults 20, 8,
  * 1, FK_RAY_ORDER_SECTOR, from full-size sweeps of the plane workload);
  * fk_tune_hemisphere picks them by measurement.  No knob changes a result:
  * each ray still writes the slot of its own sample, and the per-texel sums
