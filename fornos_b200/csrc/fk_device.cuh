@@ -136,9 +136,10 @@ __device__ __forceinline__ float above(float v) {
 }
 
 // Returns ray_box(o, d, lo, hi) < thr exactly, and in `entry` the filtered
-// entry distance (for ordering / deferred culling only).
-__device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
-  f3 n1 = sub(lo, r.o), n2 = sub(hi, r.o);
+// entry distance (for ordering / deferred culling only).  o and d are the
+// ray's (kept outside `r` where registers are short); r supplies 1 / d.
+__device__ __forceinline__ bool box_hit(const RayPre& r, f3 o, f3 d, f3 lo, f3 hi, float thr, float& entry) {
+  f3 n1 = sub(lo, o), n2 = sub(hi, o);
   if (!r.exact_only) {
     f3 t1 = mk3(__fmul_rn(n1.x, r.inv.x), __fmul_rn(n1.y, r.inv.y), __fmul_rn(n1.z, r.inv.z));
     f3 t2 = mk3(__fmul_rn(n2.x, r.inv.x), __fmul_rn(n2.y, r.inv.y), __fmul_rn(n2.z, r.inv.z));
@@ -153,12 +154,15 @@ __device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr
     const float a_hi = above(a), b_lo = below(b);
     if (b_lo >= 0.0f && a_hi <= b_lo && a_hi < thr) return true;
   }
-  f3 t1 = divv(n1, r.d), t2 = divv(n2, r.d);
+  f3 t1 = divv(n1, d), t2 = divv(n2, d);
   f3 tn = vmin(t1, t2), tx = vmax(t1, t2);
   float a = fmaxf(tn.x, fmaxf(tn.y, tn.z));
   float b = fminf(tx.x, fminf(tx.y, tx.z));
   entry = a;
   return ((b >= 0.0f && a <= b) ? a : FLT_MAX) < thr;
+}
+__device__ __forceinline__ bool box_hit(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
+  return box_hit(r, r.o, r.d, lo, hi, thr, entry);
 }
 
 // Conservative test for boxes that only prune (inner records), on the terms

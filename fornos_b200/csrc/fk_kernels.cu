@@ -530,12 +530,25 @@ __device__ __forceinline__ uint32_t list_texel(const uint32_t* ids, uint32_t lim
   return t;
 }
 
+// A lane's ray origin and direction live in shared memory, six words S
+// apart starting at the lane's own word (ray_put), so that registers hold only
+// the box-test terms: the inner visits need no more, the leaf phase and the
+// skip walk read them back, and any lane of the warp can read another's.
+template <int S>
+__device__ __forceinline__ void ray_put(float* p, f3 o, f3 d) {
+  p[0] = o.x, p[S] = o.y, p[2 * S] = o.z, p[3 * S] = d.x, p[4 * S] = d.y, p[5 * S] = d.z;
+}
+template <int S>
+__device__ __forceinline__ f3 ray_o(const float* p) { return mk3(p[0], p[S], p[2 * S]); }
+template <int S>
+__device__ __forceinline__ f3 ray_d(const float* p) { return mk3(p[3 * S], p[4 * S], p[5 * S]); }
+
 // Child box test of the traversal kernels: exact quotients, or the filtered
 // form (fk_device.cuh: box_hit) whose decision is provably the same.
 template <bool FILTER>
-__device__ __forceinline__ bool child_hit(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
-  if (FILTER) return box_hit(r, lo, hi, thr, entry);
-  entry = ray_box(r.o, r.d, lo, hi);
+__device__ __forceinline__ bool child_hit(const RayPre& r, f3 o, f3 d, f3 lo, f3 hi, float thr, float& entry) {
+  if (FILTER) return box_hit(r, o, d, lo, hi, thr, entry);
+  entry = ray_box(o, d, lo, hi);
   return entry < thr;
 }
 
@@ -546,10 +559,11 @@ __device__ __forceinline__ bool child_hit(const RayPre& r, f3 lo, f3 hi, float t
 // accepting a box the exact test would reject only adds work.  That keeps the
 // divisions out of the inner phase.  Its entry distance is a lower bound of
 // the exact one, so deferred records compare it directly (still_open).
-template <bool FILTER>
-__device__ __forceinline__ bool child_maybe(const RayPre& r, f3 lo, f3 hi, float thr, float& entry) {
+template <bool FILTER, int S>
+__device__ __forceinline__ bool child_maybe(const RayPre& r, const float* ray, f3 lo, f3 hi, float thr,
+                                            float& entry) {
   if (FILTER) return box_near(r, lo, hi, thr, entry);
-  entry = ray_box(r.o, r.d, lo, hi);
+  entry = ray_box(ray_o<S>(ray), ray_d<S>(ray), lo, hi);
   return entry < thr;
 }
 
@@ -583,8 +597,9 @@ struct OState {
 // with one overflow check per visit.  Straight-line code keeps the visit free
 // of divergent branches.  TOP: records ref >= top_base are read from the
 // staged copies in shared memory.
-template <bool COUNT, bool FILTER, int STACK = kStack, bool TOP = false>
-__device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
+template <bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false>
+__device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
+                                            OState& st, int2* stk,
                                             int* status, Tally& tally, const float4* top = nullptr,
                                             uint32_t top_base = 0xFFFFFFFFu) {
   float4 w0, w1, w2, w3;
@@ -596,8 +611,8 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
     w0 = __ldg(w), w1 = __ldg(w + 1), w2 = __ldg(w + 2), w3 = __ldg(w + 3);
   }
   float d0, d1;
-  const bool h0 = child_maybe<FILTER>(rp, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
-  const bool h1 = child_maybe<FILTER>(rp, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
+  const bool h0 = child_maybe<FILTER, S>(rp, ray, mk3(w0.x, w0.z, w2.x), mk3(w0.y, w0.w, w2.y), thr, d0);
+  const bool h1 = child_maybe<FILTER, S>(rp, ray, mk3(w1.x, w1.z, w2.z), mk3(w1.y, w1.w, w2.w), thr, d1);
   if (COUNT) tally.box += 2;
   const bool swap = d1 < d0;
   const bool hn = swap ? h1 : h0, hf = swap ? h0 : h1;
@@ -639,8 +654,9 @@ __device__ __forceinline__ void cex(float& ka, int32_t& ra, float& kb, int32_t& 
 // (a 5-comparator sorting network), keeps the nearest inner child as the next
 // node and the nearest leaf as the postponed leaf when none is held, and
 // defers the rest farthest first, so that the nearest is popped next.
-template <bool COUNT, bool FILTER, int STACK = kStack>
-__device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
+template <bool COUNT, bool FILTER, int S, int STACK = kStack>
+__device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
+                                             OState& st, int2* stk,
                                              int* status, Tally& tally) {
   const float4* w = s.wide4 + 8 * (size_t)st.cur;
   const float4 lx = __ldg(w), hx = __ldg(w + 1), ly = __ldg(w + 2), hy = __ldg(w + 3);
@@ -648,10 +664,10 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   const int cnt = __float_as_int(__ldg(w + 7).x);
   const float inf = __int_as_float(0x7f800000);
   float k0, k1, k2, k3;
-  const bool h0 = child_maybe<FILTER>(rp, mk3(lx.x, ly.x, lz.x), mk3(hx.x, hy.x, hz.x), thr, k0);
-  const bool h1 = child_maybe<FILTER>(rp, mk3(lx.y, ly.y, lz.y), mk3(hx.y, hy.y, hz.y), thr, k1);
-  const bool h2 = child_maybe<FILTER>(rp, mk3(lx.z, ly.z, lz.z), mk3(hx.z, hy.z, hz.z), thr, k2) && cnt > 2;
-  const bool h3 = child_maybe<FILTER>(rp, mk3(lx.w, ly.w, lz.w), mk3(hx.w, hy.w, hz.w), thr, k3) && cnt > 3;
+  const bool h0 = child_maybe<FILTER, S>(rp, ray, mk3(lx.x, ly.x, lz.x), mk3(hx.x, hy.x, hz.x), thr, k0);
+  const bool h1 = child_maybe<FILTER, S>(rp, ray, mk3(lx.y, ly.y, lz.y), mk3(hx.y, hy.y, hz.y), thr, k1);
+  const bool h2 = child_maybe<FILTER, S>(rp, ray, mk3(lx.z, ly.z, lz.z), mk3(hx.z, hy.z, hz.z), thr, k2) && cnt > 2;
+  const bool h3 = child_maybe<FILTER, S>(rp, ray, mk3(lx.w, ly.w, lz.w), mk3(hx.w, hy.w, hz.w), thr, k3) && cnt > 3;
   if (COUNT) tally.box += cnt;
   // a hit's entry distance is finite (it is below thr); misses sort last as +inf
   k0 = h0 ? k0 : inf;
@@ -693,12 +709,13 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   return true;
 }
 
-template <int TRAV, bool COUNT, bool FILTER, int STACK = kStack, bool TOP = false>
-__device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp, float thr, OState& st, int2* stk,
-                                            int* status, Tally& tally, const float4* top = nullptr,
-                                            uint32_t top_base = 0xFFFFFFFFu) {
-  if (TRAV == FK_TRAVERSE_ORDERED4) return inner_visit4<COUNT, FILTER, STACK>(s, rp, thr, st, stk, status, tally);
-  return inner_visit<COUNT, FILTER, STACK, TOP>(s, rp, thr, st, stk, status, tally, top, top_base);
+template <int TRAV, bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false>
+__device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
+                                            OState& st, int2* stk, int* status, Tally& tally,
+                                            const float4* top = nullptr, uint32_t top_base = 0xFFFFFFFFu) {
+  if (TRAV == FK_TRAVERSE_ORDERED4)
+    return inner_visit4<COUNT, FILTER, S, STACK>(s, rp, ray, thr, st, stk, status, tally);
+  return inner_visit<COUNT, FILTER, S, STACK, TOP>(s, rp, ray, thr, st, stk, status, tally, top, top_base);
 }
 
 // Order-preserving key of a non-negative distance (total order, -0 below +0)
@@ -724,18 +741,21 @@ __device__ __forceinline__ float dist_unkey(uint32_t k) {
 // this lane visited a leaf.  MULTI: lanes may trace different jobs of a
 // batch, whose scenes lie in one concatenated array but whose distance
 // ranges differ, so the owner's minimum distance travels with its ray.
-template <bool COUNT, bool FILTER, bool MULTI = false>
-__device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
-                                                OState& st, bool active, uint32_t* skey, Tally& tally) {
+template <bool COUNT, bool FILTER, int S, bool MULTI = false>
+__device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre& rp, const float* wray, float lo,
+                                                float hi, float& best, OState& st, bool active, uint32_t* skey,
+                                                Tally& tally) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   uint32_t first = 0, cnt = 0;
   const bool mine = active && st.pend >= 0;
+  __syncwarp();  // the lanes' rays, written at their set-up, are read by other lanes below
   if (mine) {
     const float4 L = __ldg(s.node_lo + st.pend), H = __ldg(s.node_hi + st.pend);
     float entry;
     if (COUNT) tally.box++;
-    if (child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry)) {
+    if (child_hit<FILTER>(rp, ray_o<S>(wray + lane), ray_d<S>(wray + lane), xyz(L), xyz(H), fminf(best, hi),
+                          entry)) {
       first = as_u32(L.w) / 3;
       cnt = (as_u32(H.w) - as_u32(L.w)) / 3;
       if (COUNT) tally.tri += cnt;
@@ -761,8 +781,7 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
       const uint32_t v = __shfl_sync(full, incl, o + step - 1);
       if (v <= j) o += step;
     }
-    const f3 ro = mk3(__shfl_sync(full, rp.o.x, o), __shfl_sync(full, rp.o.y, o), __shfl_sync(full, rp.o.z, o));
-    const f3 rd = mk3(__shfl_sync(full, rp.d.x, o), __shfl_sync(full, rp.d.y, o), __shfl_sync(full, rp.d.z, o));
+    const f3 ro = ray_o<S>(wray + o), rd = ray_d<S>(wray + o);
     const float ob = __shfl_sync(full, best, o);
     const uint32_t tri = __shfl_sync(full, first, o) + (j - __shfl_sync(full, excl, o));
     const float4* rec = s.rec;
@@ -798,18 +817,19 @@ __device__ __forceinline__ bool pop(OState& st, const int2* stk, float thr) {
 }
 
 // Skip-pointer walk, one flattened node per call.
-template <int STOP, bool COUNT, bool FILTER>
-__device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, float lo, float hi, float& best,
-                                          int32_t& cur, Tally& tally) {
+template <int STOP, bool COUNT, bool FILTER, int S>
+__device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, const float* ray, float lo, float hi,
+                                          float& best, int32_t& cur, Tally& tally) {
   uint32_t i = (uint32_t)cur;
   float4 L = __ldg(s.node_lo + i), H = __ldg(s.node_hi + i);
   float entry;
-  bool h = child_hit<FILTER>(rp, xyz(L), xyz(H), fminf(best, hi), entry);
+  const f3 o = ray_o<S>(ray), d = ray_d<S>(ray);
+  bool h = child_hit<FILTER>(rp, o, d, xyz(L), xyz(H), fminf(best, hi), entry);
   if (COUNT) tally.box++;
   if (h) {
     uint32_t e = as_u32(H.w);
     if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
-    for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, rp.o, rp.d, lo, best);
+    for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
     if (settled<STOP>(best, hi)) return true;
     ++i;
   } else {
@@ -841,6 +861,9 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
   int2 stk[is_ordered(TRAV) ? STACK : 1];  // deferred (ref, entry) pairs
   __shared__ uint32_t leaf_keys[BLOCK / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
+  __shared__ float srays[6 * BLOCK];  // the lanes' ray origins and directions (ray_put)
+  float* const myray = srays + threadIdx.x;
+  const float* const wray = srays + (threadIdx.x & ~31u);
   extern __shared__ float4 top_smem[];  // p.top_count staged records (TOP)
   if (TOP) {
     for (uint32_t i = threadIdx.x; i < 4 * p.top_count; i += blockDim.x) top_smem[i] = __ldg(p.top + i);
@@ -885,13 +908,14 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
             if (KIND == FK_THICK) d = neg(d);
             float4 rs = __ldg(p.samples + (size_t)(g % p.perms) * p.spp + k);
             f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+            ray_put<BLOCK>(myray, o, dir);
             if (is_ordered(TRAV)) {
               const float4 L = __ldg(p.s.node_lo), H = __ldg(p.s.node_hi);
               rp = ray_pre_bounded(o, dir, xyz(L), xyz(H));
               if (!p.s.filter_ok) rp.exact_only = true;
               float a;
               if (COUNT) tally.box++;
-              if (child_hit<FILTER>(rp, xyz(L), xyz(H), p.hi, a)) {  // ray_box(o, dir, root) < hi, exactly
+              if (child_hit<FILTER>(rp, o, dir, xyz(L), xyz(H), p.hi, a)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
                 st.cur = p.s.root_is_leaf ? -1 : (TOP ? (int32_t)top_base : 0);
                 st.pend = p.s.root_is_leaf ? 0 : -1;
@@ -928,14 +952,14 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
         wc[leaf_phase ? 3 : 2] += __popc(leaf_phase ? leaves : need);
       }
       const bool visited =
-          leaf_phase && leaf_phase_warp<COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, st, active, skey, tally);
+          leaf_phase && leaf_phase_warp<COUNT, FILTER, BLOCK>(p.s, rp, wray, p.lo, p.hi, best, st, active, skey, tally);
       if (active) {
         bool fin = false;
         if (leaf_phase) {
           if (visited) fin = settled<STOP>(best, p.hi);
         } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
-          if (!visit_inner<TRAV, COUNT, FILTER, STACK, TOP>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally,
-                                                             top_smem, top_base))
+          if (!visit_inner<TRAV, COUNT, FILTER, BLOCK, STACK, TOP>(p.s, rp, myray, fminf(best, p.hi), st, stk,
+                                                                    p.status, tally, top_smem, top_base))
             fin = true;
           // further visits in the same iteration, continuing from the stack
           for (int v = 1; v < kInnerVisits && !fin; ++v) {
@@ -944,8 +968,8 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
               break;
             }
             if (!(st.cur >= 0 && (st.pend < 0 || (p.speculate && st.sp < STACK - 4)))) break;
-            if (!visit_inner<TRAV, COUNT, FILTER, STACK, TOP>(p.s, rp, fminf(best, p.hi), st, stk, p.status, tally,
-                                                               top_smem, top_base))
+            if (!visit_inner<TRAV, COUNT, FILTER, BLOCK, STACK, TOP>(p.s, rp, myray, fminf(best, p.hi), st, stk,
+                                                                      p.status, tally, top_smem, top_base))
               fin = true;
           }
         }
@@ -956,7 +980,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
         }
       }
     } else if (active) {
-      if (skip_step<STOP, COUNT, FILTER>(p.s, rp, p.lo, p.hi, best, cur, tally)) {
+      if (skip_step<STOP, COUNT, FILTER, BLOCK>(p.s, rp, myray, p.lo, p.hi, best, cur, tally)) {
         p.scratch[slot] = best;
         active = false;
       }
@@ -1302,6 +1326,9 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
   int2 stk[is_ordered(TRAV) ? kStack : 1];  // deferred (ref, entry) pairs
   __shared__ uint32_t leaf_keys[256 / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
+  __shared__ float srays[6 * 256];  // the lanes' ray origins and directions (ray_put)
+  float* const myray = srays + threadIdx.x;
+  const float* const wray = srays + (threadIdx.x & ~31u);
   Tally tally;
   bool active = false, exhausted = false;
   uint32_t slot = 0;  // scratch slot of the lane's ray (its sample's, in sample order)
@@ -1355,12 +1382,13 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
             if (KIND == FK_THICK) d = neg(d);
             float4 rs = __ldg(J.samples + (size_t)(g % J.perms) * J.spp + k);
             f3 dir = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+            ray_put<256>(myray, o, dir);
             if (is_ordered(TRAV)) {
               const float4 L = __ldg(s.node_lo + J.node_base), H = __ldg(s.node_hi + J.node_base);
               rp = ray_pre_bounded(o, dir, xyz(L), xyz(H));
               if (!J.s.filter_ok) rp.exact_only = true;
               float aa;
-              if (child_hit<FILTER>(rp, xyz(L), xyz(H), hi, aa)) {  // ray_box(o, dir, root) < hi, exactly
+              if (child_hit<FILTER>(rp, o, dir, xyz(L), xyz(H), hi, aa)) {  // ray_box(o, dir, root) < hi, exactly
                 st.sp = 0;
                 st.cur = J.s.root_is_leaf ? -1 : (TRAV == FK_TRAVERSE_ORDERED4 ? J.root4 : J.root2);
                 st.pend = J.s.root_is_leaf ? (int32_t)J.node_base : -1;
@@ -1389,13 +1417,13 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
       const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
       const bool visited =
-          leaf_phase && leaf_phase_warp<false, FILTER, true>(s, rp, lo, hi, best, st, active, skey, tally);
+          leaf_phase && leaf_phase_warp<false, FILTER, 256, true>(s, rp, wray, lo, hi, best, st, active, skey, tally);
       if (active) {
         bool fin = false;
         if (leaf_phase) {
           if (visited) fin = settled<STOP>(best, hi);
         } else if (st.cur >= 0 && (st.pend < 0 || (p.speculate && spec_ok))) {
-          if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally))
+          if (!visit_inner<TRAV, false, FILTER, 256>(s, rp, myray, fminf(best, hi), st, stk, p.status, tally))
             fin = true;
           for (int v = 1; v < kInnerVisits && !fin; ++v) {  // as in hemi_trace_kernel
             if (st.cur < 0 && st.pend < 0 && !pop<FILTER>(st, stk, fminf(best, hi))) {
@@ -1403,7 +1431,8 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
               break;
             }
             if (!(st.cur >= 0 && (st.pend < 0 || (p.speculate && st.sp < kStack - 4)))) break;
-            if (!visit_inner<TRAV, false, FILTER>(s, rp, fminf(best, hi), st, stk, p.status, tally)) fin = true;
+            if (!visit_inner<TRAV, false, FILTER, 256>(s, rp, myray, fminf(best, hi), st, stk, p.status, tally))
+              fin = true;
           }
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, hi));
@@ -1413,7 +1442,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
         }
       }
     } else if (active) {
-      if (skip_step<STOP, false, FILTER>(s, rp, lo, hi, best, cur, tally) || (uint32_t)cur >= end) {
+      if (skip_step<STOP, false, FILTER, 256>(s, rp, myray, lo, hi, best, cur, tally) || (uint32_t)cur >= end) {
         p.scratch[slot] = best;
         active = false;
       }
