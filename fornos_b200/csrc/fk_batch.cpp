@@ -1,10 +1,14 @@
 // Batched bakes and the traversal autotuner.
 //
 // A batch is a set of hemisphere-sampling jobs, each with its own scene,
-// mapped texels, sample table, parameters and output buffers, that share
-// one persistent launch: their rays are laid end to end in one 64-bit ray
-// space (chunked at texel boundaries to fit the scratch), and every lane maps
-// its ray back to its job.  The launches of a run can be recorded once into a
+// mapped texels, sample table, parameters and output buffers.  Jobs smaller
+// than one chunk (2^27 rays) share persistent launches: their rays are laid
+// end to end in one 64-bit ray space (chunked at texel boundaries to fit the
+// scratch), and every lane maps its ray back to its job, so small jobs fill
+// the GPU together instead of each paying a launch and its tail.  A job of a
+// chunk or more gains nothing from sharing and runs alone through the
+// single-job path (its launches' tails are a small part of its time), on the
+// batch's scratch, in the same run and the same graph.  The launches of a run can be recorded once into a
 // CUDA graph and replayed.  The autotuner times a strided sample of the
 // batch's rays (every job represented) for each candidate schedule and keeps
 // the fastest: ordered vs skip-pointer traversal, filtered vs divided box
@@ -24,6 +28,12 @@ struct Chunk {
 
 constexpr unsigned long long kMaxChunkRays = 1ull << 27;  // 512 MB of distances
 
+// A job run alone (fk_batch's `solo`): its scene and its launch.
+struct Solo {
+  const fk_scene* scene;
+  fk::HemiLaunch h;
+};
+
 }  // namespace
 
 struct fk_batch {
@@ -37,6 +47,8 @@ struct fk_batch {
   float* scratch = nullptr;
   unsigned long long scratch_rays = 0;
   std::vector<Chunk> chunks;
+  std::vector<Solo> solo;                 // jobs of at least kMaxChunkRays rays, run alone
+  uint64_t solo_launches = 0;             // kernel launches of the solo jobs in one run
   int traverse = FK_TRAVERSE_ORDERED;     // tuned choice
   bool ordered_ok = true;                 // every tree fits the 2-wide ordered traversal's stack
   bool ordered4_ok = true;                // every collapsed tree fits the 4-wide traversal's stack
@@ -54,6 +66,21 @@ static bool fits(const fk_buf* b, uint64_t bytes) { return b && b->bytes >= byte
 
 static int batch_run_chunks(fk_batch* b, int trav, bool filter, const fk_tuning& tun) {
   fk_ctx* ctx = b->ctx;
+  if (!b->solo.empty()) {
+    // the solo jobs take the batch's schedule: the context's tuning for the duration of their launches
+    const fk_tuning saved = ctx->tuning;
+    const uint64_t before = ctx->launches;
+    ctx->tuning = tun;
+    int rc = FK_OK;
+    for (Solo& j : b->solo) {
+      if (rc != FK_OK) break;
+      j.h.traverse = trav | FK_SCHEDULE_DYNAMIC | (filter && b->filter_ok ? 0 : FK_EXACT_BOX_TESTS);
+      rc = fk::launch_hemisphere(ctx, j.scene, j.h);
+    }
+    ctx->tuning = saved;
+    if (rc != FK_OK) return rc;
+    b->solo_launches = ctx->launches - before;
+  }
   for (size_t c = 0; c < b->chunks.size(); ++c) {
     const Chunk& ch = b->chunks[c];
     FK_CUDA(ctx, cudaMemsetAsync(b->queues + c, 0, sizeof(unsigned long long), ctx->stream));
@@ -195,10 +222,36 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   b->njobs = njobs;
   b->total_rays = rays;
   b->total_texels = (uint32_t)texels;
-  // chunks at texel boundaries, at most kMaxChunkRays rays each
+  // chunks at texel boundaries, at most kMaxChunkRays rays each, over the
+  // jobs that share launches; a solo job's rays and texels are stepped over
   Chunk cur = {0, 0, 0, 0};
   for (uint32_t i = 0; i < njobs; ++i) {
     const fk::BatchJobDev& d = table[i];
+    const unsigned long long job_rays = (unsigned long long)d.texels * d.spp;
+    if (job_rays >= kMaxChunkRays) {
+      if (cur.t1 > cur.t0) b->chunks.push_back(cur);
+      cur = {cur.r1 + job_rays, cur.r1 + job_rays, cur.t1 + d.texels, cur.t1 + d.texels};
+      const fk_batch_job& J = jobs[i];
+      Solo so;
+      so.scene = J.scene;
+      so.h.kind = kind;
+      so.h.spp = J.params.sample_count;
+      so.h.perms = J.params.perm_count;
+      so.h.min_d = J.params.min_distance;
+      so.h.max_d = J.params.max_distance;
+      so.h.samples = d.samples;
+      so.h.coords = d.coords;
+      so.h.tidx = d.tidx;
+      so.h.offset = 0;
+      so.h.count = d.texels;
+      so.h.traverse = 0;
+      so.h.out0 = d.out0;
+      so.h.out1 = d.out1;
+      so.h.hits0 = d.hits0;
+      so.h.hits1 = d.hits1;
+      b->solo.push_back(so);
+      continue;
+    }
     uint32_t t = 0;
     while (t < d.texels) {
       unsigned long long room = (kMaxChunkRays - (cur.r1 - cur.r0)) / d.spp;
@@ -215,6 +268,10 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   }
   if (cur.t1 > cur.t0) b->chunks.push_back(cur);
   b->scratch_rays = std::min<unsigned long long>(std::max<unsigned long long>(rays, 1), kMaxChunkRays);
+  for (Solo& j : b->solo) {
+    j.h.scratch = nullptr;  // set once the scratch exists (below)
+    j.h.scratch_rays = b->scratch_rays;
+  }
   int rc = fk_dev_alloc(ctx, (void**)&b->jobs, sizeof(fk::BatchJobDev) * njobs);
   // the concatenated scene: nodes (lo, hi, jump), corners (positions, normals), triangle records, both layouts
   const size_t cat_bytes[7] = {16 * (size_t)nodes, 16 * (size_t)nodes, 4 * (size_t)nodes, 16 * (size_t)corners,
@@ -240,6 +297,7 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   }
   if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->queues, sizeof(unsigned long long) * (b->chunks.size() + 1));
   if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->scratch, sizeof(float) * b->scratch_rays);
+  for (Solo& j : b->solo) j.h.scratch = b->scratch;
   if (rc == FK_OK) {
     cudaError_t e = cudaMemcpyAsync(b->jobs, table.data(), sizeof(fk::BatchJobDev) * njobs, cudaMemcpyHostToDevice,
                                     ctx->stream);
@@ -266,7 +324,13 @@ int fk_batch_info(const fk_batch* b, uint64_t* rays, uint32_t* texels, uint32_t*
   if (!b) return FK_ERR_INVALID;
   if (rays) *rays = b->total_rays;
   if (texels) *texels = b->total_texels;
-  if (launches_per_run) *launches_per_run = (uint32_t)(2 * b->chunks.size());
+  // a solo job launches its trace and fold per chunk of its texels
+  uint64_t solo = 0;
+  for (const Solo& j : b->solo) {
+    const uint64_t per = std::max<uint64_t>(1, std::min<uint64_t>(1ull << 27, b->scratch_rays) / j.h.spp);
+    solo += 2 * ((j.h.count + per - 1) / per);
+  }
+  if (launches_per_run) *launches_per_run = (uint32_t)(2 * b->chunks.size() + solo);
   return FK_OK;
 }
 
@@ -293,7 +357,9 @@ int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int
     t.l2_persist = FK_L2_NONE;
     return t;
   };
-  for (uint32_t refill : {8u, 16u, 24u}) {
+  // the incumbent first: the batch's current schedule
+  cands.push_back({b->traverse, b->filter, b->tuning});
+  for (uint32_t refill : {8u, 16u, 20u, 24u}) {
     if (ordered_ok)
       for (uint32_t lb : {4u, 8u, 16u}) cands.push_back({FK_TRAVERSE_ORDERED, true, knobs(refill, lb, 1)});
     if (b->ordered4_ok)
@@ -309,11 +375,15 @@ int fk_batch_tune(fk_batch* b, uint64_t sample_rays, fk_tuning* best_tuning, int
   Cand best = cands[0];
   float warm = 0.0f;
   int rc = batch_time(b, stride, cands[0].trav, cands[0].filter, cands[0].t, &warm);  // warms caches and code
-  for (const Cand& c : cands) {
+  // A strided sample traces rays of scattered texels, unlike a whole run whose
+  // lanes share texels, so small differences on it do not carry over: a
+  // candidate replaces the incumbent only when at least 2 % faster.
+  for (size_t i = 0; i < cands.size(); ++i) {
     if (rc != FK_OK) break;
+    const Cand& c = cands[i];
     float ms = 0.0f;
     rc = batch_time(b, stride, c.trav, c.filter, c.t, &ms);
-    if (rc == FK_OK && ms < best_ms) {
+    if (rc == FK_OK && (i == 0 || ms < 0.98f * best_ms)) {
       best_ms = ms;
       best = c;
     }
@@ -368,7 +438,7 @@ int fk_batch_replay(fk_batch* b) {
   if (!b) return FK_ERR_INVALID;
   if (!b->exec) return fk_fail(b->ctx, FK_ERR_STATE, "fk_batch_replay: nothing captured");
   FK_CUDA(b->ctx, cudaGraphLaunch(b->exec, b->ctx->stream));
-  b->ctx->launches += 2 * b->chunks.size();
+  b->ctx->launches += 2 * b->chunks.size() + b->solo_launches;
   return FK_OK;
 }
 

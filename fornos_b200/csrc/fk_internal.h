@@ -259,6 +259,10 @@ struct HemiLaunch {
   // texel_limit are skipped and flag status bit 4.
   const uint32_t* ids = nullptr;
   uint32_t texel_limit = 0;
+  // Per-ray distances in this buffer of scratch_rays floats instead of the
+  // context's scratch (which may have to grow); at least one texel's rays.
+  float* scratch = nullptr;
+  unsigned long long scratch_rays = 0;
 };
 int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h);
 // Same kernels over caller-provided scratch: `dist` holds count x spp floats,

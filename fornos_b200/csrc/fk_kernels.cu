@@ -371,6 +371,8 @@ static int run_hemi(fk_ctx* ctx, const HemiArgs& a) {
 // What a dynamic trace launch adds beyond its arguments: staged top records
 // and a persisting L2 window (fk_tuning.top_records / l2_persist).
 struct TraceExtras {
+  float* scratch = nullptr;  // the caller's per-ray scratch (HemiLaunch::scratch), or null
+  unsigned long long scratch_rays = 0;
   uint32_t odepth = 0;  // levels of the tree walked
   const float4* top = nullptr;
   uint32_t top_count = 0, top_base = 0xFFFFFFFFu;
@@ -434,6 +436,8 @@ int launch_hemisphere(fk_ctx* ctx, const fk_scene* s, const HemiLaunch& h) {
   const uint32_t speculate = h.speculate ? h.speculate : ctx->tuning.speculate;
   TraceExtras x;
   x.odepth = s->odepth;
+  x.scratch = h.scratch;
+  x.scratch_rays = h.scratch_rays;
   if (sched == FK_SCHEDULE_DYNAMIC && trav == FK_TRAVERSE_ORDERED && ctx->tuning.top_records && !h.tally) {
     fk_scene* ms = const_cast<fk_scene*>(s);
     const int rc = ensure_top(ctx, ms, ctx->tuning.top_records);
@@ -740,11 +744,12 @@ __device__ __forceinline__ float dist_unkey(uint32_t k) {
 // candidates) changes it.  All lanes of the warp call this; returns whether
 // this lane visited a leaf.  MULTI: lanes may trace different jobs of a
 // batch, whose scenes lie in one concatenated array but whose distance
-// ranges differ, so the owner's minimum distance travels with its ray.
+// ranges differ, so the owner's minimum distance is read from `wlo` (the
+// warp's lanes' minimum distances in shared memory).
 template <bool COUNT, bool FILTER, int S, bool MULTI = false>
 __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre& rp, const float* wray, float lo,
                                                 float hi, float& best, OState& st, bool active, uint32_t* skey,
-                                                Tally& tally) {
+                                                Tally& tally, const float* wlo = nullptr) {
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   uint32_t first = 0, cnt = 0;
@@ -786,7 +791,7 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
     const uint32_t tri = __shfl_sync(full, first, o) + (j - __shfl_sync(full, excl, o));
     const float4* rec = s.rec;
     float olo = lo;
-    if (MULTI) olo = __shfl_sync(full, lo, o);
+    if (MULTI) olo = wlo[o];
     if (j < total) {
       float b = ob;
       tri_sample(rec, tri, ro, rd, olo, b);
@@ -862,6 +867,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
   __shared__ uint32_t leaf_keys[BLOCK / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   __shared__ float srays[6 * BLOCK];  // the lanes' ray origins and directions (ray_put)
+  __shared__ uint32_t sslot[BLOCK];   // scratch slot of each lane's ray: its texel's row, its sample
   float* const myray = srays + threadIdx.x;
   const float* const wray = srays + (threadIdx.x & ~31u);
   extern __shared__ float4 top_smem[];  // p.top_count staged records (TOP)
@@ -872,7 +878,6 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
   const uint32_t top_base = TOP ? p.top_base : 0xFFFFFFFFu;
   Tally tally;
   bool active = false, exhausted = false;
-  uint32_t slot = 0;  // scratch slot of the lane's ray: its texel's row, its sample
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
   float best = FLT_MAX;
   int32_t cur = 0;  // skip walk: node index
@@ -897,7 +902,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
           const uint32_t tq = r / p.spp;  // texel of the ray within the launch
           const uint32_t q = r - tq * p.spp;
           const uint32_t k = p.sectors > 1 ? (q & 31u) * p.sectors + (q >> 5) : q;
-          slot = r - q + k;
+          const uint32_t slot = r - q + k;
           const uint32_t g = list_texel(p.ids, p.texel_limit, p.texel0 + tq, p.status);
           const uint32_t id = g == kMiss ? kMiss : __ldg(p.tidx + g);
           best = FLT_MAX;
@@ -932,6 +937,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
           }
           if (done) p.scratch[slot] = best;
           else active = true;
+          sslot[threadIdx.x] = slot;
         }
       }
       idle = __ballot_sync(full, !active);
@@ -975,13 +981,13 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, p.hi));
         if (fin) {
-          p.scratch[slot] = best;
+          p.scratch[sslot[threadIdx.x]] = best;
           active = false;
         }
       }
     } else if (active) {
       if (skip_step<STOP, COUNT, FILTER, BLOCK>(p.s, rp, myray, p.lo, p.hi, best, cur, tally)) {
-        p.scratch[slot] = best;
+        p.scratch[sslot[threadIdx.x]] = best;
         active = false;
       }
     }
@@ -1225,9 +1231,11 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
   if (e != cudaSuccess) return fk_cuda_fail(ctx, e, "occupancy");
   if (per_sm < 1) per_sm = 1;
   // Scratch: one float per ray, texels processed in chunks that fit it.
-  const uint64_t max_rays = 1ull << 27;  // 512 MB of distances
+  const uint64_t max_rays = x.scratch ? std::min<uint64_t>(1ull << 27, x.scratch_rays) : 1ull << 27;  // 512 MB
   uint32_t chunk = (uint32_t)std::min<uint64_t>(a.count, std::max<uint64_t>(1, max_rays / a.spp));
-  float* scratch = (float*)fk_scratch(ctx, (size_t)chunk * a.spp * sizeof(float));
+  if (x.scratch && (uint64_t)chunk * a.spp > x.scratch_rays)
+    return fk_fail(ctx, FK_ERR_INVALID, "hemisphere: the given scratch holds less than one texel's rays");
+  float* scratch = x.scratch ? x.scratch : (float*)fk_scratch(ctx, (size_t)chunk * a.spp * sizeof(float));
   if (!scratch) return fk_fail(ctx, FK_ERR_NOMEM, "hemisphere scratch allocation failed");
   for (uint32_t done = 0; done < a.count; done += chunk) {
     uint32_t n = std::min(chunk, a.count - done);
@@ -1307,16 +1315,22 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
   // the job table is read at ray set-up only (through the cache): node visits
   // need nothing per job, since the scenes are concatenated
   const BatchJobDev* __restrict__ jobs = p.jobs;
-  // The lane's job: found once for the launch's first ray by binary search,
-  // then advanced, since a lane's rays come from the queue in increasing order
-  // (usually no step, so ray set-up adds no chain of dependent loads).
-  int job = 0;
+  // Per-lane state read only at ray set-up, at a ray's end or in the leaf
+  // phase lives in shared memory, so that registers serve the traversal: the
+  // lane's job (found once for the launch's first ray by binary search, then
+  // advanced, since a lane's rays come from the queue in increasing order), its
+  // ray's scratch slot and minimum distance.
+  __shared__ int sjob[256];
+  __shared__ uint32_t sslot[256];
+  __shared__ float slo[256];
   {
-    int b = (int)p.njobs - 1;  // last job whose ray_base <= r0
+    int job = 0, b = (int)p.njobs - 1;  // last job whose ray_base <= r0
     while (job < b) {
       const int m = (job + b + 1) >> 1;
       if (jobs[m].ray_base <= p.r0) job = m; else b = m - 1;
     }
+    sjob[threadIdx.x] = job;
+    slo[threadIdx.x] = 0.0f;
   }
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
@@ -1331,9 +1345,8 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
   const float* const wray = srays + (threadIdx.x & ~31u);
   Tally tally;
   bool active = false, exhausted = false;
-  uint32_t slot = 0;  // scratch slot of the lane's ray (its sample's, in sample order)
   RayPre rp = ray_pre(mk3(0.0f, 0.0f, 0.0f), mk3(1.0f, 1.0f, 1.0f));
-  float best = FLT_MAX, lo = 0.0f, hi = 0.0f;
+  float best = FLT_MAX, hi = 0.0f;
   int32_t cur = 0;
   uint32_t end = 0;  // skip walk: one past the job's last node
   OState st = {-1, -1, 0};
@@ -1351,7 +1364,9 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
         const uint32_t q = base + __popc(idle & lower);
         if (q < total) {
           const unsigned long long r = p.r0 + (unsigned long long)q * p.stride;
+          int job = sjob[threadIdx.x];
           while (job + 1 < (int)p.njobs && jobs[job + 1].ray_base <= r) ++job;
+          sjob[threadIdx.x] = job;
           const BatchJobDev& J = jobs[job];
           const unsigned long long local = r - J.ray_base;
           // texel and sample of the ray within its job: 32-bit division when the
@@ -1364,7 +1379,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
             g = (uint32_t)(local / J.spp);
             k = (uint32_t)(local - (unsigned long long)g * J.spp);
           }
-          slot = q;
+          uint32_t slot = q;
           if (p.ray_order == FK_RAY_ORDER_SECTOR && p.stride == 1 && J.spp >= 64 && (J.spp & 31u) == 0) {
             // queue slot k of the texel traces sample (k % 32) * (spp / 32) + k / 32
             const uint32_t ks = (k & 31u) * (J.spp >> 5) + (k >> 5);
@@ -1373,7 +1388,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
           }
           const uint32_t id = __ldg(J.tidx + g);
           best = FLT_MAX;
-          lo = J.lo;
+          slo[threadIdx.x] = J.lo;
           hi = J.hi;
           bool done = true;
           if (id != kMiss && valid_hit(id, J.s.corner_count)) {
@@ -1406,6 +1421,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
           }
           if (done) p.scratch[slot] = best;
           else active = true;
+          sslot[threadIdx.x] = slot;
         }
       }
       idle = __ballot_sync(full, !active);
@@ -1417,7 +1433,8 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
       const unsigned leaves = __ballot_sync(full, active && st.pend >= 0);
       const bool leaf_phase = need == 0 || (uint32_t)__popc(leaves) >= p.leaf_batch;
       const bool visited =
-          leaf_phase && leaf_phase_warp<false, FILTER, 256, true>(s, rp, wray, lo, hi, best, st, active, skey, tally);
+          leaf_phase && leaf_phase_warp<false, FILTER, 256, true>(s, rp, wray, 0.0f, hi, best, st, active, skey,
+                                                                  tally, slo + (threadIdx.x & ~31u));
       if (active) {
         bool fin = false;
         if (leaf_phase) {
@@ -1437,13 +1454,14 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
         }
         if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, hi));
         if (fin) {
-          p.scratch[slot] = best;
+          p.scratch[sslot[threadIdx.x]] = best;
           active = false;
         }
       }
     } else if (active) {
-      if (skip_step<STOP, false, FILTER, 256>(s, rp, myray, lo, hi, best, cur, tally) || (uint32_t)cur >= end) {
-        p.scratch[slot] = best;
+      if (skip_step<STOP, false, FILTER, 256>(s, rp, myray, slo[threadIdx.x], hi, best, cur, tally) ||
+          (uint32_t)cur >= end) {
+        p.scratch[sslot[threadIdx.x]] = best;
         active = false;
       }
     }

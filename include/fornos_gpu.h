@@ -420,10 +420,12 @@ int fk_solver_free(fk_solver* s);
 /* ------------------------------------------------------------ batched bakes
  * No counterpart in the reference (which bakes one mesh pair at a time, one
  * chunk per UI frame).  Up to 64 hemisphere jobs, each with its own scene,
- * mapped texels, sample table, parameters and outputs, share one persistent
- * launch: their rays are laid end to end and every lane maps its ray back to
- * its job, so small and large jobs keep the whole GPU busy together.  Results
- * are those fk_hemisphere gives per job. */
+ * mapped texels, sample table, parameters and outputs.  Jobs of fewer than
+ * 2^27 rays share persistent launches: their rays are laid end to end and
+ * every lane maps its ray back to its job, so small jobs keep the whole GPU
+ * busy together.  A job of 2^27 rays or more runs alone through the
+ * single-job path within the same run (and the same graph), on the batch's
+ * scratch.  Results are those fk_hemisphere gives per job. */
 typedef struct fk_batch fk_batch;
 typedef struct fk_batch_job {
   const fk_scene* scene;

@@ -109,3 +109,39 @@ def test_autotuner_choice_gives_same_results(ctx, setup):
     ctx.set_tuning(**tun)
     assert trav & api.SCHEDULE_DYNAMIC
     ctx.set_tuning(refill=8, leaf_batch=8, speculate=0)
+
+
+def test_batch_with_a_job_run_alone(ctx, setup):
+    """A job of at least 2^27 rays runs alone through the single-job path in
+    the batch's run (and in its graph), beside jobs that share launches; every
+    job still gets what fk_hemisphere gives it alone."""
+    big = dict(setup[0], spp=1 << 16, perms=8)
+    big["samples"] = ctx.upload(api.samples_cosine(big["spp"], 8, 7))
+    assert big["texel_count"] * big["spp"] >= 1 << 27
+    jobs = [setup[1], big, setup[3]]
+    kind = api.AO_BN
+
+    def alone_p(j):
+        n = j["texel_count"]
+        o0, o1, h0, h1 = ctx.buffer(12 * n), ctx.buffer(12 * n), ctx.buffer(4 * n), ctx.buffer(4 * n)
+        api.hemisphere(ctx, j["scene"], j["coords"], j["tidx"], kind, j["spp"], j["min_distance"],
+                       j["max_distance"], j["samples"], o0, o1, h0, h1, 0, n, perms=j.get("perms", api.PERMS),
+                       traverse=api.TRAVERSE_ORDERED | api.SCHEDULE_DYNAMIC)
+        return read(o0, o1, h0, h1, n, kind)
+
+    want = [alone_p(j) for j in jobs]
+    b, outs = make_batch(ctx, jobs, kind)
+    launches = b.info()["launches_per_run"]
+    before = ctx.launches
+    b.run(api.TRAVERSE_ORDERED)
+    ctx.sync()
+    assert ctx.launches - before == launches
+    check(jobs, outs, kind, want)
+    b.capture(api.TRAVERSE_ORDERED)
+    for o in outs:
+        for buf in o:
+            buf.upload(np.zeros(buf.nbytes, np.uint8))
+    b.replay()
+    ctx.sync()
+    ctx.check()
+    check(jobs, outs, kind, want)
