@@ -1105,82 +1105,67 @@ int ensure_top(fk_ctx* ctx, fk_scene* s, uint32_t want) {
 }
 
 // Folds each texel's per-sample distances in sample order (the *_step2
-// shaders' sequential sums), one warp per texel.
+// shaders' sequential sums), one thread per texel: a thread walks its
+// texel's samples 0 .. spp-1 and adds each sample's term as the shader does
+// (a bent-normal term of zero for a hit), so the sums are the shader's bit for
+// bit, and the 32 lanes of a warp fold 32 texels at once.
 template <int KIND>
 __global__ void __launch_bounds__(256) hemi_reduce_kernel(HemiArgs p, const float* __restrict__ scratch,
                                                           uint32_t texel0) {
-  const unsigned full = 0xFFFFFFFFu;
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < p.count; item += warps) {
-    uint32_t g = texel0 + item;
-    if (p.ids) {
-      g = __ldg(p.ids + g);
-      if (g >= p.texel_limit) continue;  // reported by the trace kernel
+  const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+  if (item >= p.count) return;
+  uint32_t g = texel0 + item;
+  if (p.ids) {
+    g = __ldg(p.ids + g);
+    if (g >= p.texel_limit) return;  // reported by the trace kernel
+  }
+  uint32_t id = __ldg(p.tidx + g);
+  if (id != kMiss && !valid_hit(id, p.s.corner_count)) id = kMiss;
+  float* bn = KIND == FK_BN ? p.out0 : (KIND == FK_AO_BN ? p.out1 : nullptr);
+  if (id == kMiss) {
+    if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = 1.0f;
+    if (KIND == FK_THICK) p.out0[g] = p.hi;
+    if (bn) { bn[3 * (size_t)g] = 0.0f; bn[3 * (size_t)g + 1] = 0.0f; bn[3 * (size_t)g + 2] = 0.0f; }
+    if (p.hits0) p.hits0[g] = 0;
+    if (p.hits1) p.hits1[g] = 0;
+    return;
+  }
+  f3 o, d, tx, ty;
+  if (KIND == FK_BN || KIND == FK_AO_BN) texel_frame(p.s, __ldg(p.coords + g), id, o, d, tx, ty);
+  const float4* row = p.samples + (size_t)(g % p.perms) * p.spp;
+  const float* ts = scratch + (size_t)item * p.spp;
+  uint32_t occ = 0, anyhit = 0;
+  float acc = 0.0f;
+  f3 vacc = mk3(0.0f, 0.0f, 0.0f);
+  for (uint32_t k = 0; k < p.spp; ++k) {
+    const float t = __ldg(ts + k);
+    const bool hit = t != FLT_MAX;
+    if (KIND == FK_AO || KIND == FK_AO_BN) occ += (hit && t < p.hi) ? 1u : 0u;
+    anyhit += hit ? 1u : 0u;
+    if (KIND == FK_BN || KIND == FK_AO_BN) {
+      f3 v = mk3(0.0f, 0.0f, 0.0f);
+      if (!hit) {
+        const float4 rs = __ldg(row + k);
+        v = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+      }
+      vacc = add(vacc, v);
     }
-    uint32_t id = __ldg(p.tidx + g);
-    if (id != kMiss && !valid_hit(id, p.s.corner_count)) id = kMiss;
-    if (id == kMiss) {
-      if (lane == 0) {
-        if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = 1.0f;
-        if (KIND == FK_THICK) p.out0[g] = p.hi;
-        float* bn = KIND == FK_BN ? p.out0 : (KIND == FK_AO_BN ? p.out1 : nullptr);
-        if (bn) { bn[3 * (size_t)g] = 0.0f; bn[3 * (size_t)g + 1] = 0.0f; bn[3 * (size_t)g + 2] = 0.0f; }
-        if (p.hits0) p.hits0[g] = 0;
-        if (p.hits1) p.hits1[g] = 0;
-      }
-      continue;
-    }
-    f3 o, d, tx, ty;
-    if (KIND == FK_BN || KIND == FK_AO_BN) texel_frame(p.s, __ldg(p.coords + g), id, o, d, tx, ty);
-    const float4* row = p.samples + (size_t)(g % p.perms) * p.spp;
-    const float* ts = scratch + (size_t)item * p.spp;
-    uint32_t occ = 0, anyhit = 0;
-    float acc = 0.0f;
-    f3 vacc = mk3(0.0f, 0.0f, 0.0f);
-    for (uint32_t k0 = 0; k0 < p.spp; k0 += 32) {
-      const uint32_t k = k0 + lane;
-      const bool active = k < p.spp;
-      const float t = active ? ts[k] : FLT_MAX;
-      const bool hit = active && t != FLT_MAX;
-      if (KIND == FK_AO || KIND == FK_AO_BN) occ += __popc(__ballot_sync(full, hit && t < p.hi));
-      anyhit += __popc(__ballot_sync(full, hit));
-      const int nact = (int)min(32u, p.spp - k0);
-      if (KIND == FK_BN || KIND == FK_AO_BN) {
-        f3 v = mk3(0.0f, 0.0f, 0.0f);
-        if (active && !hit) {
-          float4 rs = __ldg(row + k);
-          v = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
-        }
-        for (int j = 0; j < nact; ++j) {
-          vacc.x = __fadd_rn(vacc.x, __shfl_sync(full, v.x, j));
-          vacc.y = __fadd_rn(vacc.y, __shfl_sync(full, v.y, j));
-          vacc.z = __fadd_rn(vacc.z, __shfl_sync(full, v.z, j));
-        }
-      }
-      if (KIND == FK_THICK) {
-        float v = hit ? t : p.hi;
-        for (int j = 0; j < nact; ++j) acc = __fadd_rn(acc, __shfl_sync(full, v, j));
-      }
-    }
-    if (lane == 0) {
-      const float fs = (float)p.spp;
-      if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = __fsub_rn(1.0f, __fdiv_rn((float)occ, fs));
-      if (KIND == FK_THICK) p.out0[g] = __fdiv_rn(acc, fs);
-      if (KIND == FK_BN || KIND == FK_AO_BN) {
-        float* bn = KIND == FK_BN ? p.out0 : p.out1;
-        f3 v = normalize(vacc);
-        bn[3 * (size_t)g] = v.x;
-        bn[3 * (size_t)g + 1] = v.y;
-        bn[3 * (size_t)g + 2] = v.z;
-      }
-      if (KIND == FK_AO_BN) {
-        if (p.hits0) p.hits0[g] = occ;
-        if (p.hits1) p.hits1[g] = anyhit;
-      } else if (p.hits0) {
-        p.hits0[g] = KIND == FK_AO ? occ : anyhit;
-      }
-    }
+    if (KIND == FK_THICK) acc = __fadd_rn(acc, hit ? t : p.hi);
+  }
+  const float fs = (float)p.spp;
+  if (KIND == FK_AO || KIND == FK_AO_BN) p.out0[g] = __fsub_rn(1.0f, __fdiv_rn((float)occ, fs));
+  if (KIND == FK_THICK) p.out0[g] = __fdiv_rn(acc, fs);
+  if (KIND == FK_BN || KIND == FK_AO_BN) {
+    const f3 v = normalize(vacc);
+    bn[3 * (size_t)g] = v.x;
+    bn[3 * (size_t)g + 1] = v.y;
+    bn[3 * (size_t)g + 2] = v.z;
+  }
+  if (KIND == FK_AO_BN) {
+    if (p.hits0) p.hits0[g] = occ;
+    if (p.hits1) p.hits1[g] = anyhit;
+  } else if (p.hits0) {
+    p.hits0[g] = KIND == FK_AO ? occ : anyhit;
   }
 }
 
@@ -1291,8 +1276,7 @@ static int run_hemi_dynamic(fk_ctx* ctx, const HemiArgs& a, uint32_t refill, boo
     if (rc != FK_OK) return rc;
     HemiArgs r = a;
     r.count = n;
-    uint32_t rblocks = std::min<uint32_t>((n + 7) / 8, (uint32_t)ctx->sm_count * 8);
-    hemi_reduce_kernel<KIND><<<rblocks, 256, 0, ctx->stream>>>(r, scratch, d.texel0);
+    hemi_reduce_kernel<KIND><<<(n + 255) / 256, 256, 0, ctx->stream>>>(r, scratch, d.texel0);
     rc = fk_after_launch(ctx, "hemi_reduce_kernel");
     if (rc != FK_OK) return rc;
   }
@@ -1544,87 +1528,70 @@ int concat_batch_scene(cudaStream_t st, const fk_scene* s, uint32_t node_base, u
   return FK_OK;
 }
 
-// Per-texel folds for a batch chunk: global texels [t0, t1), one warp each.
+// Per-texel folds for a batch chunk: global texels [t0, t1), one thread each,
+// in sample order as hemi_reduce_kernel folds them.
 template <int KIND>
 __global__ void __launch_bounds__(256) batch_reduce_kernel(BatchArgs p) {
   __shared__ BatchJobDev jobs[kMaxBatchJobs];
   for (uint32_t i = threadIdx.x; i < p.njobs * (uint32_t)(sizeof(BatchJobDev) / 4); i += blockDim.x)
     ((uint32_t*)jobs)[i] = ((const uint32_t*)p.jobs)[i];
   __syncthreads();
-  const unsigned full = 0xFFFFFFFFu;
-  const int lane = threadIdx.x & 31;
-  const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t t = p.t0 + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); t < p.t1; t += warps) {
-    int a = 0, b = (int)p.njobs - 1;
-    while (a < b) {
-      int m = (a + b + 1) >> 1;
-      if (jobs[m].texel_base <= t) a = m; else b = m - 1;
+  const uint32_t t = p.t0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= p.t1) return;
+  int a = 0, b = (int)p.njobs - 1;
+  while (a < b) {
+    int m = (a + b + 1) >> 1;
+    if (jobs[m].texel_base <= t) a = m; else b = m - 1;
+  }
+  const BatchJobDev& J = jobs[a];
+  const uint32_t g = t - J.texel_base;
+  const float* ts = p.scratch + (J.ray_base + (unsigned long long)g * J.spp - p.r0);
+  uint32_t id = __ldg(J.tidx + g);
+  if (id != kMiss && !valid_hit(id, J.s.corner_count)) id = kMiss;
+  float* bn = KIND == FK_BN ? J.out0 : (KIND == FK_AO_BN ? J.out1 : nullptr);
+  if (id == kMiss) {
+    if (KIND == FK_AO || KIND == FK_AO_BN) J.out0[g] = 1.0f;
+    if (KIND == FK_THICK) J.out0[g] = J.hi;
+    if (bn) { bn[3 * (size_t)g] = 0.0f; bn[3 * (size_t)g + 1] = 0.0f; bn[3 * (size_t)g + 2] = 0.0f; }
+    if (J.hits0) J.hits0[g] = 0;
+    if (J.hits1) J.hits1[g] = 0;
+    return;
+  }
+  f3 o, d, tx, ty;
+  if (KIND == FK_BN || KIND == FK_AO_BN) texel_frame(J.s, __ldg(J.coords + g), id, o, d, tx, ty);
+  const float4* row = J.samples + (size_t)(g % J.perms) * J.spp;
+  uint32_t occ = 0, anyhit = 0;
+  float acc = 0.0f;
+  f3 vacc = mk3(0.0f, 0.0f, 0.0f);
+  for (uint32_t k = 0; k < J.spp; ++k) {
+    const float tk = __ldg(ts + k);
+    const bool hit = tk != FLT_MAX;
+    if (KIND == FK_AO || KIND == FK_AO_BN) occ += (hit && tk < J.hi) ? 1u : 0u;
+    anyhit += hit ? 1u : 0u;
+    if (KIND == FK_BN || KIND == FK_AO_BN) {
+      f3 v = mk3(0.0f, 0.0f, 0.0f);
+      if (!hit) {
+        const float4 rs = __ldg(row + k);
+        v = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
+      }
+      vacc = add(vacc, v);
     }
-    const BatchJobDev& J = jobs[a];
-    const uint32_t g = t - J.texel_base;
-    const float* ts = p.scratch + (J.ray_base + (unsigned long long)g * J.spp - p.r0);
-    uint32_t id = __ldg(J.tidx + g);
-    if (id != kMiss && !valid_hit(id, J.s.corner_count)) id = kMiss;
-    if (id == kMiss) {
-      if (lane == 0) {
-        if (KIND == FK_AO || KIND == FK_AO_BN) J.out0[g] = 1.0f;
-        if (KIND == FK_THICK) J.out0[g] = J.hi;
-        float* bn = KIND == FK_BN ? J.out0 : (KIND == FK_AO_BN ? J.out1 : nullptr);
-        if (bn) { bn[3 * (size_t)g] = 0.0f; bn[3 * (size_t)g + 1] = 0.0f; bn[3 * (size_t)g + 2] = 0.0f; }
-        if (J.hits0) J.hits0[g] = 0;
-        if (J.hits1) J.hits1[g] = 0;
-      }
-      continue;
-    }
-    f3 o, d, tx, ty;
-    if (KIND == FK_BN || KIND == FK_AO_BN) texel_frame(J.s, __ldg(J.coords + g), id, o, d, tx, ty);
-    const float4* row = J.samples + (size_t)(g % J.perms) * J.spp;
-    uint32_t occ = 0, anyhit = 0;
-    float acc = 0.0f;
-    f3 vacc = mk3(0.0f, 0.0f, 0.0f);
-    for (uint32_t k0 = 0; k0 < J.spp; k0 += 32) {
-      const uint32_t k = k0 + lane;
-      const bool on = k < J.spp;
-      const float tk = on ? ts[k] : FLT_MAX;
-      const bool hit = on && tk != FLT_MAX;
-      if (KIND == FK_AO || KIND == FK_AO_BN) occ += __popc(__ballot_sync(full, hit && tk < J.hi));
-      anyhit += __popc(__ballot_sync(full, hit));
-      const int nact = (int)min(32u, J.spp - k0);
-      if (KIND == FK_BN || KIND == FK_AO_BN) {
-        f3 v = mk3(0.0f, 0.0f, 0.0f);
-        if (on && !hit) {
-          float4 rs = __ldg(row + k);
-          v = normalize(add(add(scale(tx, rs.x), scale(ty, rs.y)), scale(d, rs.z)));
-        }
-        for (int i = 0; i < nact; ++i) {
-          vacc.x = __fadd_rn(vacc.x, __shfl_sync(full, v.x, i));
-          vacc.y = __fadd_rn(vacc.y, __shfl_sync(full, v.y, i));
-          vacc.z = __fadd_rn(vacc.z, __shfl_sync(full, v.z, i));
-        }
-      }
-      if (KIND == FK_THICK) {
-        float v = hit ? tk : J.hi;
-        for (int i = 0; i < nact; ++i) acc = __fadd_rn(acc, __shfl_sync(full, v, i));
-      }
-    }
-    if (lane == 0) {
-      const float fs = (float)J.spp;
-      if (KIND == FK_AO || KIND == FK_AO_BN) J.out0[g] = __fsub_rn(1.0f, __fdiv_rn((float)occ, fs));
-      if (KIND == FK_THICK) J.out0[g] = __fdiv_rn(acc, fs);
-      if (KIND == FK_BN || KIND == FK_AO_BN) {
-        float* bn = KIND == FK_BN ? J.out0 : J.out1;
-        f3 v = normalize(vacc);
-        bn[3 * (size_t)g] = v.x;
-        bn[3 * (size_t)g + 1] = v.y;
-        bn[3 * (size_t)g + 2] = v.z;
-      }
-      if (KIND == FK_AO_BN) {
-        if (J.hits0) J.hits0[g] = occ;
-        if (J.hits1) J.hits1[g] = anyhit;
-      } else if (J.hits0) {
-        J.hits0[g] = KIND == FK_AO ? occ : anyhit;
-      }
-    }
+    if (KIND == FK_THICK) acc = __fadd_rn(acc, hit ? tk : J.hi);
+  }
+  const float fs = (float)J.spp;
+  if (KIND == FK_AO || KIND == FK_AO_BN) J.out0[g] = __fsub_rn(1.0f, __fdiv_rn((float)occ, fs));
+  if (KIND == FK_THICK) J.out0[g] = __fdiv_rn(acc, fs);
+  if (KIND == FK_BN || KIND == FK_AO_BN) {
+    const f3 v = normalize(vacc);
+    bn[3 * (size_t)g] = v.x;
+    bn[3 * (size_t)g + 1] = v.y;
+    bn[3 * (size_t)g + 2] = v.z;
+  }
+  if (KIND == FK_AO_BN) {
+    if (J.hits0) J.hits0[g] = occ;
+    if (J.hits1) J.hits1[g] = anyhit;
+  } else if (J.hits0) {
+    J.hits0[g] = KIND == FK_AO ? occ : anyhit;
   }
 }
 
@@ -1643,7 +1610,7 @@ static cudaError_t batch_launch(const BatchArgs& a, cudaStream_t stream, int sm_
   if (blocks == 0) return cudaSuccess;
   trace<<<(uint32_t)blocks, 256, 0, stream>>>(a);
   if ((e = cudaGetLastError()) != cudaSuccess || !reduce) return e;
-  uint32_t rblocks = std::min<uint32_t>((a.t1 - a.t0 + 7) / 8, (uint32_t)sm_count * 8);
+  const uint32_t rblocks = (a.t1 - a.t0 + 255) / 256;
   if (rblocks) batch_reduce_kernel<KIND><<<rblocks, 256, 0, stream>>>(a);
   return cudaGetLastError();
 }
@@ -1713,8 +1680,7 @@ static cudaError_t run_hemi_external(const HemiArgs& a, cudaStream_t stream, int
   if (blocks > need) blocks = need;
   trace<<<blocks, 256, 0, stream>>>(d);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  uint32_t rblocks = std::min<uint32_t>((a.count + 7) / 8, (uint32_t)sm_count * 8);
-  hemi_reduce_kernel<KIND><<<rblocks, 256, 0, stream>>>(a, dist, a.offset);
+  hemi_reduce_kernel<KIND><<<(a.count + 255) / 256, 256, 0, stream>>>(a, dist, a.offset);
   return cudaGetLastError();
 }
 
