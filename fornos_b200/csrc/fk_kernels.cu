@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <type_traits>
 
 #include "fk_device.cuh"
 #include "fk_internal.h"
@@ -616,8 +617,25 @@ struct OState {
   int sp;
 };
 
-// Deferred entries are (ref, entry distance bits) pairs: one 8-byte access
-// per push or pop.
+// Deferred entries (SE): (ref, entry distance bits) pairs, one 8-byte
+// access per push or pop, when the distance can still cull the entry (the
+// closest-hit search, whose threshold min(best, max) shrinks as hits are
+// found); the ref alone otherwise.  A ray that stops at its first hit under
+// the maximum distance (AO, AO + bent normals) or at its first hit at all
+// (bent normals) keeps min(best, max) = max while it runs, so every entry
+// deferred below that threshold stays open and its distance is never read.
+template <typename SE>
+__device__ __forceinline__ SE stack_entry(int32_t r, float d);
+template <>
+__device__ __forceinline__ int2 stack_entry<int2>(int32_t r, float d) { return make_int2(r, __float_as_int(d)); }
+template <>
+__device__ __forceinline__ int32_t stack_entry<int32_t>(int32_t r, float) { return r; }
+__device__ __forceinline__ int32_t entry_ref(int2 e) { return e.x; }
+__device__ __forceinline__ int32_t entry_ref(int32_t e) { return e; }
+template <bool FILTER>
+__device__ __forceinline__ bool entry_open(int2 e, float thr) { return still_open<FILTER>(__int_as_float(e.y), thr); }
+template <bool FILTER>
+__device__ __forceinline__ bool entry_open(int32_t, float) { return true; }
 
 // Inner phase: tests both children of record `cur` against `thr` and takes
 // them nearer entry first.  Their roles are decided by selects, in the order
@@ -627,9 +645,9 @@ struct OState {
 // with one overflow check per visit.  Straight-line code keeps the visit free
 // of divergent branches.  TOP: records ref >= top_base are read from the
 // staged copies in shared memory.
-template <bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false>
+template <bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false, typename SE>
 __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
-                                            OState& st, int2* stk,
+                                            OState& st, SE* stk,
                                             int* status, Tally& tally, const float4* top = nullptr,
                                             uint32_t top_base = 0xFFFFFFFFu) {
   float4 w0, w1, w2, w3;
@@ -654,9 +672,9 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   const bool push_n = nl && !take_nl;
   const bool push_f = (fl && !take_fl) || (fi && ni);
   int sp = st.sp;
-  if (push_n && sp < STACK) stk[sp] = make_int2(rn, __float_as_int(dn));
+  if (push_n && sp < STACK) stk[sp] = stack_entry<SE>(rn, dn);
   sp += push_n;
-  if (push_f && sp < STACK) stk[sp] = make_int2(rf, __float_as_int(df));
+  if (push_f && sp < STACK) stk[sp] = stack_entry<SE>(rf, df);
   sp += push_f;
   st.pend = take_nl ? -rn - 1 : (take_fl ? -rf - 1 : st.pend);
   st.cur = ni ? rn : (fi ? rf : -1);
@@ -684,9 +702,9 @@ __device__ __forceinline__ void cex(float& ka, int32_t& ra, float& kb, int32_t& 
 // (a 5-comparator sorting network), keeps the nearest inner child as the next
 // node and the nearest leaf as the postponed leaf when none is held, and
 // defers the rest farthest first, so that the nearest is popped next.
-template <bool COUNT, bool FILTER, int S, int STACK = kStack>
+template <bool COUNT, bool FILTER, int S, int STACK = kStack, typename SE>
 __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
-                                             OState& st, int2* stk,
+                                             OState& st, SE* stk,
                                              int* status, Tally& tally) {
   const float4* w = s.wide4 + 8 * (size_t)st.cur;
   const float4 lx = __ldg(w), hx = __ldg(w + 1), ly = __ldg(w + 2), hy = __ldg(w + 3);
@@ -720,13 +738,13 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   const bool p3 = v3 && ni != 3 && keep != 3, p2 = v2 && ni != 2 && keep != 2;
   const bool p1 = v1 && ni != 1 && keep != 1, p0 = v0 && ni != 0 && keep != 0;
   int sp = st.sp;
-  if (p3 && sp < STACK) stk[sp] = make_int2(r3, __float_as_int(k3));
+  if (p3 && sp < STACK) stk[sp] = stack_entry<SE>(r3, k3);
   sp += p3;
-  if (p2 && sp < STACK) stk[sp] = make_int2(r2, __float_as_int(k2));
+  if (p2 && sp < STACK) stk[sp] = stack_entry<SE>(r2, k2);
   sp += p2;
-  if (p1 && sp < STACK) stk[sp] = make_int2(r1, __float_as_int(k1));
+  if (p1 && sp < STACK) stk[sp] = stack_entry<SE>(r1, k1);
   sp += p1;
-  if (p0 && sp < STACK) stk[sp] = make_int2(r0, __float_as_int(k0));
+  if (p0 && sp < STACK) stk[sp] = stack_entry<SE>(r0, k0);
   sp += p0;
   st.sp = sp;
   const int32_t rk = keep == 0 ? r0 : (keep == 1 ? r1 : (keep == 2 ? r2 : r3));
@@ -739,9 +757,9 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   return true;
 }
 
-template <int TRAV, bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false>
+template <int TRAV, bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false, typename SE>
 __device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
-                                            OState& st, int2* stk, int* status, Tally& tally,
+                                            OState& st, SE* stk, int* status, Tally& tally,
                                             const float4* top = nullptr, uint32_t top_base = 0xFFFFFFFFu) {
   if (TRAV == FK_TRAVERSE_ORDERED4)
     return inner_visit4<COUNT, FILTER, S, STACK>(s, rp, ray, thr, st, stk, status, tally);
@@ -831,16 +849,16 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
 }
 
 // Takes the nearest still-open deferred entry; false when none is left.
-template <bool FILTER>
-__device__ __forceinline__ bool pop(OState& st, const int2* stk, float thr) {
+template <bool FILTER, typename SE>
+__device__ __forceinline__ bool pop(OState& st, const SE* stk, float thr) {
   while (st.sp > 0) {
-    const int2 e = stk[--st.sp];
-    const float dist = __int_as_float(e.y);
-    if (!still_open<FILTER>(dist, thr)) continue;
-    if (e.x < 0) {
-      st.pend = -e.x - 1;
+    const SE e = stk[--st.sp];
+    if (!entry_open<FILTER>(e, thr)) continue;
+    const int32_t r = entry_ref(e);
+    if (r < 0) {
+      st.pend = -r - 1;
     } else {
-      st.cur = e.x;
+      st.cur = r;
     }
     return true;
   }
@@ -889,7 +907,8 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
-  int2 stk[is_ordered(TRAV) ? STACK : 1];  // deferred (ref, entry) pairs
+  using SE = typename std::conditional<STOP == kClosest, int2, int32_t>::type;
+  SE stk[is_ordered(TRAV) ? STACK : 1];  // deferred entries (stack_entry)
   __shared__ uint32_t leaf_keys[BLOCK / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   __shared__ float srays[6 * BLOCK];  // the lanes' ray origins and directions (ray_put)
@@ -1348,7 +1367,8 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
   const unsigned lower = (1u << lane) - 1u;
   // a launch traces at most the scratch's 2^27 rays: lane indices fit 32 bits
   const uint32_t total = (uint32_t)((p.r1 - p.r0 + p.stride - 1) / p.stride);
-  int2 stk[is_ordered(TRAV) ? kStack : 1];  // deferred (ref, entry) pairs
+  using SE = typename std::conditional<STOP == kClosest, int2, int32_t>::type;
+  SE stk[is_ordered(TRAV) ? kStack : 1];  // deferred entries (stack_entry)
   __shared__ uint32_t leaf_keys[256 / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   __shared__ float srays[6 * 256];  // the lanes' ray origins and directions (ray_put)
