@@ -285,6 +285,7 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
     b->cat.pos4 = (const float4*)b->cat_mem[3];
     b->cat.nrm4 = (const float4*)b->cat_mem[4];
     b->cat.rec = (const float4*)b->cat_mem[5];
+    b->cat.rec_bary = b->cat.rec + corners / 3;  // the planes of every job's triangles, then their barycentric terms
     b->cat.wide = (const float4*)b->cat_mem[6];
     b->cat.node_count = (uint32_t)nodes;
     b->cat.corner_count = (uint32_t)corners;

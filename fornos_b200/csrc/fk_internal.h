@@ -137,7 +137,11 @@ struct SceneDev {
   const float4* __restrict__ nrm4;
   const float4* __restrict__ wide;
   const float4* __restrict__ wide4;
+  // Triangle records in two blocks: rec[t] = (n, a.n), read by every
+  // triangle test; rec_bary[3 t .. 3 t + 2] = (a, d01), (v0, d00), (v1, d11),
+  // read only for hits inside the distance range.
   const float4* __restrict__ rec;
+  const float4* __restrict__ rec_bary;
   uint32_t node_count;
   uint32_t root_is_leaf;
   uint32_t corner_count;

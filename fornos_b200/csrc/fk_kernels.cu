@@ -18,7 +18,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <type_traits>
 
 #include "fk_device.cuh"
 #include "fk_internal.h"
@@ -41,6 +40,7 @@ static SceneDev dev_of(const fk_scene* s) {
   d.wide = s->wide;
   d.wide4 = s->wide4;
   d.rec = s->tri_rec;
+  d.rec_bary = s->tri_rec + s->corner_count / 3;
   d.node_count = s->node_count;
   d.root_is_leaf = s->root_is_leaf;
   d.corner_count = s->corner_count;
@@ -53,7 +53,10 @@ __device__ __forceinline__ uint32_t as_u32(float f) { return __float_as_uint(f);
 // ------------------------------------------------------------------ records
 // Per triangle (a, b, c): n = normalize(cross(b - a, c - a)) and dot(a, n) as
 // Shaders/ao_step1.comp:73-77 computes them, plus the barycentric terms of
-// :54-62.  Layout: (n, a.n), (a, d01), (v0, d00), (v1, d11).
+// :54-62.  Two blocks (SceneDev::rec, rec_bary): (n, a.n) of every triangle,
+// then (a, d01), (v0, d00), (v1, d11) of every triangle.  Every triangle test
+// reads the first, a leaf's triangles' planes being 16 bytes apart; only hits
+// inside the distance range read the second.
 __global__ void tri_records_kernel(const float4* __restrict__ pos4, float4* __restrict__ rec, uint32_t ntri) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ntri) return;
@@ -61,10 +64,11 @@ __global__ void tri_records_kernel(const float4* __restrict__ pos4, float4* __re
   f3 v0 = sub(b, a), v1 = sub(c, a);
   f3 n = normalize(cross(v0, v1));
   float an = dot(a, n);
-  rec[4 * (size_t)t + 0] = make_float4(n.x, n.y, n.z, an);
-  rec[4 * (size_t)t + 1] = make_float4(a.x, a.y, a.z, dot(v0, v1));
-  rec[4 * (size_t)t + 2] = make_float4(v0.x, v0.y, v0.z, dot(v0, v0));
-  rec[4 * (size_t)t + 3] = make_float4(v1.x, v1.y, v1.z, dot(v1, v1));
+  float4* bary = rec + ntri;
+  rec[t] = make_float4(n.x, n.y, n.z, an);
+  bary[3 * (size_t)t + 0] = make_float4(a.x, a.y, a.z, dot(v0, v1));
+  bary[3 * (size_t)t + 1] = make_float4(v0.x, v0.y, v0.z, dot(v0, v0));
+  bary[3 * (size_t)t + 2] = make_float4(v1.x, v1.y, v1.z, dot(v1, v1));
 }
 
 int launch_tri_records(fk_ctx* ctx, fk_scene* s) {
@@ -78,18 +82,17 @@ int launch_tri_records(fk_ctx* ctx, fk_scene* s) {
 // true and lowers `best` when the triangle is hit at t in [lo, best).  The
 // barycentric part only runs for hits inside the range (rejecting earlier
 // cannot change which t survive).
-__device__ __forceinline__ void tri_sample(const float4* __restrict__ rec, uint32_t t, f3 o, f3 d, float lo,
-                                           float& best) {
-  float4 A = __ldg(rec + 4 * (size_t)t);
+__device__ __forceinline__ void tri_sample(const SceneDev& s, uint32_t t, f3 o, f3 d, float lo, float& best) {
+  float4 A = __ldg(s.rec + t);
   f3 n = xyz(A);
   float nd = dot(d, n);
   if (!(fabsf(nd) > 0.0f)) return;
   float pn = dot(o, n);
   float th = __fdiv_rn(__fsub_rn(A.w, pn), nd);
   if (!(th >= 0.0f && th >= lo && th < best)) return;
-  float4 B = __ldg(rec + 4 * (size_t)t + 1);
-  float4 C = __ldg(rec + 4 * (size_t)t + 2);
-  float4 D = __ldg(rec + 4 * (size_t)t + 3);
+  float4 B = __ldg(s.rec_bary + 3 * (size_t)t);
+  float4 C = __ldg(s.rec_bary + 3 * (size_t)t + 1);
+  float4 D = __ldg(s.rec_bary + 3 * (size_t)t + 2);
   f3 p = add(o, scale(d, th));
   f3 v2 = sub(p, xyz(B));
   float d20 = dot(v2, xyz(C)), d21 = dot(v2, xyz(D));
@@ -130,7 +133,7 @@ __device__ float trace_skip(const SceneDev& s, f3 o, f3 d, float lo, float hi, T
     if (a < best && a < hi) {
       uint32_t e = as_u32(H.w);
       if (COUNT) c.tri += (e - as_u32(L.w)) / 3;
-      for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
+      for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s, k / 3, o, d, lo, best);
       if (settled<STOP>(best, hi)) break;
       ++i;
     } else {
@@ -162,7 +165,7 @@ __device__ float trace_ordered(const SceneDev& s, f3 o, f3 d, float lo, float hi
     if (s.root_is_leaf) {
       uint32_t e = as_u32(H.w);
       if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
-      for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
+      for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s, k / 3, o, d, lo, best);
       return best;
     }
   }
@@ -188,7 +191,7 @@ __device__ float trace_ordered(const SceneDev& s, f3 o, f3 d, float lo, float hi
       if (ref[c] < 0) {
         uint32_t t0 = as_u32(__ldg(s.node_lo + (-ref[c] - 1)).w) / 3;
         if (COUNT) tally.tri += (uint32_t)cnt[c];
-        for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s.rec, t, o, d, lo, best);
+        for (uint32_t t = t0; t < t0 + (uint32_t)cnt[c]; ++t) tri_sample(s, t, o, d, lo, best);
         if (settled<STOP>(best, hi)) return best;
       } else if (next < 0) {
         next = ref[c];
@@ -588,19 +591,13 @@ __device__ __forceinline__ bool child_hit(const RayPre& r, f3 o, f3 d, f3 lo, f3
 // slab test is monotone, so a box inside one the ray misses is missed too),
 // and every leaf's box is tested exactly when the leaf is visited, so
 // accepting a box the exact test would reject only adds work.  That keeps the
-// divisions out of the inner phase.  Its entry distance is a lower bound of
-// the exact one, so deferred records compare it directly (still_open).
+// divisions out of the inner phase.  Its entry distance, a lower bound of the
+// exact one, orders the two children.
 template <bool FILTER, int S>
 __device__ __forceinline__ bool child_maybe(const RayPre& r, const float* ray, f3 lo, f3 hi, float thr,
                                             float& entry) {
   if (FILTER) return box_near(r, lo, hi, thr, entry);
   entry = ray_box(ray_o<S>(ray), ray_d<S>(ray), lo, hi);
-  return entry < thr;
-}
-
-// Deferred node still worth visiting.
-template <bool FILTER>
-__device__ __forceinline__ bool still_open(float entry, float thr) {
   return entry < thr;
 }
 
@@ -617,25 +614,15 @@ struct OState {
   int sp;
 };
 
-// Deferred entries (SE): (ref, entry distance bits) pairs, one 8-byte
-// access per push or pop, when the distance can still cull the entry (the
-// closest-hit search, whose threshold min(best, max) shrinks as hits are
-// found); the ref alone otherwise.  A ray that stops at its first hit under
-// the maximum distance (AO, AO + bent normals) or at its first hit at all
-// (bent normals) keeps min(best, max) = max while it runs, so every entry
-// deferred below that threshold stays open and its distance is never read.
-template <typename SE>
-__device__ __forceinline__ SE stack_entry(int32_t r, float d);
-template <>
-__device__ __forceinline__ int2 stack_entry<int2>(int32_t r, float d) { return make_int2(r, __float_as_int(d)); }
-template <>
-__device__ __forceinline__ int32_t stack_entry<int32_t>(int32_t r, float) { return r; }
-__device__ __forceinline__ int32_t entry_ref(int2 e) { return e.x; }
-__device__ __forceinline__ int32_t entry_ref(int32_t e) { return e; }
-template <bool FILTER>
-__device__ __forceinline__ bool entry_open(int2 e, float thr) { return still_open<FILTER>(__int_as_float(e.y), thr); }
-template <bool FILTER>
-__device__ __forceinline__ bool entry_open(int32_t, float) { return true; }
+// Deferred entries are record refs, 4 bytes each: the entry distance is not
+// kept.  A popped inner record is visited, which tests its children against
+// the threshold of that moment, and a popped leaf is tested exactly in the
+// leaf phase, so an entry that a shrunken threshold would have culled costs
+// one visit and changes nothing.  (A ray that stops at its first hit under
+// the maximum distance, or at its first hit at all, keeps its threshold at
+// the maximum while it runs, so none of its entries could be culled anyway.)
+// Half the bytes of (ref, distance) pairs keep more of L1 for nodes and
+// triangles, which outweighs the closest-hit search's extra visits.
 
 // Inner phase: tests both children of record `cur` against `thr` and takes
 // them nearer entry first.  Their roles are decided by selects, in the order
@@ -645,9 +632,9 @@ __device__ __forceinline__ bool entry_open(int32_t, float) { return true; }
 // with one overflow check per visit.  Straight-line code keeps the visit free
 // of divergent branches.  TOP: records ref >= top_base are read from the
 // staged copies in shared memory.
-template <bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false, typename SE>
+template <bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false>
 __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
-                                            OState& st, SE* stk,
+                                            OState& st, int32_t* stk,
                                             int* status, Tally& tally, const float4* top = nullptr,
                                             uint32_t top_base = 0xFFFFFFFFu) {
   float4 w0, w1, w2, w3;
@@ -664,7 +651,6 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   if (COUNT) tally.box += 2;
   const bool swap = d1 < d0;
   const bool hn = swap ? h1 : h0, hf = swap ? h0 : h1;
-  const float dn = swap ? d1 : d0, df = swap ? d0 : d1;
   const int32_t rn = __float_as_int(swap ? w3.y : w3.x), rf = __float_as_int(swap ? w3.x : w3.y);
   const bool nl = hn && rn < 0, ni = hn && rn >= 0, fl = hf && rf < 0, fi = hf && rf >= 0;
   const bool take_nl = nl && st.pend < 0;
@@ -672,9 +658,9 @@ __device__ __forceinline__ bool inner_visit(const SceneDev& s, const RayPre& rp,
   const bool push_n = nl && !take_nl;
   const bool push_f = (fl && !take_fl) || (fi && ni);
   int sp = st.sp;
-  if (push_n && sp < STACK) stk[sp] = stack_entry<SE>(rn, dn);
+  if (push_n && sp < STACK) stk[sp] = rn;
   sp += push_n;
-  if (push_f && sp < STACK) stk[sp] = stack_entry<SE>(rf, df);
+  if (push_f && sp < STACK) stk[sp] = rf;
   sp += push_f;
   st.pend = take_nl ? -rn - 1 : (take_fl ? -rf - 1 : st.pend);
   st.cur = ni ? rn : (fi ? rf : -1);
@@ -702,9 +688,9 @@ __device__ __forceinline__ void cex(float& ka, int32_t& ra, float& kb, int32_t& 
 // (a 5-comparator sorting network), keeps the nearest inner child as the next
 // node and the nearest leaf as the postponed leaf when none is held, and
 // defers the rest farthest first, so that the nearest is popped next.
-template <bool COUNT, bool FILTER, int S, int STACK = kStack, typename SE>
+template <bool COUNT, bool FILTER, int S, int STACK = kStack>
 __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
-                                             OState& st, SE* stk,
+                                             OState& st, int32_t* stk,
                                              int* status, Tally& tally) {
   const float4* w = s.wide4 + 8 * (size_t)st.cur;
   const float4 lx = __ldg(w), hx = __ldg(w + 1), ly = __ldg(w + 2), hy = __ldg(w + 3);
@@ -738,13 +724,13 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   const bool p3 = v3 && ni != 3 && keep != 3, p2 = v2 && ni != 2 && keep != 2;
   const bool p1 = v1 && ni != 1 && keep != 1, p0 = v0 && ni != 0 && keep != 0;
   int sp = st.sp;
-  if (p3 && sp < STACK) stk[sp] = stack_entry<SE>(r3, k3);
+  if (p3 && sp < STACK) stk[sp] = r3;
   sp += p3;
-  if (p2 && sp < STACK) stk[sp] = stack_entry<SE>(r2, k2);
+  if (p2 && sp < STACK) stk[sp] = r2;
   sp += p2;
-  if (p1 && sp < STACK) stk[sp] = stack_entry<SE>(r1, k1);
+  if (p1 && sp < STACK) stk[sp] = r1;
   sp += p1;
-  if (p0 && sp < STACK) stk[sp] = stack_entry<SE>(r0, k0);
+  if (p0 && sp < STACK) stk[sp] = r0;
   sp += p0;
   st.sp = sp;
   const int32_t rk = keep == 0 ? r0 : (keep == 1 ? r1 : (keep == 2 ? r2 : r3));
@@ -757,9 +743,9 @@ __device__ __forceinline__ bool inner_visit4(const SceneDev& s, const RayPre& rp
   return true;
 }
 
-template <int TRAV, bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false, typename SE>
+template <int TRAV, bool COUNT, bool FILTER, int S, int STACK = kStack, bool TOP = false>
 __device__ __forceinline__ bool visit_inner(const SceneDev& s, const RayPre& rp, const float* ray, float thr,
-                                            OState& st, SE* stk, int* status, Tally& tally,
+                                            OState& st, int32_t* stk, int* status, Tally& tally,
                                             const float4* top = nullptr, uint32_t top_base = 0xFFFFFFFFu) {
   if (TRAV == FK_TRAVERSE_ORDERED4)
     return inner_visit4<COUNT, FILTER, S, STACK>(s, rp, ray, thr, st, stk, status, tally);
@@ -833,12 +819,11 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
     const f3 ro = ray_o<S>(wray + o), rd = ray_d<S>(wray + o);
     const float ob = __shfl_sync(full, best, o);
     const uint32_t tri = __shfl_sync(full, first, o) + (j - __shfl_sync(full, excl, o));
-    const float4* rec = s.rec;
     float olo = lo;
     if (MULTI) olo = wlo[o];
     if (j < total) {
       float b = ob;
-      tri_sample(rec, tri, ro, rd, olo, b);
+      tri_sample(s, tri, ro, rd, olo, b);
       if (b < ob) atomicMin(skey + o, dist_key(b));
     }
   }
@@ -848,21 +833,13 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
   return mine;
 }
 
-// Takes the nearest still-open deferred entry; false when none is left.
-template <bool FILTER, typename SE>
-__device__ __forceinline__ bool pop(OState& st, const SE* stk, float thr) {
-  while (st.sp > 0) {
-    const SE e = stk[--st.sp];
-    if (!entry_open<FILTER>(e, thr)) continue;
-    const int32_t r = entry_ref(e);
-    if (r < 0) {
-      st.pend = -r - 1;
-    } else {
-      st.cur = r;
-    }
-    return true;
-  }
-  return false;
+// Takes the nearest deferred entry; false when none is left.
+__device__ __forceinline__ bool pop(OState& st, const int32_t* stk) {
+  if (st.sp == 0) return false;
+  const int32_t r = stk[--st.sp];
+  if (r < 0) st.pend = -r - 1;
+  else st.cur = r;
+  return true;
 }
 
 // Skip-pointer walk, one flattened node per call.
@@ -878,7 +855,7 @@ __device__ __forceinline__ bool skip_step(const SceneDev& s, const RayPre& rp, c
   if (h) {
     uint32_t e = as_u32(H.w);
     if (COUNT) tally.tri += (e - as_u32(L.w)) / 3;
-    for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s.rec, k / 3, o, d, lo, best);
+    for (uint32_t k = as_u32(L.w); k < e; k += 3) tri_sample(s, k / 3, o, d, lo, best);
     if (settled<STOP>(best, hi)) return true;
     ++i;
   } else {
@@ -907,8 +884,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
   const unsigned full = 0xFFFFFFFFu;
   const int lane = threadIdx.x & 31;
   const unsigned lower = (1u << lane) - 1u;
-  using SE = typename std::conditional<STOP == kClosest, int2, int32_t>::type;
-  SE stk[is_ordered(TRAV) ? STACK : 1];  // deferred entries (stack_entry)
+  int32_t stk[is_ordered(TRAV) ? STACK : 1];  // deferred record refs
   __shared__ uint32_t leaf_keys[BLOCK / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   __shared__ float srays[6 * BLOCK];  // the lanes' ray origins and directions (ray_put)
@@ -1014,7 +990,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
             fin = true;
           // further visits in the same iteration, continuing from the stack
           for (int v = 1; v < kInnerVisits && !fin; ++v) {
-            if (st.cur < 0 && st.pend < 0 && !pop<FILTER>(st, stk, fminf(best, p.hi))) {
+            if (st.cur < 0 && st.pend < 0 && !pop(st, stk)) {
               fin = true;
               break;
             }
@@ -1024,7 +1000,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 512 ? 2 : 1280 / BLOCK) hemi_t
               fin = true;
           }
         }
-        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, p.hi));
+        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop(st, stk);
         if (fin) {
           p.scratch[sslot[threadIdx.x]] = best;
           active = false;
@@ -1367,8 +1343,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
   const unsigned lower = (1u << lane) - 1u;
   // a launch traces at most the scratch's 2^27 rays: lane indices fit 32 bits
   const uint32_t total = (uint32_t)((p.r1 - p.r0 + p.stride - 1) / p.stride);
-  using SE = typename std::conditional<STOP == kClosest, int2, int32_t>::type;
-  SE stk[is_ordered(TRAV) ? kStack : 1];  // deferred entries (stack_entry)
+  int32_t stk[is_ordered(TRAV) ? kStack : 1];  // deferred record refs
   __shared__ uint32_t leaf_keys[256 / 32][32];  // leaf-phase distance minimum, per warp
   uint32_t* skey = leaf_keys[threadIdx.x >> 5];
   __shared__ float srays[6 * 256];  // the lanes' ray origins and directions (ray_put)
@@ -1474,7 +1449,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
           if (!visit_inner<TRAV, false, FILTER, 256>(s, rp, myray, fminf(best, hi), st, stk, p.status, tally))
             fin = true;
           for (int v = 1; v < kInnerVisits && !fin; ++v) {  // as in hemi_trace_kernel
-            if (st.cur < 0 && st.pend < 0 && !pop<FILTER>(st, stk, fminf(best, hi))) {
+            if (st.cur < 0 && st.pend < 0 && !pop(st, stk)) {
               fin = true;
               break;
             }
@@ -1483,7 +1458,7 @@ __global__ void __launch_bounds__(256, FK_BATCH_MIN_BLOCKS) batch_trace_kernel(B
               fin = true;
           }
         }
-        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop<FILTER>(st, stk, fminf(best, hi));
+        if (!fin && st.cur < 0 && st.pend < 0) fin = !pop(st, stk);
         if (fin) {
           p.scratch[sslot[threadIdx.x]] = best;
           active = false;
@@ -1568,8 +1543,10 @@ int concat_batch_scene(cudaStream_t st, const fk_scene* s, uint32_t node_base, u
                         st) != cudaSuccess ||
         cudaMemcpyAsync(const_cast<float4*>(cat.nrm4) + corner_base, s->nrm4, 16 * nc, cudaMemcpyDeviceToDevice,
                         st) != cudaSuccess ||
-        cudaMemcpyAsync(const_cast<float4*>(cat.rec) + 4 * (size_t)(corner_base / 3), s->tri_rec, 64 * (nc / 3),
-                        cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+        cudaMemcpyAsync(const_cast<float4*>(cat.rec) + corner_base / 3, s->tri_rec, 16 * (nc / 3),
+                        cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(const_cast<float4*>(cat.rec_bary) + 3 * (size_t)(corner_base / 3), s->tri_rec + nc / 3,
+                        48 * (nc / 3), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
       return FK_ERR_CUDA;
   }
   return FK_OK;
@@ -1808,7 +1785,7 @@ __device__ void walk_oneside(const SceneDev& s, f3 o, f3 d, float& cur, uint32_t
     if (a < cur) {
       uint32_t e = as_u32(H.w);
       for (uint32_t k = as_u32(L.w); k < e; k += 3) {
-        float4 A = __ldg(s.rec + 4 * (size_t)(k / 3));
+        float4 A = __ldg(s.rec + k / 3);
         f3 n = xyz(A);
         float nd = dot(d, n);
         if (SIGN > 0 ? !(nd > 0.0f) : !(nd < 0.0f)) continue;
@@ -1842,7 +1819,7 @@ __device__ float walk_twoside(const SceneDev& s, f3 o, f3 d, float mint, uint32_
       f3 lw = mk3(0.0f, 0.0f, 0.0f);
       uint32_t e = as_u32(H.w);
       for (uint32_t k = as_u32(L.w); k < e; k += 3) {
-        float4 A = __ldg(s.rec + 4 * (size_t)(k / 3));
+        float4 A = __ldg(s.rec + k / 3);
         f3 n = xyz(A);
         float nd = dot(d, n);
         if (!(fabsf(nd) > 0.0f)) continue;
