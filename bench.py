@@ -75,9 +75,8 @@ TRAVERSE = {"auto": 0, "ordered": 1, "skip": 2, "ordered4": 3}
 SCHEDULE = {"auto": 0, "static": 0x10, "dynamic": 0x20}
 # DRAM bytes (read + write) per hemisphere-kernel launch from ncu captures, by workload: plane250, one AO+BN
 # trace launch of 968,256 rays (profiles/hemi_trace_kernel_plane250.md); plane2048, the mean of two AO+BN
-# chunk launches of 134,217,728 rays each, 5.31 and 3.64 GB (profiles/hemi_trace_traffic_plane2048.md, captured
-# before the last L1 changes, which cut the plane250 case's DRAM reads by 18 %).
-NCU_TRAFFIC = {"plane250": 245.5e6, "plane2048": 4.474e9}
+# chunk launches of 134,217,728 rays each, 4.46 and 2.94 GB (profiles/hemi_trace_traffic_plane2048.md).
+NCU_TRAFFIC = {"plane250": 245.5e6, "plane2048": 3.700e9}
 
 
 def rays_per_texel(wl):
