@@ -57,7 +57,7 @@ struct fk_batch {
   fk_tuning tuning = {8, 8, 0, 0, 0, FK_L2_NONE, 256, 64};
   // the jobs' scenes laid end to end (fk::BatchArgs::cat) and its allocations
   fk::SceneDev cat = {};
-  void* cat_mem[7] = {};
+  void* cat_mem[8] = {};
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -273,10 +273,12 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
     j.h.scratch_rays = b->scratch_rays;
   }
   int rc = fk_dev_alloc(ctx, (void**)&b->jobs, sizeof(fk::BatchJobDev) * njobs);
-  // the concatenated scene: nodes (lo, hi, jump), corners (positions, normals), triangle records, both layouts
-  const size_t cat_bytes[7] = {16 * (size_t)nodes, 16 * (size_t)nodes, 4 * (size_t)nodes, 16 * (size_t)corners,
-                               16 * (size_t)corners, 64 * (size_t)(corners / 3), 64 * (size_t)recs2};
-  for (int k = 0; k < 7 && rc == FK_OK; ++k) rc = fk_dev_alloc(ctx, &b->cat_mem[k], std::max<size_t>(cat_bytes[k], 16));
+  // the concatenated scene: nodes (lo, hi, jump), corners (positions, normals), triangle records, both layouts,
+  // node boxes side by side
+  const size_t cat_bytes[8] = {16 * (size_t)nodes,   16 * (size_t)nodes,   4 * (size_t)nodes,
+                               16 * (size_t)corners, 16 * (size_t)corners, 64 * (size_t)(corners / 3),
+                               64 * (size_t)recs2,   32 * (size_t)nodes};
+  for (int k = 0; k < 8 && rc == FK_OK; ++k) rc = fk_dev_alloc(ctx, &b->cat_mem[k], std::max<size_t>(cat_bytes[k], 16));
   if (rc == FK_OK && recs4) rc = fk_dev_alloc(ctx, (void**)&b->cat.wide4, 128 * (size_t)recs4);
   if (rc == FK_OK) {
     b->cat.node_lo = (const float4*)b->cat_mem[0];
@@ -287,6 +289,7 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
     b->cat.rec = (const float4*)b->cat_mem[5];
     b->cat.rec_bary = b->cat.rec + corners / 3;  // the planes of every job's triangles, then their barycentric terms
     b->cat.wide = (const float4*)b->cat_mem[6];
+    b->cat.node_box = (const float4*)b->cat_mem[7];
     b->cat.node_count = (uint32_t)nodes;
     b->cat.corner_count = (uint32_t)corners;
     b->cat.filter_ok = 1;
@@ -295,6 +298,10 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
                                  table[i].root2 < 0 ? 0 : (uint32_t)table[i].root2,
                                  table[i].root4 < 0 ? 0 : (uint32_t)table[i].root4, b->cat) != FK_OK)
         rc = fk_fail(ctx, FK_ERR_CUDA, "fk_batch_create: scene concatenation");
+    if (rc == FK_OK &&
+        fk::pair_node_boxes(ctx->stream, b->cat.node_lo, b->cat.node_hi, (uint32_t)nodes,
+                            const_cast<float4*>(b->cat.node_box)) != cudaSuccess)
+      rc = fk_fail(ctx, FK_ERR_CUDA, "fk_batch_create: node boxes");
   }
   if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->queues, sizeof(unsigned long long) * (b->chunks.size() + 1));
   if (rc == FK_OK) rc = fk_dev_alloc(ctx, (void**)&b->scratch, sizeof(float) * b->scratch_rays);

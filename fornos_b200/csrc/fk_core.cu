@@ -458,6 +458,15 @@ static int scene_create(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, cons
   }
   if (rc == FK_OK) rc = fk::launch_tri_records(ctx, s);
   if (rc == FK_OK) {
+    rc = fk_dev_alloc(ctx, (void**)&s->node_box, 2 * sizeof(float4) * (size_t)nn);
+    s->bytes += 2 * sizeof(float4) * (size_t)nn;
+  }
+  if (rc == FK_OK) {
+    const cudaError_t e = fk::pair_node_boxes(ctx->stream, s->node_lo, s->node_hi, nn, s->node_box);
+    if (e != cudaSuccess) rc = fk_cuda_fail(ctx, e, "pair_boxes_kernel");
+    else ++ctx->launches;
+  }
+  if (rc == FK_OK) {
     cudaError_t e = cudaStreamSynchronize(ctx->stream);
     if (e != cudaSuccess) rc = fk_cuda_fail(ctx, e, "scene upload sync");
   }
@@ -564,7 +573,7 @@ int fk_scene_free(fk_ctx* ctx, fk_scene* s) {
   if (!ctx || !s || !ctx->scenes.count(s)) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_free: unknown scene");
   cudaStreamSynchronize(ctx->stream);
   void* ps[] = {s->node_lo,         s->node_hi,         s->node_jump, s->pos4,    s->nrm4,  s->tree_wide[0],
-                s->tree_wide[1],   s->tree_wide4[0],   s->tree_wide4[1], s->tri_rec, s->top};
+                s->tree_wide[1],   s->tree_wide4[0],   s->tree_wide4[1], s->tri_rec, s->top, s->node_box};
   for (void* p : ps) fk_dev_free(ctx, p);
   ctx->scenes.erase(s);
   delete s;

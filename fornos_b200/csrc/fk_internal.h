@@ -55,6 +55,7 @@ struct fk_scene {
   // Reference layout, one entry per flattened node (skip-pointer walk):
   float4* node_lo = nullptr;     // aabbMin.xyz, start (bits)
   float4* node_hi = nullptr;     // aabbMax.xyz, end (bits)
+  float4* node_box = nullptr;    // node_lo[i], node_hi[i] side by side (one 32-byte sector), for the leaf phase
   uint32_t* node_jump = nullptr;
   float4* pos4 = nullptr;        // triangle corners, DFS leaf order
   float4* nrm4 = nullptr;
@@ -132,6 +133,7 @@ namespace fk {
 struct SceneDev {
   const float4* __restrict__ node_lo;
   const float4* __restrict__ node_hi;
+  const float4* __restrict__ node_box;  // node_lo[i], node_hi[i] at 2 i, 2 i + 1
   const uint32_t* __restrict__ node_jump;
   const float4* __restrict__ pos4;
   const float4* __restrict__ nrm4;
@@ -277,6 +279,8 @@ int launch_gather(fk_ctx* ctx, const fk_scene* s, int kind, const float4* coords
                   uint32_t offset, uint32_t count, float* out);
 int launch_tangent_space(fk_ctx* ctx, const fk_texel_map* m, uint32_t offset, uint32_t count, float* io3);
 int launch_tri_records(fk_ctx* ctx, fk_scene* s);
+// Fills box[2 i], box[2 i + 1] = lo[i], hi[i] for i < n on `stream`.
+cudaError_t pair_node_boxes(cudaStream_t stream, const float4* lo, const float4* hi, uint32_t n, float4* box);
 struct RasterTri;  // defined in fk_raster.cu
 
 // Learned denoiser: parameter layout (fp32, row-major) and kernel launchers.

@@ -34,6 +34,7 @@ static SceneDev dev_of(const fk_scene* s) {
   SceneDev d;
   d.node_lo = s->node_lo;
   d.node_hi = s->node_hi;
+  d.node_box = s->node_box;
   d.node_jump = s->node_jump;
   d.pos4 = s->pos4;
   d.nrm4 = s->nrm4;
@@ -69,6 +70,19 @@ __global__ void tri_records_kernel(const float4* __restrict__ pos4, float4* __re
   bary[3 * (size_t)t + 0] = make_float4(a.x, a.y, a.z, dot(v0, v1));
   bary[3 * (size_t)t + 1] = make_float4(v0.x, v0.y, v0.z, dot(v0, v0));
   bary[3 * (size_t)t + 2] = make_float4(v1.x, v1.y, v1.z, dot(v1, v1));
+}
+
+__global__ void pair_boxes_kernel(const float4* __restrict__ lo, const float4* __restrict__ hi, uint32_t n,
+                                  float4* __restrict__ box) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  box[2 * (size_t)i] = lo[i];
+  box[2 * (size_t)i + 1] = hi[i];
+}
+
+cudaError_t pair_node_boxes(cudaStream_t stream, const float4* lo, const float4* hi, uint32_t n, float4* box) {
+  if (n) pair_boxes_kernel<<<(n + 255) / 256, 256, 0, stream>>>(lo, hi, n, box);
+  return cudaGetLastError();
 }
 
 int launch_tri_records(fk_ctx* ctx, fk_scene* s) {
@@ -786,7 +800,7 @@ __device__ __forceinline__ bool leaf_phase_warp(const SceneDev& s, const RayPre&
   const bool mine = active && st.pend >= 0;
   __syncwarp();  // the lanes' rays, written at their set-up, are read by other lanes below
   if (mine) {
-    const float4 L = __ldg(s.node_lo + st.pend), H = __ldg(s.node_hi + st.pend);
+    const float4 L = __ldg(s.node_box + 2 * (size_t)st.pend), H = __ldg(s.node_box + 2 * (size_t)st.pend + 1);
     float entry;
     if (COUNT) tally.box++;
     if (child_hit<FILTER>(rp, ray_o<S>(wray + lane), ray_d<S>(wray + lane), xyz(L), xyz(H), fminf(best, hi),
