@@ -1,14 +1,15 @@
 // Batched bakes and the traversal autotuner.
 //
 // A batch is a set of hemisphere-sampling jobs, each with its own scene,
-// mapped texels, sample table, parameters and output buffers.  Jobs smaller
-// than one chunk (2^27 rays) share persistent launches: their rays are laid
-// end to end in one 64-bit ray space (chunked at texel boundaries to fit the
-// scratch), and every lane maps its ray back to its job, so small jobs fill
-// the GPU together instead of each paying a launch and its tail.  A job of a
-// chunk or more gains nothing from sharing and runs alone through the
-// single-job path (its launches' tails are a small part of its time), on the
-// batch's scratch, in the same run and the same graph.  The launches of a run can be recorded once into a
+// mapped texels, sample table, parameters and output buffers.  Jobs of fewer
+// than 2^21 rays share persistent launches: their rays are laid end to end in
+// one 64-bit ray space (chunked at texel boundaries to fit the scratch), and
+// every lane maps its ray back to its job, so small jobs fill the GPU together
+// instead of each paying a launch and its tail.  A larger job gains nothing
+// from sharing (its launches' tails are a small part of its time, and the
+// shared kernel carries each lane's job beside the traversal) and runs alone
+// through the single-job path, on the batch's scratch, in the same run and the
+// same graph.  The launches of a run can be recorded once into a
 // CUDA graph and replayed.  The autotuner times a strided sample of the
 // batch's rays (every job represented) for each candidate schedule and keeps
 // the fastest: ordered vs skip-pointer traversal, filtered vs divided box
@@ -27,6 +28,11 @@ struct Chunk {
 };
 
 constexpr unsigned long long kMaxChunkRays = 1ull << 27;  // 512 MB of distances
+// Jobs of at least this many rays run alone through the single-job path.
+#ifndef FK_BATCH_SOLO_RAYS
+#define FK_BATCH_SOLO_RAYS (1ull << 21)
+#endif
+constexpr unsigned long long kSoloRays = FK_BATCH_SOLO_RAYS;
 
 // A job run alone (fk_batch's `solo`): its scene and its launch.
 struct Solo {
@@ -47,7 +53,7 @@ struct fk_batch {
   float* scratch = nullptr;
   unsigned long long scratch_rays = 0;
   std::vector<Chunk> chunks;
-  std::vector<Solo> solo;                 // jobs of at least kMaxChunkRays rays, run alone
+  std::vector<Solo> solo;                 // jobs of at least kSoloRays rays, run alone
   uint64_t solo_launches = 0;             // kernel launches of the solo jobs in one run
   int traverse = FK_TRAVERSE_ORDERED;     // tuned choice
   bool ordered_ok = true;                 // every tree fits the 2-wide ordered traversal's stack
@@ -228,7 +234,7 @@ int fk_batch_create(fk_ctx* ctx, const fk_batch_job* jobs, uint32_t njobs, int k
   for (uint32_t i = 0; i < njobs; ++i) {
     const fk::BatchJobDev& d = table[i];
     const unsigned long long job_rays = (unsigned long long)d.texels * d.spp;
-    if (job_rays >= kMaxChunkRays) {
+    if (job_rays >= kSoloRays) {
       if (cur.t1 > cur.t0) b->chunks.push_back(cur);
       cur = {cur.r1 + job_rays, cur.r1 + job_rays, cur.t1 + d.texels, cur.t1 + d.texels};
       const fk_batch_job& J = jobs[i];

@@ -421,9 +421,9 @@ int fk_solver_free(fk_solver* s);
  * No counterpart in the reference (which bakes one mesh pair at a time, one
  * chunk per UI frame).  Up to 64 hemisphere jobs, each with its own scene,
  * mapped texels, sample table, parameters and outputs.  Jobs of fewer than
- * 2^27 rays share persistent launches: their rays are laid end to end and
+ * 2^21 rays share persistent launches: their rays are laid end to end and
  * every lane maps its ray back to its job, so small jobs keep the whole GPU
- * busy together.  A job of 2^27 rays or more runs alone through the
+ * busy together.  A job of 2^21 rays or more runs alone through the
  * single-job path within the same run (and the same graph), on the batch's
  * scratch.  Results are those fk_hemisphere gives per job. */
 typedef struct fk_batch fk_batch;
