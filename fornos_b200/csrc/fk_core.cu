@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "fk_internal.h"
+#include "fk_layout.h"
 #include "fk_sah_rules.h"
 
 int fk_fail(fk_ctx* ctx, int code, const std::string& msg) {
@@ -176,6 +177,8 @@ int fk_ctx_destroy(fk_ctx* ctx) {
   cudaFree(ctx->scratch);
   if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
   if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
+  if (ctx->stage_done) cudaEventDestroy(ctx->stage_done);
+  if (ctx->stage) cudaFreeHost(ctx->stage);
   cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return FK_OK;
@@ -185,6 +188,9 @@ int fk_ctx_trim(fk_ctx* ctx) {
   if (!ctx) return FK_ERR_INVALID;
   FK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
   if (ctx->pool) FK_CUDA(ctx, cudaMemPoolTrimTo(ctx->pool, 0));
+  if (ctx->stage) FK_CUDA(ctx, cudaFreeHost(ctx->stage));  // its copies were on the stream
+  ctx->stage = nullptr;
+  ctx->stage_bytes = 0;
   return FK_OK;
 }
 
@@ -301,72 +307,29 @@ static int scene_create(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, cons
                         uint32_t nc, fk::DevBvh* dev, fk_scene** out) {
   if (!ctx || !out || !nodes || (!dev && (!pos4 || !nrm4)) || nn == 0 || nc == 0 || nc % 3 != 0)
     return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: empty or malformed scene");
-  // Validate the skip-pointer structure so no kernel can walk outside it.
-  std::vector<float4> lo(nn), hi(nn);
-  std::vector<uint32_t> jump(nn);
-  uint32_t leaves = 0;
-  std::vector<uint32_t> leaf_ids;  // flattened indices of the leaves, ascending
-  bool sah_ok = true;              // leaf boxes within the rebuilt tree's coordinate range
-  for (uint32_t i = 0; i < nn; ++i) {
-    const fk_bvh_node& n = nodes[i];
-    if (n.start > n.end || n.end > nc || n.start % 3 || n.end % 3 || n.jump <= i || n.jump > nn)
-      return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node " + std::to_string(i) + " is malformed");
-    bool leaf = n.jump == i + 1;
-    if (leaf != (n.end > n.start))
-      return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node " + std::to_string(i) + " mixes children and triangles");
-    leaves += leaf;
-    if (leaf) {
-      leaf_ids.push_back(i);
-      for (int a = 0; a < 3; ++a)
-        sah_ok = sah_ok && fk::sah::coord_ok(n.aabb_min[a]) && fk::sah::coord_ok(n.aabb_max[a]);
+  // Check the skip-pointer structure so no kernel can walk outside it, and
+  // lay out the device arrays (fk_layout.cpp, over host threads) in the
+  // context's pinned staging, once the previous upload's copies from it are
+  // done.
+  const size_t stage_need = fk::layout_bytes(nn);
+  if (ctx->stage_done) FK_CUDA(ctx, cudaEventSynchronize(ctx->stage_done));
+  if (ctx->stage_bytes < stage_need) {
+    if (ctx->stage) FK_CUDA(ctx, cudaFreeHost(ctx->stage));
+    ctx->stage = nullptr;
+    ctx->stage_bytes = 0;
+    if (cudaMallocHost(&ctx->stage, stage_need) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->stage = nullptr;
+      return fk_fail(ctx, FK_ERR_NOMEM, "fk_scene_upload: pinned staging of " + std::to_string(stage_need) + " bytes");
     }
-    uint32_t s = n.start, e = n.end;
-    float fs, fe;
-    std::memcpy(&fs, &s, 4);
-    std::memcpy(&fe, &e, 4);
-    lo[i] = make_float4(n.aabb_min[0], n.aabb_min[1], n.aabb_min[2], fs);
-    hi[i] = make_float4(n.aabb_max[0], n.aabb_max[1], n.aabb_max[2], fe);
-    jump[i] = n.jump;
+    ctx->stage_bytes = stage_need;
   }
-  if (nodes[0].jump != nn) return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node 0 does not span the array");
-  // Inner node i has children i + 1 and nodes[i + 1].jump; depth and the
-  // ordered (children-in-parent) layout follow from that.
-  std::vector<int32_t> wide_of(nn, -1);
-  uint32_t nw = 0;
-  for (uint32_t i = 0; i < nn; ++i)
-    if (nodes[i].jump != i + 1) {
-      uint32_t r = nodes[i + 1].jump;
-      if (i + 1 >= nn || r >= nodes[i].jump || nodes[r].jump != nodes[i].jump)
-        return fk_fail(ctx, FK_ERR_INVALID, "fk_scene_upload: node " + std::to_string(i) + " children inconsistent");
-      wide_of[i] = (int32_t)nw++;
-    }
-  std::vector<float4> wide(4 * (size_t)nw);
-  std::vector<uint32_t> depth(nn, 1);
-  uint32_t maxd = 1;
-  for (uint32_t i = 0; i < nn; ++i) {
-    maxd = depth[i] > maxd ? depth[i] : maxd;
-    if (wide_of[i] < 0) continue;
-    uint32_t c[2] = {i + 1, nodes[i + 1].jump};
-    depth[c[0]] = depth[c[1]] = depth[i] + 1;
-    int32_t ref[2], cnt[2];
-    for (int k = 0; k < 2; ++k) {
-      const fk_bvh_node& n = nodes[c[k]];
-      // inner child: its record index; leaf child: -(flattened node index + 1),
-      // the triangle range being that node's [start, end)
-      if (wide_of[c[k]] >= 0) { ref[k] = wide_of[c[k]]; cnt[k] = 0; }
-      else { ref[k] = -(int32_t)c[k] - 1; cnt[k] = (int32_t)((n.end - n.start) / 3); }
-    }
-    const fk_bvh_node& L = nodes[c[0]];
-    const fk_bvh_node& R = nodes[c[1]];
-    float4* w = &wide[4 * (size_t)wide_of[i]];
-    w[0] = make_float4(L.aabb_min[0], L.aabb_max[0], L.aabb_min[1], L.aabb_max[1]);
-    w[1] = make_float4(R.aabb_min[0], R.aabb_max[0], R.aabb_min[1], R.aabb_max[1]);
-    w[2] = make_float4(L.aabb_min[2], L.aabb_max[2], R.aabb_min[2], R.aabb_max[2]);
-    float f[4];
-    int32_t ints[4] = {ref[0], ref[1], cnt[0], cnt[1]};
-    std::memcpy(f, ints, 16);
-    w[3] = make_float4(f[0], f[1], f[2], f[3]);
-  }
+  fk::NodeLayout lay;
+  const std::string bad = fk::layout_nodes(nodes, nn, nc, ctx->stage, lay);
+  if (!bad.empty()) return fk_fail(ctx, FK_ERR_INVALID, bad);
+  const uint32_t leaves = lay.leaves, nw = lay.wide_count, maxd = lay.depth;
+  const bool sah_ok = lay.sah_ok;  // leaf boxes within the rebuilt tree's coordinate range
+  const std::vector<uint32_t>& leaf_ids = lay.leaf_ids;
   fk_scene* s = new (std::nothrow) fk_scene();
   if (!s) return FK_ERR_NOMEM;
   s->ctx = ctx;
@@ -384,11 +347,7 @@ static int scene_create(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, cons
   // The conservative inner test also takes each box's faces in order.
   {
     const float lim = 16777216.0f;
-    bool ok = true;
-    for (uint32_t i = 0; i < nn && ok; ++i)
-      for (int a = 0; a < 3; ++a)
-        ok = ok && std::fabs(nodes[i].aabb_min[a]) < lim && std::fabs(nodes[i].aabb_max[a]) < lim &&
-             nodes[i].aabb_min[a] <= nodes[i].aabb_max[a];
+    bool ok = lay.coords_ok;
     if (!dev) {
       // the corners are checked on the device once uploaded (below)
     } else if (ok) {
@@ -422,13 +381,22 @@ static int scene_create(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t nn, cons
     *dev = fk::DevBvh{};
     s->bytes += 2 * nb + sizeof(uint32_t) * nn + 2 * cb;
   } else {
-    up((void**)&s->node_lo, lo.data(), nb);
-    up((void**)&s->node_hi, hi.data(), nb);
-    up((void**)&s->node_jump, jump.data(), sizeof(uint32_t) * nn);
+    up((void**)&s->node_lo, lay.lo, nb);
+    up((void**)&s->node_hi, lay.hi, nb);
+    up((void**)&s->node_jump, lay.jump, sizeof(uint32_t) * nn);
     up((void**)&s->pos4, pos4, cb);
     up((void**)&s->nrm4, nrm4, cb);
   }
-  up((void**)&s->wide, wide.data(), sizeof(float4) * wide.size());
+  up((void**)&s->wide, lay.wide, sizeof(float4) * 4 * (size_t)nw);
+  {  // the copies above read the staging: the next upload waits for them
+    cudaError_t e = cudaSuccess;
+    if (!ctx->stage_done) e = cudaEventCreateWithFlags(&ctx->stage_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->stage_done, ctx->stream);
+    if (e != cudaSuccess) {
+      cudaStreamSynchronize(ctx->stream);
+      if (rc == FK_OK) rc = fk_cuda_fail(ctx, e, "scene upload staging");
+    }
+  }
   if (rc == FK_OK && !dev && s->filter_ok) {  // the uploaded corners, on the device: 100 MB take ~20 us there
     bool below = false;
     rc = fk::corners_below(ctx, s->pos4, nc, 16777216.0f, &below);

@@ -31,6 +31,12 @@ struct fk_ctx {
   // bakes reuse it instead of mapping and unmapping pages (fk_ctx_trim).
   cudaMemPool_t pool = nullptr;
   size_t scratch_bytes = 0;
+  // Pinned host memory the scene upload lays the node arrays out in (kept
+  // between uploads, released by fk_ctx_trim); stage_done is recorded after
+  // the copies that read it, and the next upload waits for it.
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+  cudaEvent_t stage_done = nullptr;
   fk_tuning tuning = {20, 8, 1, FK_RAY_ORDER_SECTOR, 0, FK_L2_NONE, 256, 64};  // fk_ctx_set_tuning
   // Persisting L2 set-aside (fk_tuning.l2_persist): the device's limit before
   // the context raised it, restored when the knob is turned off or the
