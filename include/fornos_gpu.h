@@ -70,7 +70,8 @@ int fk_ctx_set_stream(fk_ctx* ctx, void* cuda_stream);
 void* fk_ctx_stream(const fk_ctx* ctx);
 int fk_sync(fk_ctx* ctx);
 /* No counterpart in the reference.  Waits for the context's stream and
- * releases the pool memory no live object uses. */
+ * releases the pool memory no live object uses and the scene uploads' pinned
+ * host staging. */
 int fk_ctx_trim(fk_ctx* ctx);
 /* Kernel launches issued by this context so far. */
 uint64_t fk_launch_count(const fk_ctx* ctx);
@@ -199,6 +200,10 @@ int fk_bvh_build_flat(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint3
                       uint32_t node_capacity, uint32_t* node_count, float* positions4, float* normals4);
 
 /* ------------------------------------------------------------ device scene */
+/* Checks the node array (FK_ERR_INVALID names the first defective node) and
+ * lays it out for the device on host threads, in pinned host memory that the
+ * context keeps for later uploads (about 68 bytes per node; fk_ctx_trim
+ * releases it).  Returns once the scene is on the device. */
 int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t node_count, const float* positions4,
                     const float* normals4, uint32_t corner_count, fk_scene** out);
 int fk_scene_free(fk_ctx* ctx, fk_scene* scene);
