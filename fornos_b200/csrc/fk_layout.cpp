@@ -1,6 +1,7 @@
 // Host side of the scene upload (fk_layout.h): three passes over node ranges,
 // one host thread per range, and a scan in node order for the tree depth
-// (on a thread of its own, beside the last two passes).
+// (on a thread of its own beside the last two passes when there are several
+// ranges).  A range whose thread cannot be started runs on the calling thread.
 //
 //   1. each range checks its nodes, writes their device layout and counts
 //      leaves and inner nodes; the first defect of each range is kept, so
@@ -15,6 +16,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <system_error>
 #include <thread>
 
 #include "fk_sah_rules.h"
@@ -33,18 +35,23 @@ struct RangeScan {
   bool sah_ok = true, coords_ok = true;
 };
 
-// fn(t, a, b) over [0, nn) cut into `threads` ranges in node order.
+// fn(t, a, b) over [0, nn) cut into `threads` ranges in node order; the
+// calling thread takes the last range, and any range whose thread could not
+// be started.
 template <typename F>
 void over_ranges(unsigned threads, uint32_t nn, F&& fn) {
-  if (threads <= 1) {
-    fn(0u, 0u, nn);
-    return;
-  }
   std::vector<std::thread> pool;
   pool.reserve(threads);
   for (unsigned t = 0; t < threads; ++t) {
     const uint32_t a = (uint32_t)((uint64_t)nn * t / threads), b = (uint32_t)((uint64_t)nn * (t + 1) / threads);
-    pool.emplace_back([&fn, t, a, b] { fn(t, a, b); });
+    if (t + 1 < threads) {
+      try {
+        pool.emplace_back([&fn, t, a, b] { fn(t, a, b); });
+        continue;
+      } catch (const std::system_error&) {
+      }
+    }
+    fn(t, a, b);
   }
   for (auto& th : pool) th.join();
 }
@@ -137,19 +144,26 @@ std::string layout_nodes(const fk_bvh_node* nodes, uint32_t nn, uint32_t nc, voi
   out.leaves = leaves;
   out.wide_count = inner;
   out.leaf_ids.resize(leaves);
-  // the depth scan reads only the skip pointers: beside the record passes
+  // With the structure checked, node i's subtree is [i, jump[i]) and the
+  // subtrees nest, so the inner nodes whose subtree still holds node i (a
+  // stack of their ends) are its ancestors.  The scan reads only the skip
+  // pointers: with several ranges it runs beside the record passes.
   uint32_t depth = 1;
-  std::thread depth_scan([&] {
-    // with the structure checked, node i's subtree is [i, jump[i]) and the
-    // subtrees nest, so the inner nodes whose subtree still holds node i (a
-    // stack of their ends) are its ancestors
+  auto depth_scan = [&] {
     std::vector<uint32_t> ends;
     for (uint32_t i = 0; i < nn; ++i) {
       while (!ends.empty() && ends.back() <= i) ends.pop_back();
       depth = std::max(depth, (uint32_t)ends.size() + 1);
       if (jump[i] != i + 1) ends.push_back(jump[i]);
     }
-  });
+  };
+  std::thread depth_thread;
+  if (T > 1) {
+    try {
+      depth_thread = std::thread(depth_scan);
+    } catch (const std::system_error&) {
+    }
+  }
   over_ranges(T, nn, [&](unsigned t, uint32_t a, uint32_t b) {
     uint32_t l = leaf_base[t], w = wide_base[t];
     for (uint32_t i = a; i < b; ++i) {
@@ -180,7 +194,8 @@ std::string layout_nodes(const fk_bvh_node* nodes, uint32_t nn, uint32_t nc, voi
       std::memcpy(w + 12, ints, 16);
     }
   });
-  depth_scan.join();
+  if (depth_thread.joinable()) depth_thread.join();
+  else depth_scan();
   out.depth = depth;
   return {};
 }
