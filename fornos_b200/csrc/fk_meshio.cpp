@@ -47,6 +47,7 @@
 #include <map>
 #include <sstream>
 #include <string>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -61,8 +62,11 @@ bool read_file(const char* path, std::string& out) {
   if (!f) return false;
   if (std::fseek(f, 0, SEEK_END) == 0) {  // one read of the whole file where its size is known
     const long size = std::ftell(f);
-    if (size > 0) out.reserve((size_t)size);
     std::rewind(f);
+    if (size > 0) {
+      out.resize((size_t)size);
+      out.resize(std::fread(&out[0], 1, (size_t)size, f));  // then whatever a growing file added
+    }
   }
   char chunk[1 << 16];
   size_t n;
@@ -450,6 +454,14 @@ class PlyReader {
           const size_t old = g.first->size();
           g.first->resize(old + el.size * per);
           uint8_t* dst = g.first->data() + old;
+          // little-endian values of adjacent properties (x, y, z) are one span of each record
+          bool span = !big_;
+          for (size_t k = 1; k < g.second.size() && span; ++k)
+            span = g.second[k].first == g.second[k - 1].first + g.second[k - 1].second;
+          if (span) {
+            strided_copy(dst, base + g.second[0].first, el.size, rec, per);
+            continue;
+          }
           for (size_t i = 0; i < el.size; ++i)
             for (const auto& f : g.second) {
               const uint8_t* src = base + i * rec + f.first;
@@ -463,6 +475,7 @@ class PlyReader {
         at_ += el.size * rec;
         continue;
       }
+      if (binary_ && el.props.size() == 1 && uniform_list(el, sink[0])) continue;
       for (size_t i = 0; i < el.size; ++i)
         for (size_t k = 0; k < el.props.size(); ++k) {
           const PlyProp& p = el.props[k];
@@ -503,6 +516,66 @@ class PlyReader {
     for (const auto& p : el.props)
       if (p.list || p.type != kInvalid) return false;
     return true;
+  }
+  // A binary element of one list property whose every instance has the
+  // first one's length (a face element of triangles): its records have one
+  // size, so the items are copied record by record without per-instance
+  // count reads or buffer growth.  Leaves the data untouched and returns
+  // false otherwise, for the value-by-value path (which also rejects what is
+  // malformed).
+  bool uniform_list(const PlyElem& el, std::vector<uint8_t>* sink) {
+    if (el.props.size() != 1 || !el.props[0].list || el.props[0].type == kInvalid ||
+        el.props[0].count_type == kInvalid || el.size == 0)
+      return false;
+    const PlyProp& p = el.props[0];
+    const size_t cs = (size_t)kStride[p.count_type], st = (size_t)kStride[p.type];
+    const size_t left = buf_.size() - at_;
+    if (left < cs) return false;
+    const uint8_t* base = reinterpret_cast<const uint8_t*>(buf_.data()) + at_;
+    uint8_t v[8] = {0};
+    for (size_t b = 0; b < cs; ++b) v[b] = base[big_ ? cs - 1 - b : b];
+    uint64_t n;
+    std::memcpy(&n, v, 8);
+    if (n > (left - cs) / st) return false;
+    const size_t rec = cs + (size_t)n * st;
+    if (el.size > left / rec) return false;
+    if (cs == 1) {
+      for (size_t i = 1; i < el.size; ++i)
+        if (base[i * rec] != base[0]) return false;
+    } else {
+      for (size_t i = 1; i < el.size; ++i)
+        if (std::memcmp(base + i * rec, base, cs) != 0) return false;
+    }
+    if (sink) {
+      const size_t old = sink->size(), item_bytes = (size_t)n * st;
+      sink->resize(old + el.size * item_bytes);
+      uint8_t* dst = sink->data() + old;
+      if (!big_) {
+        strided_copy(dst, base + cs, el.size, rec, item_bytes);
+      } else {
+        for (size_t i = 0; i < el.size; ++i, dst += item_bytes) {
+          const uint8_t* src = base + i * rec + cs;
+          for (size_t j = 0; j < n; ++j)
+            for (size_t b = 0; b < st; ++b) dst[j * st + b] = src[j * st + st - 1 - b];
+        }
+      }
+    }
+    at_ += el.size * rec;
+    return true;
+  }
+  // count pieces of `size` bytes, `stride` apart at src, packed at dst; the
+  // usual piece sizes as fixed-size copies.
+  static void strided_copy(uint8_t* dst, const uint8_t* src, size_t count, size_t stride, size_t size) {
+    switch (size) {
+      case 4: for (size_t i = 0; i < count; ++i) std::memcpy(dst + 4 * i, src + i * stride, 4); break;
+      case 6: for (size_t i = 0; i < count; ++i) std::memcpy(dst + 6 * i, src + i * stride, 6); break;
+      case 8: for (size_t i = 0; i < count; ++i) std::memcpy(dst + 8 * i, src + i * stride, 8); break;
+      case 12: for (size_t i = 0; i < count; ++i) std::memcpy(dst + 12 * i, src + i * stride, 12); break;
+      case 16: for (size_t i = 0; i < count; ++i) std::memcpy(dst + 16 * i, src + i * stride, 16); break;
+      default:
+        if (size == stride) std::memcpy(dst, src, count * size);
+        else for (size_t i = 0; i < count; ++i) std::memcpy(dst + size * i, src + i * stride, size);
+    }
   }
   static bool fixed_layout(const PlyElem& el) {
     for (const auto& p : el.props)
@@ -630,31 +703,51 @@ int load_ply(const char* path, fk_mesh& m) {
     if (f.bytes.size() < (size_t)fs * 3 * f.count) return FK_ERR_INVALID;
     m.vertices.resize(9 * f.count);
     m.triangles.resize(3 * f.count);
-    uint32_t normal = kNone;
-    for (size_t i = 0; i < f.count; ++i) {
-      const uint32_t v0 = (uint32_t)(3 * i);
-      if (from == kFace) normal = (uint32_t)i * 3;
-      for (size_t j = 0; j < 3; ++j) {
-        const uint8_t* q = f.bytes.data() + (size_t)fs * (3 * i + j);
-        uint32_t vi = 0;
-        switch (f.type) {
-          case kU32: std::memcpy(&vi, q, 4); break;
-          case kU16: { uint16_t x; std::memcpy(&x, q, 2); vi = x; } break;
-          case kI32: { int32_t x; std::memcpy(&x, q, 4); vi = (uint32_t)x; } break;
-          case kI16: { int16_t x; std::memcpy(&x, q, 2); vi = (uint32_t)(int32_t)x; } break;
-          case kI8: { int8_t x; std::memcpy(&x, q, 1); vi = (uint32_t)(int32_t)x; } break;
-          default: vi = *q; break;  // kU8
+    // every face's three corners are vertices of their own: faces [a, b)
+    // write their own slots, so large files split them over threads
+    auto corners = [&](size_t a, size_t b) {
+      uint32_t normal = kNone;
+      for (size_t i = a; i < b; ++i) {
+        const uint32_t v0 = (uint32_t)(3 * i);
+        if (from == kFace) normal = (uint32_t)i * 3;
+        for (size_t j = 0; j < 3; ++j) {
+          const uint8_t* q = f.bytes.data() + (size_t)fs * (3 * i + j);
+          uint32_t vi = 0;
+          switch (f.type) {
+            case kU32: std::memcpy(&vi, q, 4); break;
+            case kU16: { uint16_t x; std::memcpy(&x, q, 2); vi = x; } break;
+            case kI32: { int32_t x; std::memcpy(&x, q, 4); vi = (uint32_t)x; } break;
+            case kI16: { int16_t x; std::memcpy(&x, q, 2); vi = (uint32_t)(int32_t)x; } break;
+            case kI8: { int8_t x; std::memcpy(&x, q, 1); vi = (uint32_t)(int32_t)x; } break;
+            default: vi = *q; break;  // kU8
+          }
+          if (from == kVertex) normal = vi;
+          uint32_t* vx = &m.vertices[9 * i + 3 * j];
+          vx[0] = vi;
+          vx[1] = uvs >= 0 ? vi : kNone;
+          vx[2] = normal;
         }
-        if (from == kVertex) normal = vi;
-        uint32_t* vx = &m.vertices[9 * i + 3 * j];
-        vx[0] = vi;
-        vx[1] = uvs >= 0 ? vi : kNone;
-        vx[2] = normal;
+        m.triangles[3 * i] = v0;
+        m.triangles[3 * i + 1] = v0 + 1;
+        m.triangles[3 * i + 2] = v0 + 2;
       }
-      m.triangles[3 * i] = v0;
-      m.triangles[3 * i + 1] = v0 + 1;
-      m.triangles[3 * i + 2] = v0 + 2;
+    };
+    const size_t nf = (size_t)f.count;
+    size_t parts = nf < ((size_t)1 << 16) ? 1 : std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(), 16));
+    std::vector<std::thread> pool;
+    pool.reserve(parts);  // so that only starting a thread can throw below
+    for (size_t k = 0; k < parts; ++k) {
+      const size_t a = nf * k / parts, b = nf * (k + 1) / parts;
+      if (k + 1 < parts) {
+        try {
+          pool.emplace_back(corners, a, b);
+          continue;
+        } catch (const std::system_error&) {  // no more threads: this range on this one
+        }
+      }
+      corners(a, b);
     }
+    for (auto& t : pool) t.join();
     return FK_OK;
   } catch (const BadPly&) {
     return FK_ERR_INVALID;
