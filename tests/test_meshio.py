@@ -172,6 +172,25 @@ def test_ply_matches_reference(reference, tmp_path, name):
         assert list(mine[3][3:6, 2]) == [3, 3, 3]  # face i's corners name normal 3 i
 
 
+@pytest.mark.parametrize("fmt", ["binary_little_endian", "binary_big_endian"])
+@pytest.mark.parametrize("count_type,index_type", [("uchar", "uint"), ("int", "ushort"), ("ushort", "uint")])
+@pytest.mark.parametrize("lengths", ["triangles", "quads", "mixed"])
+def test_ply_face_lists_of_one_length(reference, tmp_path, fmt, count_type, index_type, lengths):
+    """A face element holding only the index list: when every face has the
+    first one's length the loader copies the records in bulk, otherwise face
+    by face; both read what the reference reads."""
+    pos, uv, nrm, _, faces = MF.random_ply_mesh(5, n=40, m=60)
+    if lengths == "quads":
+        faces = [f + [int((f[0] + 1) % 40)] for f in faces]
+    elif lengths == "mixed":
+        faces[17] = faces[17] + [int((faces[17][0] + 1) % 40)]
+    p = write(tmp_path, "u.ply", MF.ply_bytes(pos, faces, fmt=fmt, uv=uv, nrm=nrm, count_type=count_type,
+                                               index_type=index_type, extra=False))
+    ref = reference.load_mesh(p)
+    assert resolves(ref)
+    assert same_mesh(load(p), ref)
+
+
 def test_ply_polygons_read_as_triples(reference, tmp_path):
     # quads: the reference reads the flattened index list three at a time
     pos, uv, nrm, _, _ = MF.random_ply_mesh(3, n=30, m=4)
