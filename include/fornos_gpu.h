@@ -202,7 +202,7 @@ int fk_bvh_build_flat(fk_ctx* ctx, const fk_mesh* mesh, uint32_t max_tris, uint3
 /* ------------------------------------------------------------ device scene */
 /* Checks the node array (FK_ERR_INVALID names the first defective node) and
  * lays it out for the device on host threads, in pinned host memory that the
- * context keeps for later uploads (about 68 bytes per node; fk_ctx_trim
+ * context keeps for later uploads (72 bytes per node; fk_ctx_trim
  * releases it).  Returns once the scene is on the device. */
 int fk_scene_upload(fk_ctx* ctx, const fk_bvh_node* nodes, uint32_t node_count, const float* positions4,
                     const float* normals4, uint32_t corner_count, fk_scene** out);
