@@ -53,3 +53,24 @@ def test_layout_of_a_single_leaf_and_a_large_tree(checker):
     leaf = c.nodes[:1].copy()
     leaf["start"], leaf["end"], leaf["jump"] = 0, 3, 1
     run(checker, leaf, 3, 50, 6, "leaf")
+
+
+@pytest.mark.parametrize("sanitizer,name,mutations", [("address,undefined", "icosphere", 400),
+                                                      ("thread", "large", 10)])
+def test_layout_under_sanitizers(checker, sanitizer, name, mutations):
+    """The same comparison with the layout built under AddressSanitizer /
+    UBSan (reads past the node array on malformed trees) and ThreadSanitizer
+    (races between the ranges' threads)."""
+    c = cases.icosphere() if name == "icosphere" else cases.plane(hi=384)
+    exe = os.path.join(OUT, "layout_check_" + sanitizer.split(",")[0])
+    p = subprocess.run(["g++", "-std=c++17", "-O1", "-g", "-pthread", "-fno-omit-frame-pointer",
+                        "-fsanitize=" + sanitizer, os.path.join(ROOT, "tests", "layout_check", "check.cpp"),
+                        os.path.join(ROOT, "fornos_b200", "csrc", "fk_layout.cpp"), "-o", exe],
+                       capture_output=True, text=True)
+    if p.returncode != 0:
+        pytest.skip("no %s runtime: %s" % (sanitizer, p.stderr.strip().splitlines()[-1:]))
+    path = os.path.join(OUT, "layout_san_%s.bin" % name)
+    np.ascontiguousarray(c.nodes).tofile(path)
+    r = subprocess.run([exe, path, str(c.pos4.shape[0]), str(mutations), "9"], capture_output=True, text=True)
+    assert r.returncode == 0 and "ERROR" not in r.stderr and "WARNING" not in r.stderr, r.stderr[-2000:]
+    assert "mismatches 0" in r.stdout.splitlines()[-1]
