@@ -566,6 +566,7 @@ class PlyReader {
   // count pieces of `size` bytes, `stride` apart at src, packed at dst; the
   // usual piece sizes as fixed-size copies.
   static void strided_copy(uint8_t* dst, const uint8_t* src, size_t count, size_t stride, size_t size) {
+    if (count == 0 || size == 0) return;  // dst may be an empty vector's null data
     switch (size) {
       case 4: for (size_t i = 0; i < count; ++i) std::memcpy(dst + 4 * i, src + i * stride, 4); break;
       case 6: for (size_t i = 0; i < count; ++i) std::memcpy(dst + 6 * i, src + i * stride, 6); break;
@@ -660,7 +661,7 @@ bool tuples(const Request* r, int w, std::vector<float>& out) {
   if (r->type == kF32) {
     if (r->bytes.size() < 4 * (size_t)w * r->count) return false;
     out.resize((size_t)w * r->count);
-    std::memcpy(out.data(), r->bytes.data(), 4 * out.size());
+    if (!out.empty()) std::memcpy(out.data(), r->bytes.data(), 4 * out.size());
   } else if (r->type == kF64) {
     if (r->bytes.size() < 8 * (size_t)w * r->count) return false;
     out.resize((size_t)w * r->count);

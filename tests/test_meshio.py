@@ -16,6 +16,7 @@ elements, truncated data; and the cases this loader defines where the
 reference's result is unusable (no s / t or no normals, int index lists).
 """
 import os
+import re
 
 import numpy as np
 import pytest
@@ -356,3 +357,54 @@ def test_obj_large_file_in_ranges(reference, tmp_path):
         mine = load(p)
         assert same_mesh(mine, ref), name
         assert (ref is None) == name.startswith("late"), name
+
+
+def test_loaders_under_sanitizers(tmp_path):
+    """fk_meshio.cpp built alone under AddressSanitizer / UBSan
+    (tests/meshio_check/load_files.cpp) over seeded mutations of valid PLY files
+    (ASCII and both binary orders; uchar / ushort / int counts; triangles,
+    quads and extra properties) and OBJ files: no read or write outside a
+    buffer, no undefined behaviour, whatever the bytes."""
+    import subprocess
+
+    from fornos_b200 import build as fk_build
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "load_files")
+    p = subprocess.run(["g++", "-std=c++17", "-O1", "-g", "-pthread", "-fno-omit-frame-pointer",
+                        "-fsanitize=address,undefined", "-I" + os.path.join(fk_build.CUDA, "include"),
+                        os.path.join(root, "tests", "meshio_check", "load_files.cpp"),
+                        os.path.join(root, "fornos_b200", "csrc", "fk_meshio.cpp"),
+                        os.path.join(root, "fornos_b200", "csrc", "fk_mesh.cpp"), "-o", exe],
+                       capture_output=True, text=True)
+    if p.returncode != 0:
+        pytest.skip("no sanitizer build: %s" % p.stderr.strip().splitlines()[-1:])
+    rng = np.random.default_rng(31)
+    pos, uv, nrm, _, faces = MF.random_ply_mesh(1, n=12, m=10)
+    quads = [f + [int((f[0] + 1) % 12)] for f in faces]
+    bases = []
+    for fmt in ("binary_little_endian", "binary_big_endian", "ascii"):
+        for ct, it in (("uchar", "uint"), ("ushort", "uint"), ("int", "ushort")):
+            for fc in (faces, quads):
+                bases.append((".ply", MF.ply_bytes(pos, fc, fmt=fmt, uv=uv, nrm=nrm, count_type=ct, index_type=it,
+                                                   extra=False)))
+        bases.append((".ply", MF.ply_bytes(pos, faces, fmt=fmt, uv=uv, nrm=nrm)))
+    bases += [(".obj", MF.obj_text(3, c, n_pos=8, n_faces=6).encode()) for c in ("v", "vt", "vn", "vtn")]
+    files = []
+    for i in range(4000):
+        ext, data = bases[i % len(bases)]
+        b = bytearray(data)
+        for _ in range(int(rng.integers(1, 4))):
+            k = int(rng.integers(3))
+            if k == 0:
+                b[int(rng.integers(len(b)))] = int(rng.integers(256))
+            elif k == 1 and len(b) > 2:
+                b = b[:int(rng.integers(1, len(b)))]
+            else:
+                j = int(rng.integers(len(b) + 1))
+                b[j:j] = bytes(rng.integers(0, 256, int(rng.integers(1, 9)), dtype=np.uint8))
+        files.append(write(tmp_path, "m%04d%s" % (i, ext), bytes(b)))
+    files += [write(tmp_path, "base%02d%s" % (i, ext), data) for i, (ext, data) in enumerate(bases)]
+    r = subprocess.run([exe] + files, capture_output=True, text=True)
+    assert r.returncode == 0 and "runtime error" not in r.stderr and "ERROR" not in r.stderr, r.stderr[-2000:]
+    counts = dict(re.findall(r"(\w+) (\d+)", r.stdout))
+    assert int(counts["loaded"]) >= len(bases)  # every valid base file loads
