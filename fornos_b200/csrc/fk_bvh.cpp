@@ -12,6 +12,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <system_error>
 #include <thread>
 
 #include "fk_bvh_rules.h"
@@ -144,9 +145,14 @@ struct Build {
     int32_t li, ri;
     if ((int)depth < par_depth && (e - b) > 65536) {
       std::vector<Node> lv(1, L), rv(1, R);
-      std::thread th([&] { divide(lv, 0, b, w, depth + 1); });
+      std::thread th;
+      try {
+        th = std::thread([&] { divide(lv, 0, b, w, depth + 1); });
+      } catch (const std::system_error&) {  // no thread to be had: the left half here, first
+        divide(lv, 0, b, w, depth + 1);
+      }
       divide(rv, 0, w, e, depth + 1);
-      th.join();
+      if (th.joinable()) th.join();
       li = (int32_t)out.size();
       append(out, lv);
       ri = (int32_t)out.size();

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstring>
 #include <random>
+#include <system_error>
 #include <thread>
 #include <unordered_map>
 
@@ -265,10 +266,17 @@ int fk_samples_cosine(uint32_t spp, uint32_t perms, uint32_t seed, float* out4) 
     return FK_OK;
   }
   std::vector<std::thread> pool;
-  for (unsigned t = 0; t < threads; ++t)
-    pool.emplace_back([&, t] {
-      for (uint32_t row = t; row < perms; row += threads) fill(row);
-    });
+  pool.reserve(threads);
+  unsigned t = 0;
+  try {
+    for (; t < threads; ++t)
+      pool.emplace_back([&, t] {
+        for (uint32_t row = t; row < perms; row += threads) fill(row);
+      });
+  } catch (const std::system_error&) {  // no more threads: the remaining rows here
+  }
+  for (unsigned u = t; u < threads; ++u)
+    for (uint32_t row = u; row < perms; row += threads) fill(row);
   for (auto& th : pool) th.join();
   return FK_OK;
 }

@@ -9,6 +9,7 @@
 #include <array>
 #include <atomic>
 #include <cstring>
+#include <system_error>
 #include <thread>
 #include <vector>
 
@@ -101,7 +102,11 @@ struct SahBuilder {
       refs[s] = (int32_t)kids[s];
       cnts[s] = 0;
       if (s == 0 && hi[1] - lo[1] > 1 && hi[0] - lo[0] >= kParallelLeaves) {
-        side = std::thread([this, &boxes, &kids, &lo, &hi, level] { boxes[0] = build(kids[0], lo[0], hi[0], level + 1); });
+        try {
+          side = std::thread([this, &boxes, &kids, &lo, &hi, level] { boxes[0] = build(kids[0], lo[0], hi[0], level + 1); });
+        } catch (const std::system_error&) {  // no thread to be had: built here
+          boxes[0] = build(kids[0], lo[0], hi[0], level + 1);
+        }
       } else {
         boxes[s] = build(kids[s], lo[s], hi[s], level + 1);
       }
