@@ -19,7 +19,9 @@
 #include <cfloat>
 #include <cstring>
 #include <future>
+#include <memory>
 #include <string>
+#include <system_error>
 #include <vector>
 
 #include "fk_internal.h"
@@ -165,10 +167,20 @@ int fk_run(fk_ctx* ctx, const fk_run_params* p) {
     if (r != FK_OK) return r;
     const uint32_t planes = vec3 ? 3 : 1;
     std::string file(path);
-    writes.emplace_back(file, std::async(std::launch::async, [host = std::move(host), file, f, w, h, planes]() {
-      return f == kRgb8 ? fk_image_write_rgb8(file.c_str(), w, h, reinterpret_cast<const uint8_t*>(host.data()))
-                        : fk_image_write_exr(file.c_str(), w, h, planes, host.data());
-    }));
+    auto pixels = std::make_shared<std::vector<float>>(std::move(host));
+    auto job = [pixels, file, f, w, h, planes]() {
+      return f == kRgb8 ? fk_image_write_rgb8(file.c_str(), w, h, reinterpret_cast<const uint8_t*>(pixels->data()))
+                        : fk_image_write_exr(file.c_str(), w, h, planes, pixels->data());
+    };
+    std::future<int> done;
+    try {
+      done = std::async(std::launch::async, job);
+    } catch (const std::system_error&) {  // no thread to be had: written here
+      std::promise<int> now;
+      now.set_value(job());
+      done = now.get_future();
+    }
+    writes.emplace_back(file, std::move(done));
     return FK_OK;
   };
   auto gather = [&](int kind, size_t width, int tangent, fk_buf** out) -> int {
