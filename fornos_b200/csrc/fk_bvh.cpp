@@ -12,6 +12,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <system_error>
 #include <thread>
 
@@ -57,39 +58,114 @@ struct Pre {
 
 using Node = fk_bvh_tree_node;
 
+// Threads for one pass of the build over n triangles: one below 2^18, else
+// as many as the host has (16 at most) with at least 2^17 triangles each.
+unsigned pass_threads(uint32_t n) {
+  if (n < (1u << 18)) return 1;
+  const unsigned hw = std::thread::hardware_concurrency();
+  return std::max(1u, std::min(std::min(hw ? hw : 1u, 16u), n >> 17));
+}
+
+// fn(k, x, y) over [b, e) cut into T chunks in order; the calling thread takes
+// the last chunk, and any chunk whose thread cannot be started.
+template <typename F>
+void over_chunks(uint32_t b, uint32_t e, unsigned T, F&& fn) {
+  std::vector<std::thread> pool;
+  pool.reserve(T);
+  for (unsigned k = 0; k < T; ++k) {
+    const uint32_t x = b + (uint32_t)((uint64_t)(e - b) * k / T);
+    const uint32_t y = b + (uint32_t)((uint64_t)(e - b) * (k + 1) / T);
+    if (k + 1 < T) {
+      try {
+        pool.emplace_back([&fn, k, x, y] { fn(k, x, y); });
+        continue;
+      } catch (const std::system_error&) {
+      }
+    }
+    fn(k, x, y);
+  }
+  for (auto& th : pool) th.join();
+}
+
+// Bucket counts and triangle bounds of one axis choice (Src/bvh.cpp:139-170).
+struct Bins {
+  uint32_t cnt[3][16];
+  float blo[3][16][3], bhi[3][16][3];
+  void clear() {
+    for (int a = 0; a < 3; ++a)
+      for (int k = 0; k < 16; ++k) {
+        cnt[a][k] = 0;
+        for (int q = 0; q < 3; ++q) {
+          blo[a][k][q] = FLT_MAX;
+          bhi[a][k][q] = -FLT_MAX;
+        }
+      }
+  }
+  void merge(const Bins& o) {
+    for (int a = 0; a < 3; ++a)
+      for (int k = 0; k < 16; ++k) {
+        cnt[a][k] += o.cnt[a][k];
+        for (int q = 0; q < 3; ++q) {
+          blo[a][k][q] = fk::bvh::fmin(o.blo[a][k][q], blo[a][k][q]);
+          bhi[a][k][q] = fk::bvh::fmax(o.bhi[a][k][q], bhi[a][k][q]);
+        }
+      }
+  }
+};
+
+// Large ranges run their passes (centroid bounds, buckets, partition) over
+// chunks on several threads: counts add up and the bounds are min / max folds
+// whose order does not matter, and the chunks' sides are joined in chunk order,
+// so the tree is the sequential build's, bit for bit.
 struct Build {
-  const std::vector<Pre>& pre;
+  const Pre* pre;
   std::vector<uint32_t>& order;
   size_t max_tris, max_depth;
   int par_depth;
 
   // Returns (axis, split value) of Src/bvh.cpp:128-203.
-  void choose(uint32_t b, uint32_t e, int* axis, float* value) const {
-    Box cb = empty_box();
-    for (uint32_t i = b; i < e; ++i) add_point(cb, pre[order[i]].cdiv);
-    uint32_t cnt[3][16] = {};
-    float blo[3][16][3], bhi[3][16][3];
-    for (int a = 0; a < 3; ++a)
-      for (int k = 0; k < 16; ++k)
-        for (int q = 0; q < 3; ++q) {
-          blo[a][k][q] = FLT_MAX;
-          bhi[a][k][q] = -FLT_MAX;
-        }
-    float ext[3];
-    for (int a = 0; a < 3; ++a) ext[a] = cb.hi[a] - cb.lo[a];
-    for (uint32_t i = b; i < e; ++i) {
+  Box centroid_bounds(uint32_t x, uint32_t y) const {
+    Box c = empty_box();
+    for (uint32_t i = x; i < y; ++i) add_point(c, pre[order[i]].cdiv);
+    return c;
+  }
+  void fill_bins(uint32_t x, uint32_t y, const Box& cb, const float* ext, Bins& B) const {
+    B.clear();
+    for (uint32_t i = x; i < y; ++i) {
       const Pre& p = pre[order[i]];
       for (int a = 0; a < 3; ++a) {
-        const uint32_t k = fk::bvh::bucket(p.cdiv[a], cb.lo[a], ext[a]);
-        cnt[a][k]++;
+        const uint32_t q = fk::bvh::bucket(p.cdiv[a], cb.lo[a], ext[a]);
+        B.cnt[a][q]++;
         for (int c = 0; c < 3; ++c)
-          for (int q = 0; q < 3; ++q) {
-            blo[a][k][q] = fk::bvh::fmin(p.p[c][q], blo[a][k][q]);
-            bhi[a][k][q] = fk::bvh::fmax(p.p[c][q], bhi[a][k][q]);
+          for (int r = 0; r < 3; ++r) {
+            B.blo[a][q][r] = fk::bvh::fmin(p.p[c][r], B.blo[a][q][r]);
+            B.bhi[a][q][r] = fk::bvh::fmax(p.p[c][r], B.bhi[a][q][r]);
           }
       }
     }
-    fk::bvh::pick_split(blo, bhi, cnt, (int)(e - b), cb.lo, cb.hi, axis, value);
+  }
+
+  void choose(uint32_t b, uint32_t e, int* axis, float* value) const {
+    const unsigned T = pass_threads(e - b);
+    Box cb;
+    float ext[3];
+    if (T == 1) {
+      cb = centroid_bounds(b, e);
+      for (int a = 0; a < 3; ++a) ext[a] = cb.hi[a] - cb.lo[a];
+      Bins B;
+      fill_bins(b, e, cb, ext, B);
+      fk::bvh::pick_split(B.blo, B.bhi, B.cnt, (int)(e - b), cb.lo, cb.hi, axis, value);
+      return;
+    }
+    std::vector<Box> cbs(T);
+    over_chunks(b, e, T, [&](unsigned k, uint32_t x, uint32_t y) { cbs[k] = centroid_bounds(x, y); });
+    cb = cbs[0];
+    for (unsigned k = 1; k < T; ++k) cb = join(cb, cbs[k]);
+    for (int a = 0; a < 3; ++a) ext[a] = cb.hi[a] - cb.lo[a];
+    std::vector<Bins> bins(T);
+    over_chunks(b, e, T, [&](unsigned k, uint32_t x, uint32_t y) { fill_bins(x, y, cb, ext, bins[k]); });
+    for (unsigned k = 1; k < T; ++k) bins[0].merge(bins[k]);
+    fk::bvh::pick_split(bins[0].blo, bins[0].bhi, bins[0].cnt, (int)(e - b), cb.lo, cb.hi, axis, value);
   }
 
   static void set_box(Node& n, const Box& b) {
@@ -111,25 +187,55 @@ struct Build {
     int axis;
     float split;
     choose(b, e, &axis, &split);
-    // Order-preserving partition (triangles keep their relative order on each side).
+    // Order-preserving partition (triangles keep their relative order on each
+    // side).  A large range splits in chunks, each into its own two sides; the
+    // left sides then go back in chunk order, followed by the right sides.
     std::vector<uint32_t> right;
     Box lb = empty_box(), rb = empty_box();
     uint32_t w = b;
-    for (uint32_t i = b; i < e; ++i) {
-      uint32_t t = order[i];
+    auto side_of = [&](uint32_t t, Box& l, Box& r, bool& left) {
       const Pre& p = pre[t];
       float lo[3], hi[3];
       for (int a = 0; a < 3; ++a) {
         lo[a] = fk::bvh::fmin(p.p[0][a], fk::bvh::fmin(p.p[1][a], p.p[2][a]));
         hi[a] = fk::bvh::fmax(p.p[0][a], fk::bvh::fmax(p.p[1][a], p.p[2][a]));
       }
-      if (p.cmul[axis] <= split) {
-        order[w++] = t;
-        grow_acc(lb, lo, hi);
-      } else {
-        right.push_back(t);
-        grow_acc(rb, lo, hi);
+      left = p.cmul[axis] <= split;
+      grow_acc(left ? l : r, lo, hi);
+    };
+    const unsigned T = pass_threads(e - b);
+    if (T == 1) {
+      for (uint32_t i = b; i < e; ++i) {
+        const uint32_t t = order[i];
+        bool left;
+        side_of(t, lb, rb, left);
+        if (left) order[w++] = t;
+        else right.push_back(t);
       }
+    } else {
+      struct Sides {
+        std::vector<uint32_t> left, right;
+        Box lb, rb;
+      };
+      std::vector<Sides> parts(T);
+      over_chunks(b, e, T, [&](unsigned k, uint32_t x, uint32_t y) {
+        Sides& s = parts[k];
+        s.lb = s.rb = empty_box();
+        for (uint32_t i = x; i < y; ++i) {
+          const uint32_t t = order[i];
+          bool left;
+          side_of(t, s.lb, s.rb, left);
+          (left ? s.left : s.right).push_back(t);
+        }
+      });
+      for (Sides& s : parts) {
+        std::copy(s.left.begin(), s.left.end(), order.begin() + w);
+        w += (uint32_t)s.left.size();
+        lb = join(lb, s.lb);
+        rb = join(rb, s.rb);
+      }
+      right.reserve(e - w);
+      for (Sides& s : parts) right.insert(right.end(), s.right.begin(), s.right.end());
     }
     if (w == b || w == e) {  // Src/bvh.cpp:248-256: cannot split, stays a leaf
       std::copy(right.begin(), right.end(), order.begin() + w);
@@ -250,18 +356,22 @@ extern "C" {
 int fk_bvh_build(const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, fk_bvh** out) {
   if (!mesh || !out || max_tris == 0) return FK_ERR_INVALID;
   const uint32_t nf = mesh->triangle_count();
-  std::vector<Pre> pre(nf);
-  for (uint32_t f = 0; f < nf; ++f) {
-    const float* p[3];
-    for (int k = 0; k < 3; ++k) p[k] = &mesh->positions[3 * (size_t)mesh->vertices[3 * (size_t)mesh->triangles[3 * (size_t)f + k]]];
-    Pre& q = pre[f];
-    for (int a = 0; a < 3; ++a) {
-      float s = p[0][a] + p[1][a] + p[2][a];
-      q.cdiv[a] = s / 3.0f;
-      q.cmul[a] = s * (1.0f / 3.0f);
-      for (int k = 0; k < 3; ++k) q.p[k][a] = p[k][a];
+  std::unique_ptr<Pre[]> pre(new (std::nothrow) Pre[nf ? nf : 1]);
+  if (!pre) return FK_ERR_NOMEM;
+  over_chunks(0, nf, pass_threads(nf), [&](unsigned, uint32_t x, uint32_t y) {
+    for (uint32_t f = x; f < y; ++f) {
+      const float* p[3];
+      for (int k = 0; k < 3; ++k)
+        p[k] = &mesh->positions[3 * (size_t)mesh->vertices[3 * (size_t)mesh->triangles[3 * (size_t)f + k]]];
+      Pre& q = pre[f];
+      for (int a = 0; a < 3; ++a) {
+        float s = p[0][a] + p[1][a] + p[2][a];
+        q.cdiv[a] = s / 3.0f;
+        q.cmul[a] = s * (1.0f / 3.0f);
+        for (int k = 0; k < 3; ++k) q.p[k][a] = p[k][a];
+      }
     }
-  }
+  });
   fk_bvh* t = new (std::nothrow) fk_bvh();
   if (!t) return FK_ERR_NOMEM;
   t->triangle_count = nf;
@@ -280,7 +390,7 @@ int fk_bvh_build(const fk_mesh* mesh, uint32_t max_tris, uint32_t max_depth, fk_
   unsigned hw = std::thread::hardware_concurrency();
   int par = 0;
   while ((1u << par) < (hw ? hw : 1) && par < 6) ++par;
-  Build b{pre, t->order, max_tris, max_depth, par};
+  Build b{pre.get(), t->order, max_tris, max_depth, par};
   b.divide(t->nodes, 0, 0, nf, 0);
   *out = t;
   return FK_OK;

@@ -3,7 +3,8 @@ AddressSanitizer / UBSan and under ThreadSanitizer (tests/host_check): mesh
 generators, the BVH build with its threaded top levels and the flatten
 (Src/bvh.cpp, Src/meshmapping.cpp:62-125), the host surface-area tree, the
 scene upload's node layout, the sample table and the image writers, on a
-seeded random mesh large enough for every threaded path."""
+seeded random mesh large enough for every threaded path (300k triangles: the
+BVH build's chunked passes start at 2^18)."""
 import os
 import subprocess
 
@@ -25,7 +26,7 @@ def test_host_code_under_sanitizers(tmp_path, sanitizer, seed):
                        capture_output=True, text=True)
     if p.returncode != 0:
         pytest.skip("no %s build: %s" % (sanitizer, p.stderr.strip().splitlines()[-1:]))
-    r = subprocess.run([exe, str(seed), "150000", str(tmp_path)], capture_output=True, text=True)
+    r = subprocess.run([exe, str(seed), "300000", str(tmp_path)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.strip().endswith("ok"), r.stdout[-1000:] + r.stderr[-2000:]
     assert "runtime error" not in r.stderr and "WARNING" not in r.stderr and "ERROR" not in r.stderr, \
         r.stderr[-3000:]
