@@ -295,12 +295,16 @@ struct Build {
 };
 
 // Walks the fillMeshData recursion: emits nodes / corners through callbacks.
+// A leaf's corners in the flattened arrays: from corner `corner`, the
+// corners of triangles order[first .. first + count).
+struct LeafRun {
+  uint32_t corner, first, count;
+};
+
 struct Flatten {
   const fk_bvh& t;
-  const fk_mesh* mesh;
   fk_bvh_node* nodes;
-  float* pos4;
-  float* nrm4;
+  std::vector<LeafRun>* runs;  // the leaves' corner runs, written after the walk (or null: counts only)
   uint32_t n_nodes = 0, n_corners = 0;
 
   void visit(int32_t ni) {
@@ -316,21 +320,8 @@ struct Flatten {
     uint32_t me = n_nodes++;
     uint32_t start = n_corners;
     if (!kids) {
-      for (uint32_t i = 0; i < n.count; ++i) {
-        uint32_t f = t.order[n.first + i];
-        for (int k = 0; k < 3; ++k) {
-          if (pos4) {
-            const uint32_t* v = &mesh->vertices[3 * (size_t)mesh->triangles[3 * (size_t)f + k]];
-            const float* p = &mesh->positions[3 * (size_t)v[0]];
-            const float* q = &mesh->normals[3 * (size_t)v[2]];
-            float* dp = pos4 + 4 * (size_t)n_corners;
-            float* dn = nrm4 + 4 * (size_t)n_corners;
-            dp[0] = p[0]; dp[1] = p[1]; dp[2] = p[2]; dp[3] = 0.0f;
-            dn[0] = q[0]; dn[1] = q[1]; dn[2] = q[2]; dn[3] = 0.0f;
-          }
-          ++n_corners;
-        }
-      }
+      if (runs) runs->push_back({n_corners, n.first, n.count});
+      n_corners += 3 * n.count;
     }
     if (nodes) {
       fk_bvh_node& d = nodes[me];
@@ -403,7 +394,7 @@ int fk_bvh_free(fk_bvh* bvh) {
 
 int fk_bvh_flatten_sizes(const fk_bvh* bvh, uint32_t* node_count, uint32_t* corner_count) {
   if (!bvh || !node_count || !corner_count) return FK_ERR_INVALID;
-  Flatten f{*bvh, nullptr, nullptr, nullptr, nullptr};
+  Flatten f{*bvh, nullptr, nullptr};
   f.visit(0);
   *node_count = f.n_nodes;
   *corner_count = f.n_corners;
@@ -416,8 +407,30 @@ int fk_bvh_flatten(const fk_bvh* bvh, const fk_mesh* mesh, fk_bvh_node* nodes, f
   uint32_t nn = (uint32_t)(mesh->normals.size() / 3);
   for (uint32_t v = 0; v < mesh->vertex_count(); ++v)
     if (mesh->vertices[3 * (size_t)v + 2] >= nn) return FK_ERR_INVALID;
-  Flatten f{*bvh, mesh, nodes, pos4, nrm4};
+  // the walk numbers the nodes and the leaves' corner runs in depth-first
+  // order; the corners (the bulk of the bytes) are then written run by run
+  // over chunks on several threads
+  std::vector<LeafRun> runs;
+  Flatten f{*bvh, nodes, &runs};
   f.visit(0);
+  over_chunks(0, (uint32_t)runs.size(), pass_threads(bvh->triangle_count), [&](unsigned, uint32_t x, uint32_t y) {
+    for (uint32_t r = x; r < y; ++r) {
+      const LeafRun& run = runs[r];
+      uint32_t c = run.corner;
+      for (uint32_t i = 0; i < run.count; ++i) {
+        const uint32_t tri = bvh->order[run.first + i];
+        for (int k = 0; k < 3; ++k, ++c) {
+          const uint32_t* v = &mesh->vertices[3 * (size_t)mesh->triangles[3 * (size_t)tri + k]];
+          const float* p = &mesh->positions[3 * (size_t)v[0]];
+          const float* q = &mesh->normals[3 * (size_t)v[2]];
+          float* dp = pos4 + 4 * (size_t)c;
+          float* dn = nrm4 + 4 * (size_t)c;
+          dp[0] = p[0], dp[1] = p[1], dp[2] = p[2], dp[3] = 0.0f;
+          dn[0] = q[0], dn[1] = q[1], dn[2] = q[2], dn[3] = 0.0f;
+        }
+      }
+    }
+  });
   return FK_OK;
 }
 
