@@ -103,19 +103,21 @@ def test_shaders(oracle, reference, name):
     assert same_bits(a, b)
 
 
-def test_host_bvh_build_of_a_large_mesh(oracle, reference):
+@pytest.mark.parametrize("max_tris,max_depth", [(8, 8192), (1, 3)])
+def test_host_bvh_build_of_a_large_mesh(oracle, reference, max_tris, max_depth):
     """The library's host build (fk_bvh_build + fk_bvh_flatten), whose top
     levels run their passes over chunks on several threads from 2^18
     triangles up, against the reference's own BVH::createBinary +
     fillMeshData on a 627k-triangle heightfield: the same nodes and corner
-    arrays, bit for bit."""
+    arrays, bit for bit (also with the depth limit reached while the splits
+    still run in chunks)."""
     from fornos_b200 import api
     _, hi = W.plane_pair(seed=4, lo_quads=8, hi_quads=560, bumps=40)
     assert hi.triangle_count > 1 << 19  # chunked passes at the root and at its children
     v, n = oracle.normals(hi, "vertex")
     hi.vertices, hi.normals = v, n
     mesh = api.Mesh(hi)
-    mine = api.BVH.create_binary(mesh, 8, 8192).flatten(mesh)
-    ref = reference.scene(hi, 8)
+    mine = api.BVH.create_binary(mesh, max_tris, max_depth).flatten(mesh)
+    ref = reference.scene(hi, max_tris, max_depth)
     assert mine[0].tobytes() == ref[0].tobytes()
     assert same_bits(mine[1], ref[1]) and same_bits(mine[2], ref[2])
